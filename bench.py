@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 FFT provider on the batched C2C workload.
+
+Workload (one step): the three batched 1-D C2C plans of the headline configuration,
+each executed forward then backward, in place, orthogonal normalization, inputs
+uniform[-1, 1) from a seed, all device-resident (every plan's buffer exceeds the
+126 MB L2, so no flush is needed between steps):
+    complex<float>  N=4096  x batch 16384   (512 MiB)
+    complex<float>  N=13440 x batch 4096    (420 MiB)
+    complex<double> N=65536 x batch 512     (512 MiB)
+value  = GFLOP/s over the step (5 N log2 N per transform), all ranks' work / max rank time.
+e2e    = the same metric through the public plan API with pinned HOST buffers: every step
+         copies the inputs host->device, runs the six executes and copies the results back.
+roofline: the dominant kernel's algorithmic bytes (2 * elements * sizeof(complex) per
+         launch) / its CUDA-event launch time, against the measured HBM copy bandwidth.
+cpu_baseline: the CPU restatement of the reference's portable provider (oracle/) on the
+         host cores, on a bounded sample of the same workload.
+--impl reference: times that CPU restatement alone (the reference's portable provider
+         cannot be built here: no SYCL compiler), rank 0 only.
+
+Multi-GPU: one process per GPU (torchrun); every rank runs the same per-GPU workload on
+its own device (independent batches, no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sycl-fft_b200"))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = [
+    # (label, lengths, batch, double)
+    ("c64_4096x16384", [4096], 16384, False),
+    ("c64_13440x4096", [13440], 4096, False),
+    ("c128_65536x512", [65536], 512, True),
+]
+METRIC = "batched C2C GFLOP/s (5N log2N), 1D fwd+bwd in-place orthogonal: c64 4096x16384, c64 13440x4096, c128 65536x512"
+UNIT = "GFLOP/s"
+DOMINANT = "c64_4096x16384"  # its plan is one kernel launch per execute
+
+
+def flops(lengths, batch):
+    n = math.prod(lengths)
+    return 5.0 * n * math.log2(n) * batch
+
+
+def step_flops(workload=WORKLOAD):
+    return sum(2 * flops(l, b) for _, l, b, _ in workload)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dram_traffic_record():
+    p = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(sample_div: int = 16, repeats: int = 3):
+    """Oracle (CPU restatement of the portable provider) on 1/sample_div of each batch."""
+    import numpy as np
+    from oracle import portable
+    portable.build()
+    threads = portable.max_threads()
+    portable.set_threads(threads)
+    total_flops, total_t = 0.0, 0.0
+    for label, lengths, batch, dbl in WORKLOAD:
+        b = max(1, batch // sample_div)
+        n = math.prod(lengths)
+        rng = np.random.default_rng(n)
+        dt = np.complex128 if dbl else np.complex64
+        x = (rng.uniform(-1, 1, n * b) + 1j * rng.uniform(-1, 1, n * b)).astype(dt)
+        plans = [portable.OraclePlan(lengths, b, d, "orthogonal", dbl) for d in (-1, 1)]
+        y = plans[0].execute(x)
+        plans[1].execute(y)
+        t0 = time.perf_counter()
+        for _ in range(repeats):
+            y = plans[0].execute(x)
+            plans[1].execute(y)
+        total_t += time.perf_counter() - t0
+        total_flops += repeats * 2 * flops(lengths, b)
+    return {
+        "value": total_flops / total_t / 1e9, "unit": UNIT, "cores": threads, "kind": "port",
+        "sample": f"1/{sample_div} of each batch ({', '.join(f'{l} x {max(1, b // sample_div)}' for _, l, b, _ in WORKLOAD)}),"
+                  f" fwd+bwd, {repeats} repeats, {total_t:.1f} s; CPU restatement of src/sycl/sycl.cpp"
+                  f" (portable provider), g++ -O3 -fopenmp",
+    }
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import portable
+    portable.build()
+    threads = portable.max_threads()
+    portable.set_threads(threads)
+    # one step = fwd+bwd of each sub-config on a bounded sample sized so K steps take ~1 minute
+    div = 256
+    setups = []
+    for label, lengths, batch, dbl in WORKLOAD:
+        n = math.prod(lengths)
+        rng = np.random.default_rng(n)
+        dt = np.complex128 if dbl else np.complex64
+        setups.append((lengths, batch, dbl, dt, rng))
+
+    def build(div):
+        out = []
+        for lengths, batch, dbl, dt, rng in setups:
+            b = max(1, batch // div)
+            n = math.prod(lengths)
+            x = (rng.uniform(-1, 1, n * b) + 1j * rng.uniform(-1, 1, n * b)).astype(dt)
+            out.append((x, [portable.OraclePlan(lengths, b, d, "orthogonal", dbl) for d in (-1, 1)], lengths, b))
+        return out
+
+    def one_step(sets):
+        for x, plans, _, _ in sets:
+            plans[1].execute(plans[0].execute(x))
+
+    sets = build(div)
+    one_step(sets)
+    t0 = time.perf_counter()
+    one_step(sets)
+    t1 = time.perf_counter() - t0
+    budget = 60.0
+    while div < 16384 and t1 * args.steps > budget:
+        div *= 2
+        t1 /= 2
+    sets = build(div)
+    for _ in range(args.warmup):
+        one_step(sets)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one_step(sets)
+    elapsed = time.perf_counter() - t0
+    fl = sum(2 * flops(l, b) for _, _, l, b in sets)
+    value = fl * args.steps / elapsed / 1e9
+    sample = f"1/{div} of each batch ({', '.join(f'{l} x {b}' for _, _, l, b in sets)}) fwd+bwd per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+        "data": "synthetic", "config": {"workload": "config2_batched_c2c", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample + "; CPU restatement of the portable provider (src/sycl/sycl.cpp), "
+                                            "the SYCL reference itself cannot be built here (no SYCL compiler)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import syclfft_b200 as sf
+
+    world, rank, local = dist_env()
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (the provider has no CPU path)")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal)
+    plans, bufs, hosts = [], [], []
+    for label, lengths, batch, dbl in WORKLOAD:
+        n = math.prod(lengths)
+        g = torch.Generator(device=dev).manual_seed(1000 * rank + n)
+        fdt = torch.float64 if dbl else torch.float32
+        re = torch.rand(n * batch, device=dev, generator=g, dtype=fdt) * 2 - 1
+        im = torch.rand(n * batch, device=dev, generator=g, dtype=fdt) * 2 - 1
+        x = torch.complex(re, im)
+        del re, im
+        kind = "double" if dbl else "float"
+        f = sf.plan_many_dft(kind, lengths, batch, sf.direction.forward, opts)
+        b = sf.plan_many_dft(kind, lengths, batch, sf.direction.backward, opts)
+        plans.append((label, lengths, batch, dbl, f, b))
+        bufs.append(x)
+    stream = torch.cuda.current_stream(dev)
+    launches_per_step = sum(f.launches() + b.launches() for _, _, _, _, f, b in plans)
+
+    def step(record=None):
+        for i, (label, lengths, batch, dbl, f, b) in enumerate(plans):
+            if record is not None:
+                record[i][0].record(stream)
+            f.execute(bufs[i])
+            if record is not None:
+                record[i][1].record(stream)
+            b.execute(bufs[i])
+            if record is not None:
+                record[i][2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    # per-execute events across the timed region (for the roofline of the dominant kernel)
+    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in plans] for _ in range(args.steps)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    start.record(stream)
+    for k in range(args.steps):
+        step(ev[k])
+    end.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier()
+    elapsed_ms = start.elapsed_time(end)
+    t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    elapsed_ms = float(t.item())
+    total_flops = step_flops() * args.steps * world
+    value = total_flops / (elapsed_ms / 1e3) / 1e9
+
+    # per-plan execute times inside the timed region
+    per_plan = {}
+    for i, (label, lengths, batch, dbl, f, b) in enumerate(plans):
+        fw = [ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)]
+        bw = [ev[k][i][1].elapsed_time(ev[k][i][2]) for k in range(args.steps)]
+        nbytes = 2 * math.prod(lengths) * batch * (16 if dbl else 8)
+        per_plan[label] = {"fwd_ms": statistics.mean(fw), "bwd_ms": statistics.mean(bw),
+                           "launches_per_execute": f.launches(),
+                           "gbs_alg": nbytes / (statistics.mean(fw + bw) / 1e3) / 1e9}
+    dom = per_plan[DOMINANT]
+    dom_plan = [p for p in plans if p[0] == DOMINANT][0]
+    dom_bytes = 2 * math.prod(dom_plan[1]) * dom_plan[2] * (16 if dom_plan[3] else 8)
+    dom_ms = (dom["fwd_ms"] + dom["bwd_ms"]) / 2 / dom["launches_per_execute"]
+    peak, peak_kind = measured_peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    traffic = dram_traffic_record()
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "kernel": f"fft_pass_kernel<float,16,256,plain> ({DOMINANT}, radix 16^3, 1 launch per execute)",
+                "alg_bytes_per_launch": dom_bytes,
+                "traffic": traffic.get("bytes_per_launch") if traffic else None}
+
+    # e2e through the public API with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_in = [torch.empty(x.numel(), dtype=x.dtype, pin_memory=True) for x in bufs]
+        host_out = [torch.empty_like(h, pin_memory=True) for h in host_in]
+        for h, x in zip(host_in, bufs):
+            h.copy_(x)
+        h2d = sum(h.numel() * h.element_size() for h in host_in)
+
+        def e2e_step():
+            for i, (_, _, _, _, f, b) in enumerate(plans):
+                bufs[i].copy_(host_in[i], non_blocking=True)
+                f.execute(bufs[i])
+                b.execute(bufs[i])
+                host_out[i].copy_(bufs[i], non_blocking=True)
+
+        for _ in range(2):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        s2, e2 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s2.record(stream)
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        t2 = torch.tensor([s2.elapsed_time(e2)], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t2.item())
+        e2e = {"value": step_flops() * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": args.e2e_steps,
+               "ms_per_step": e2e_ms / args.e2e_steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        alg_bytes_step = sum(2 * 2 * math.prod(l) * b * (16 if d else 8) for _, l, b, d in WORKLOAD)
+        line = {
+            "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (complex64, complex128)",
+            "data": "synthetic (seeded uniform[-1,1) complex)",
+            "config": {"workload": "config2_batched_c2c", "plans": [w[0] for w in WORKLOAD],
+                       "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
+                       "parallelism": f"replicas x{world} (independent batches per GPU)",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "gbs_alg": round(alg_bytes_step * world / (elapsed_ms / 1e3) / 1e9, 1),
+            "per_plan": per_plan,
+            "roofline": roofline,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

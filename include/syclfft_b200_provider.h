@@ -1,0 +1,98 @@
+/* syclfft B200 device provider: C ABI v1.
+ *
+ * This is the drop-in boundary of the B200-native FFT provider for syclfft. It is
+ * modelled on the reference's provider ABIs:
+ *   - include/syclfft/detail/provider_abi.h:23-54 (C ABI v1 of the host/FFTW module:
+ *     plan config struct, provider table {abi_version, name, create, destroy,
+ *     execute}, exported getter) -- same shape, same error-buffer convention;
+ *   - include/syclfft/detail/cufft_provider_abi.hpp:14-47 (C++ ABI v2 of the device
+ *     module: config {double_precision, direction, placement, rank, lengths[3] in
+ *     C order, batch_count}, table {supports, create, destroy, execute}) -- the
+ *     device-provider semantics this module replaces, with the SYCL queue replaced
+ *     by a CUDA device ordinal and the event list by a cudaStream_t.
+ * Differences from cufft_provider_abi.hpp v2: the config also carries the
+ * normalization (fused into the last kernel instead of the front end's extra
+ * scaling pass, src/sycl/sycl.cpp:677-683) and the planning mode (measure runs the
+ * autotuner, matching plan_options::planning, include/syclfft/common.hpp:66-72).
+ *
+ * Errors never cross the boundary as exceptions: functions write a NUL-terminated
+ * message into `err` (capacity `cap`, 1024 bytes is what the front end passes, as
+ * in include/syclfft/detail/provider_error_buffer.hpp:10-18) and return NULL / a
+ * non-zero status. All pointers passed to execute are device (or managed)
+ * allocations of interleaved complex<float> or complex<double> values.
+ */
+#ifndef SYCLFFT_B200_PROVIDER_H
+#define SYCLFFT_B200_PROVIDER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__cplusplus)
+#define SYCLFFT_B200_EXTERN_C extern "C"
+#else
+#define SYCLFFT_B200_EXTERN_C
+#endif
+#define SYCLFFT_B200_EXPORT SYCLFFT_B200_EXTERN_C __attribute__((visibility("default")))
+
+#define SYCLFFT_B200_PROVIDER_ABI_VERSION 1u
+
+/* Same values as SYCLFFT_SCALAR_*_V1 and SYCLFFT_DIRECTION_*_V1 (provider_abi.h:41-46). */
+#define SYCLFFT_B200_SCALAR_FLOAT 1u
+#define SYCLFFT_B200_SCALAR_DOUBLE 2u
+#define SYCLFFT_B200_DIRECTION_FORWARD (-1)
+#define SYCLFFT_B200_DIRECTION_BACKWARD 1
+/* syclfft::normalization order (common.hpp:44-50). */
+#define SYCLFFT_B200_NORM_NONE 0u
+#define SYCLFFT_B200_NORM_FORWARD 1u
+#define SYCLFFT_B200_NORM_BACKWARD 2u
+#define SYCLFFT_B200_NORM_ORTHOGONAL 3u
+
+typedef struct syclfft_b200_plan_config_v1 {
+    uint32_t abi_version;   /* SYCLFFT_B200_PROVIDER_ABI_VERSION */
+    uint32_t scalar;        /* SYCLFFT_B200_SCALAR_FLOAT / _DOUBLE */
+    int32_t direction;      /* -1 forward, +1 backward */
+    uint32_t rank;          /* 1..3 */
+    uint64_t lengths[3];    /* C order, last dimension contiguous */
+    uint64_t batch_count;   /* contiguous batches of prod(lengths) elements */
+    uint32_t in_place;      /* placement::in_place */
+    uint32_t normalization; /* SYCLFFT_B200_NORM_* */
+    uint32_t measure;       /* planning_mode::measure: autotune the kernel shapes */
+    int32_t device;         /* CUDA device ordinal; -1 = the calling thread's current device */
+} syclfft_b200_plan_config_v1;
+
+typedef struct syclfft_b200_provider_v1 {
+    uint32_t abi_version;
+    const char *name;
+    /* cufft_provider_v2::supports: 1 if the device can run this provider. */
+    int (*supports)(int32_t device, char *err, size_t cap);
+    /* cufft_provider_v2::create: builds tables and scratch on the device; NULL on failure. */
+    void *(*create)(const syclfft_b200_plan_config_v1 *config, char *err, size_t cap);
+    /* cufft_provider_v2::destroy: frees tables and scratch (waits for the plan's work). */
+    void (*destroy)(void *plan);
+    /* cufft_provider_v2::execute: enqueues the transform on `stream` (a cudaStream_t,
+     * NULL = legacy default stream) and returns 0, or writes err and returns non-zero.
+     * For in-place plans pass in == out. The input of an out-of-place plan is not
+     * modified. Work is stream-ordered; the caller orders dependencies on the stream. */
+    int (*execute)(void *plan, const void *in, void *out, void *stream, char *err, size_t cap);
+    /* Plan-owned device scratch in bytes (plan<Scalar>::scratch_size_bytes). */
+    uint64_t (*scratch_bytes)(const void *plan);
+} syclfft_b200_provider_v1;
+
+typedef const syclfft_b200_provider_v1 *(*syclfft_b200_get_provider_v1_fn)(void);
+
+/* Module entry point, resolved with dlsym like syclfft_get_host_provider_v1
+ * (provider_abi.h:54) and syclfft_get_cufft_provider_v2 (cufft_provider_abi.hpp:46-47). */
+SYCLFFT_B200_EXPORT const syclfft_b200_provider_v1 *syclfft_b200_get_provider_v1(void);
+
+/* ---- Diagnostics and measurement helpers (no reference counterpart; used by tests,
+ *      the benchmark and the autotuner). ---- */
+
+/* JSON description of the plan's passes (kernel kind, FFT length, radices, tile
+ * shape, bytes moved). Returns the string length, or -1 if it did not fit. */
+SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void *plan, char *buf, size_t cap);
+/* Number of kernel launches one execute performs. */
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
+/* Library version string. */
+SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
+
+#endif /* SYCLFFT_B200_PROVIDER_H */

@@ -1,0 +1,650 @@
+#include "planner.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+
+namespace sfb {
+
+namespace {
+
+constexpr int kSmemDefault = 227 * 1024;
+constexpr int64_t kNoLimit = std::numeric_limits<int64_t>::max() / 4;
+
+struct Factors {
+    int e2 = 0, e3 = 0, e5 = 0, e7 = 0;
+};
+
+bool factor7(uint64_t n, Factors& f) {
+    if (n == 0) return false;
+    while (n % 2 == 0) { n /= 2; ++f.e2; }
+    while (n % 3 == 0) { n /= 3; ++f.e3; }
+    while (n % 5 == 0) { n /= 5; ++f.e5; }
+    while (n % 7 == 0) { n /= 7; ++f.e7; }
+    return n == 1;
+}
+
+int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+int pad_shift_for(bool dbl) { return dbl ? 3 : 4; }
+
+int kmode_pitch(int n, int pad_shift) {
+    int p = n + (n >> pad_shift);
+    if ((p & 1) == 0) p += 1;  // odd pitch: columns of the tile fall in distinct banks
+    return p;
+}
+
+struct SingleCfg {
+    bool ok = false;
+    KernelChoice kc;
+    std::vector<int> radices;
+    int tpl = 0;
+};
+
+// Largest CTA the kernel variant may use, given the register arrays it holds.
+int max_threads_for(bool dbl, int maxv) {
+    if (dbl && maxv >= 16) return 512;
+    return 1024;
+}
+
+SingleCfg single_cfg(int64_t n, bool dbl, int force_maxv) {
+    SingleCfg best;
+    if (n <= 0 || n > (1 << 20) || !smooth7(static_cast<uint64_t>(n))) return best;
+    std::vector<int> cands;
+    if (force_maxv) cands = {force_maxv};
+    else if (dbl) cands = {8, 16};
+    else cands = {16};
+    for (int maxv : cands) {
+        auto r = choose_radices(static_cast<int>(n), maxv);
+        const int tpl = threads_per_line(static_cast<int>(n), r, maxv);
+        if (tpl > max_threads_for(dbl, maxv)) continue;
+        best.ok = true;
+        best.kc.maxv = maxv;
+        best.radices = r;
+        best.tpl = tpl;
+        return best;
+    }
+    return best;
+}
+
+int maxt_for(int threads) {
+    if (threads <= 256) return 256;
+    if (threads <= 512) return 512;
+    return 1024;
+}
+
+struct Builder {
+    PlanSpec& plan;
+    const PlanRequest& req;
+    int cs;
+    int smem_limit;
+    std::map<std::pair<int, int>, int> seq_tables;  // (n, maxv) -> table id
+
+    int add_table(std::vector<std::complex<double>> t) {
+        plan.tables.push_back(std::move(t));
+        return static_cast<int>(plan.tables.size()) - 1;
+    }
+
+    // Stockham stage sequence for length n with the given radices; twiddle table shared per (n, radices).
+    StageSeq make_seq(int n, const std::vector<int>& radices, int maxv, int* table_id) {
+        StageSeq s;
+        if (static_cast<int>(radices.size()) > kMaxStages) throw std::runtime_error("too many FFT stages");
+        s.nstages = static_cast<int>(radices.size());
+        int ns = 1, off = 0;
+        for (int i = 0; i < s.nstages; ++i) {
+            s.radix[i] = radices[i];
+            s.ns[i] = ns;
+            s.tw_off[i] = off;
+            off += ns * (radices[i] - 1);
+            ns *= radices[i];
+        }
+        if (ns != n) throw std::runtime_error("radix product mismatch");
+        auto key = std::make_pair(n, maxv);
+        auto it = seq_tables.find(key);
+        if (it != seq_tables.end()) {
+            *table_id = it->second;
+            return s;
+        }
+        std::vector<std::complex<double>> tw(std::max(off, 1));
+        ns = 1;
+        for (int i = 0; i < s.nstages; ++i) {
+            const int R = radices[i];
+            for (int jm = 0; jm < ns; ++jm) {
+                for (int r = 1; r < R; ++r) {
+                    tw[s.tw_off[i] + jm * (R - 1) + (r - 1)] =
+                        cis_neg(static_cast<int64_t>(r) * jm, static_cast<int64_t>(ns) * R);
+                }
+            }
+            ns *= R;
+        }
+        *table_id = add_table(std::move(tw));
+        seq_tables[key] = *table_id;
+        return s;
+    }
+
+    void add_tw4(PassSpec& ps, int64_t ntot, int sign) {
+        int shift = 0;
+        while ((int64_t(1) << (2 * shift)) < ntot) ++shift;  // 2^shift >= sqrt(ntot)
+        const int64_t B = int64_t(1) << shift;
+        const int64_t nhi = (ntot + B - 1) / B + 1;
+        std::vector<std::complex<double>> hi(nhi), lo(B);
+        for (int64_t q = 0; q < nhi; ++q) hi[q] = cis_neg(q * B, ntot);
+        for (int64_t r = 0; r < B; ++r) lo[r] = cis_neg(r, ntot);
+        ps.tables.tw4_hi = add_table(std::move(hi));
+        ps.tables.tw4_lo = add_table(std::move(lo));
+        ps.p.tw4_shift = shift;
+        ps.p.tw4_sign = sign;
+    }
+
+    // Fill launch geometry for a pass whose FFT length is p.n and mode is set.
+    void geometry(PassSpec& ps, const SingleCfg& cfg, int want_w) {
+        PassParams& p = ps.p;
+        p.tpl = cfg.tpl;
+        ps.kc = cfg.kc;
+        const int max_threads = max_threads_for(req.dbl, cfg.kc.maxv);
+        int w;
+        if (p.mode == kModeK) {
+            p.pad_shift = pad_shift_for(req.dbl);
+            p.pitch = kmode_pitch(p.n, p.pad_shift);
+            w = want_w > 0 ? want_w : std::max(1, 256 / cfg.tpl);
+            w = static_cast<int>(std::min<int64_t>(w, p.n_cols));
+            while (w > 1 && (w * cfg.tpl > max_threads ||
+                             static_cast<int64_t>(w) * p.pitch * cs > smem_limit))
+                --w;
+            ps.smem_bytes = static_cast<int64_t>(w) * p.pitch * cs;
+        } else {
+            w = want_w > 0 ? want_w : (req.dbl ? 8 : 16);
+            w = static_cast<int>(std::min<int64_t>(w, p.n_cols));
+            while (w > 1 && (w * cfg.tpl > max_threads ||
+                             static_cast<int64_t>(w) * p.n * cs > smem_limit))
+                --w;
+            ps.smem_bytes = static_cast<int64_t>(w) * p.n * cs;
+        }
+        p.w = std::max(w, 1);
+        ps.threads = round_up(p.w * cfg.tpl, 32);
+        if (ps.threads > max_threads) throw std::runtime_error("FFT pass needs too many threads per CTA");
+        if (ps.smem_bytes > smem_limit) throw std::runtime_error("FFT pass exceeds shared memory");
+        ps.kc.maxt = maxt_for(ps.threads);
+        p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+        p.tiles = p.n_outer * p.col_tiles;
+    }
+
+    bool fits(int64_t n, int mode) {
+        SingleCfg cfg = single_cfg(n, req.dbl, req.force_maxv);
+        if (!cfg.ok) return false;
+        const int64_t bytes = mode == kModeK ? int64_t(kmode_pitch(static_cast<int>(n), pad_shift_for(req.dbl))) * cs
+                                             : n * cs;
+        return bytes <= smem_limit;
+    }
+
+    void set_fft(PassSpec& ps, StageSeq& seq, int* tid, int n, const SingleCfg& cfg) {
+        seq = make_seq(n, cfg.radices, cfg.kc.maxv, tid);
+    }
+
+    // Choose N1 * N2 = n with both factors fitting one CTA; most balanced, N2 >= N1.
+    bool split(int64_t n, int64_t& n1, int64_t& n2) {
+        int64_t best1 = 0;
+        double best_score = 1e300;
+        for (int64_t d = 2; d * d <= n; ++d) {
+            if (n % d) continue;
+            const int64_t a = d, b = n / d;
+            if (!fits(a, kModeC) || !fits(b, kModeK) || !fits(b, kModeC)) continue;
+            const double score = std::fabs(std::log(double(b)) - std::log(double(a)));
+            if (score < best_score) { best_score = score; best1 = a; }
+        }
+        if (!best1) return false;
+        n1 = best1;
+        n2 = n / best1;
+        return true;
+    }
+
+    void axis(int ax, int64_t L, int64_t s, int64_t O, Buf& cur) {
+        const bool bwd = req.direction == 1;
+        const int64_t E = static_cast<int64_t>(plan.elements);
+        if (smooth7(static_cast<uint64_t>(L))) {
+            const int mode = s == 1 ? kModeK : kModeC;
+            if (fits(L, mode)) {
+                PassSpec ps;
+                ps.kind = "single";
+                ps.axis = ax;
+                PassParams& p = ps.p;
+                p.n = static_cast<int>(L);
+                p.mode = mode;
+                if (s == 1) {
+                    p.n_outer = 1; p.n_cols = O;
+                    p.in.cs = L; p.in.ks = 1;
+                } else {
+                    p.n_outer = O; p.n_cols = s;
+                    p.in.hi = L * s; p.in.cs = 1; p.in.ks = s;
+                }
+                p.out = p.in;
+                p.in_len = p.out_len = L;
+                p.conj_in = p.conj_out = bwd;
+                SingleCfg cfg = single_cfg(L, req.dbl, req.force_maxv);
+                set_fft(ps, p.fft1, &ps.tables.tw1, p.n, cfg);
+                geometry(ps, cfg, req.force_w);
+                ps.src = cur;
+                ps.dst = Buf::Output;
+                ps.bytes_moved = 2 * E * cs;
+                plan.passes.push_back(ps);
+                cur = Buf::Output;
+                return;
+            }
+            int64_t n1, n2;
+            if (!split(L, n1, n2)) throw std::runtime_error("FFT length too large for this provider");
+            plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(E));
+            // column pass
+            PassSpec a;
+            a.kind = "fourstep_cols";
+            a.axis = ax;
+            {
+                PassParams& p = a.p;
+                p.n = static_cast<int>(n1);
+                p.mode = kModeC;
+                p.g_k = n2;
+                if (s == 1) {
+                    p.n_outer = O; p.n_cols = n2;
+                    p.in.hi = L; p.in.cs = 1; p.in.ks = n2;
+                    p.sel_mode = kSelCol;
+                } else {
+                    p.n_outer = O * n2; p.n_cols = s;
+                    p.in.hi = L * s; p.in.d = n2; p.in.lo = s; p.in.cs = 1; p.in.ks = n2 * s;
+                    p.sel_mode = kSelOuterLo; p.sel_d = n2;
+                }
+                p.out = p.in;
+                p.in_len = p.out_len = L;
+                p.conj_in = bwd;
+                SingleCfg cfg = single_cfg(n1, req.dbl, req.force_maxv);
+                set_fft(a, p.fft1, &a.tables.tw1, p.n, cfg);
+                add_tw4(a, L, -1);
+                geometry(a, cfg, 0);
+                a.src = cur;
+                a.dst = Buf::Scratch;
+                a.bytes_moved = 2 * E * cs;
+            }
+            plan.passes.push_back(a);
+            PassSpec b;
+            b.kind = "fourstep_rows";
+            b.axis = ax;
+            {
+                PassParams& p = b.p;
+                p.n = static_cast<int>(n2);
+                if (s == 1) {
+                    p.mode = kModeK;
+                    p.n_outer = O; p.n_cols = n1;
+                    p.in.hi = L; p.in.cs = n2; p.in.ks = 1;
+                    p.out.hi = L; p.out.cs = 1; p.out.ks = n1;
+                    p.store_via_smem = 1;
+                } else {
+                    p.mode = kModeC;
+                    p.n_outer = O * n1; p.n_cols = s;
+                    p.in.hi = L * s; p.in.d = n1; p.in.lo = n2 * s; p.in.cs = 1; p.in.ks = s;
+                    p.out.hi = L * s; p.out.d = n1; p.out.lo = s; p.out.cs = 1; p.out.ks = n1 * s;
+                }
+                p.in_len = p.out_len = kNoLimit;
+                p.conj_out = bwd;
+                SingleCfg cfg = single_cfg(n2, req.dbl, req.force_maxv);
+                set_fft(b, p.fft1, &b.tables.tw1, p.n, cfg);
+                // rows per CTA: enough for 128-byte segments of the transposed store
+                geometry(b, cfg, s == 1 ? std::max(1, 128 / cs) : 0);
+                b.src = Buf::Scratch;
+                b.dst = Buf::Output;
+                b.bytes_moved = 2 * E * cs;
+            }
+            plan.passes.push_back(b);
+            cur = Buf::Output;
+            return;
+        }
+
+        // Bluestein: y_k = c_k * sum_n (x_n c_n) h_{k-n}, c_n = exp(-i*sgn*pi*n^2/L) conj-chirp,
+        // h_n = conj(c_n) (exact n^2 mod 2L reduction), convolution of length M via FFT.
+        const int64_t M = static_cast<int64_t>(bluestein_length(static_cast<uint64_t>(L)));
+        const int sgn = req.direction;  // -1 forward, +1 backward
+        std::vector<std::complex<double>> chirp(L), kern(M, 0.0);
+        for (int64_t n = 0; n < L; ++n) {
+            const uint64_t r = (static_cast<unsigned __int128>(n) * n) % static_cast<uint64_t>(2 * L);
+            // h_n = exp(-i*sgn*pi*r/L) = exp(-2 pi i * (sgn*r) / (2L))
+            const std::complex<double> h = cis_neg(sgn * static_cast<int64_t>(r), 2 * L);
+            kern[n] = h;
+            if (n) kern[M - n] = h;
+            chirp[n] = std::conj(h);
+        }
+        host_fft_fp64(kern, -1);
+        for (auto& v : kern) v /= static_cast<double>(M);
+        const int chirp_id = add_table(std::move(chirp));
+        const int mode = s == 1 ? kModeK : kModeC;
+        if (fits(M, mode)) {
+            PassSpec ps;
+            ps.kind = "bluestein_fused";
+            ps.axis = ax;
+            PassParams& p = ps.p;
+            p.n = static_cast<int>(M);
+            p.mode = mode;
+            if (s == 1) {
+                p.n_outer = 1; p.n_cols = O;
+                p.in.cs = L; p.in.ks = 1;
+            } else {
+                p.n_outer = O; p.n_cols = s;
+                p.in.hi = L * s; p.in.cs = 1; p.in.ks = s;
+            }
+            p.out = p.in;
+            p.in_len = p.out_len = L;
+            ps.tables.premul = chirp_id;
+            ps.tables.postmul = chirp_id;
+            ps.tables.pointwise = add_table(std::move(kern));
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            SingleCfg cfg = single_cfg(M, req.dbl, req.force_maxv);
+            set_fft(ps, p.fft1, &ps.tables.tw1, p.n, cfg);
+            set_fft(ps, p.fft2, &ps.tables.tw2, p.n, cfg);
+            geometry(ps, cfg, req.force_w);
+            ps.src = cur;
+            ps.dst = Buf::Output;
+            ps.bytes_moved = 2 * E * cs;
+            plan.passes.push_back(ps);
+            cur = Buf::Output;
+            return;
+        }
+        int64_t n1, n2;
+        if (!split(M, n1, n2)) throw std::runtime_error("Bluestein length too large for this provider");
+        // K'[k1*N2 + k2] = K[k1 + N1*k2]
+        std::vector<std::complex<double>> kp(M);
+        for (int64_t k1 = 0; k1 < n1; ++k1)
+            for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = kern[k1 + n1 * k2];
+        const int kp_id = add_table(std::move(kp));
+        const int64_t lines = E / L;
+        plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(lines * M));
+        // pass 1: columns of the zero-padded, chirp-multiplied line
+        PassSpec a;
+        a.kind = "bluestein_cols_fwd";
+        a.axis = ax;
+        {
+            PassParams& p = a.p;
+            p.n = static_cast<int>(n1);
+            p.mode = kModeC;
+            p.g_k = n2;
+            if (s == 1) {
+                p.n_outer = O; p.n_cols = n2;
+                p.in.hi = L; p.in.cs = 1; p.in.ks = n2;
+                p.out.hi = M; p.out.cs = 1; p.out.ks = n2;
+                p.sel_mode = kSelCol;
+            } else {
+                p.n_outer = O * n2; p.n_cols = s;
+                p.in.hi = L * s; p.in.d = n2; p.in.lo = s; p.in.cs = 1; p.in.ks = n2 * s;
+                p.out.hi = M * s; p.out.d = n2; p.out.lo = s; p.out.cs = 1; p.out.ks = n2 * s;
+                p.sel_mode = kSelOuterLo; p.sel_d = n2;
+            }
+            p.in_len = L;
+            p.out_len = kNoLimit;
+            a.tables.premul = chirp_id;
+            SingleCfg cfg = single_cfg(n1, req.dbl, req.force_maxv);
+            set_fft(a, p.fft1, &a.tables.tw1, p.n, cfg);
+            add_tw4(a, M, -1);
+            geometry(a, cfg, 0);
+            a.src = cur;
+            a.dst = Buf::Scratch;
+            a.bytes_moved = (E + lines * M) * cs;
+        }
+        plan.passes.push_back(a);
+        // pass 2: rows: FFT, spectrum multiply, inverse FFT, inverse twiddle
+        PassSpec b;
+        b.kind = "bluestein_rows_conv";
+        b.axis = ax;
+        {
+            PassParams& p = b.p;
+            p.n = static_cast<int>(n2);
+            if (s == 1) {
+                p.mode = kModeK;
+                p.n_outer = O; p.n_cols = n1;
+                p.in.hi = M; p.in.cs = n2; p.in.ks = 1;
+                p.sel_mode = kSelCol;
+            } else {
+                p.mode = kModeC;
+                p.n_outer = O * n1; p.n_cols = s;
+                p.in.hi = M * s; p.in.d = n1; p.in.lo = n2 * s; p.in.cs = 1; p.in.ks = s;
+                p.sel_mode = kSelOuterLo; p.sel_d = n1;
+            }
+            p.out = p.in;
+            p.in_len = p.out_len = kNoLimit;
+            b.tables.pointwise = kp_id;
+            p.pw_stride = n2;
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            SingleCfg cfg = single_cfg(n2, req.dbl, req.force_maxv);
+            set_fft(b, p.fft1, &b.tables.tw1, p.n, cfg);
+            set_fft(b, p.fft2, &b.tables.tw2, p.n, cfg);
+            add_tw4(b, M, +1);
+            geometry(b, cfg, 0);
+            b.src = Buf::Scratch;
+            b.dst = Buf::Scratch;
+            b.bytes_moved = 2 * lines * M * cs;
+        }
+        plan.passes.push_back(b);
+        // pass 3: columns: inverse FFT, chirp post-multiply, truncation to L
+        PassSpec c;
+        c.kind = "bluestein_cols_inv";
+        c.axis = ax;
+        {
+            PassParams& p = c.p;
+            p.n = static_cast<int>(n1);
+            p.mode = kModeC;
+            p.g_k = n2;
+            if (s == 1) {
+                p.n_outer = O; p.n_cols = n2;
+                p.in.hi = M; p.in.cs = 1; p.in.ks = n2;
+                p.out.hi = L; p.out.cs = 1; p.out.ks = n2;
+                p.sel_mode = kSelCol;
+            } else {
+                p.n_outer = O * n2; p.n_cols = s;
+                p.in.hi = M * s; p.in.d = n2; p.in.lo = s; p.in.cs = 1; p.in.ks = n2 * s;
+                p.out.hi = L * s; p.out.d = n2; p.out.lo = s; p.out.cs = 1; p.out.ks = n2 * s;
+                p.sel_mode = kSelOuterLo; p.sel_d = n2;
+            }
+            p.in_len = kNoLimit;
+            p.out_len = L;
+            p.conj_in = 1;
+            p.conj_out = 1;
+            c.tables.postmul = chirp_id;
+            SingleCfg cfg = single_cfg(n1, req.dbl, req.force_maxv);
+            set_fft(c, p.fft1, &c.tables.tw1, p.n, cfg);
+            geometry(c, cfg, 0);
+            c.src = Buf::Scratch;
+            c.dst = Buf::Output;
+            c.bytes_moved = (lines * M + E) * cs;
+        }
+        plan.passes.push_back(c);
+        cur = Buf::Output;
+    }
+
+    void copy_pass(Buf& cur) {
+        PassSpec ps;
+        ps.kind = "copy";
+        PassParams& p = ps.p;
+        p.n = 1;
+        p.mode = kModeK;
+        p.n_outer = 1;
+        p.n_cols = static_cast<int64_t>(plan.elements);
+        p.in.cs = 1; p.in.ks = 1;
+        p.out = p.in;
+        p.in_len = p.out_len = 1;
+        SingleCfg cfg;
+        cfg.ok = true;
+        cfg.kc.maxv = req.dbl ? 8 : 16;
+        cfg.radices = {1};
+        cfg.tpl = 1;
+        set_fft(ps, p.fft1, &ps.tables.tw1, 1, cfg);
+        geometry(ps, cfg, 256);
+        ps.src = cur;
+        ps.dst = Buf::Output;
+        ps.bytes_moved = 2 * static_cast<int64_t>(plan.elements) * cs;
+        plan.passes.push_back(ps);
+        cur = Buf::Output;
+    }
+};
+
+long double two_pi_l() { return 6.283185307179586476925286766559005768L; }
+
+}  // namespace
+
+uint64_t checked_element_count(const std::vector<uint64_t>& shape, uint64_t batch) {
+    if (shape.empty() || shape.size() > 3) throw std::invalid_argument("FFT rank must be between 1 and 3");
+    if (batch == 0) throw std::invalid_argument("FFT batch count must be non-zero");
+    uint64_t count = batch;
+    for (uint64_t len : shape) {
+        if (len == 0) throw std::invalid_argument("FFT dimensions must be non-zero");
+        if (count > std::numeric_limits<uint64_t>::max() / len)
+            throw std::invalid_argument("FFT element count overflows size_t");
+        count *= len;
+    }
+    return count;
+}
+
+double normalization_scale(int mode, int direction, uint64_t n) {
+    switch (mode) {
+        case 0: return 1.0;
+        case 1: return direction == -1 ? 1.0 / static_cast<double>(n) : 1.0;
+        case 2: return direction == 1 ? 1.0 / static_cast<double>(n) : 1.0;
+        case 3: return 1.0 / std::sqrt(static_cast<double>(n));
+        default: return 1.0;
+    }
+}
+
+bool smooth7(uint64_t n) {
+    Factors f;
+    return factor7(n, f);
+}
+
+uint64_t bluestein_length(uint64_t len) {
+    if (len > (uint64_t(1) << 40)) throw std::invalid_argument("Bluestein convolution size overflows");
+    uint64_t m = 2 * len - 1;
+    while (!smooth7(m)) ++m;
+    return m;
+}
+
+std::vector<int> choose_radices(int n, int maxv) {
+    Factors f;
+    if (!factor7(static_cast<uint64_t>(n), f)) throw std::invalid_argument("length is not 7-smooth");
+    std::vector<int> r;
+    if (maxv >= 16)
+        while (f.e2 >= 4) { r.push_back(16); f.e2 -= 4; }
+    while (f.e2 >= 3) { r.push_back(8); f.e2 -= 3; }
+    if (f.e2 == 2) r.push_back(4);
+    if (f.e2 == 1) r.push_back(2);
+    for (int i = 0; i < f.e3; ++i) r.push_back(3);
+    for (int i = 0; i < f.e5; ++i) r.push_back(5);
+    for (int i = 0; i < f.e7; ++i) r.push_back(7);
+    if (r.empty()) r.push_back(1);
+    return r;
+}
+
+int threads_per_line(int n, const std::vector<int>& radices, int maxv) {
+    int tpl = 1;
+    for (int R : radices) {
+        const int per = std::max(1, maxv / R);
+        const int nr = n / R;
+        tpl = std::max(tpl, (nr + per - 1) / per);
+    }
+    return tpl;
+}
+
+std::complex<double> cis_neg(int64_t num, int64_t den) {
+    int64_t m = num % den;
+    if (m < 0) m += den;
+    const long double a = two_pi_l() * static_cast<long double>(m) / static_cast<long double>(den);
+    return {static_cast<double>(std::cos(a)), static_cast<double>(-std::sin(a))};
+}
+
+void host_fft_fp64(std::vector<std::complex<double>>& a, int sign) {
+    const int64_t n = static_cast<int64_t>(a.size());
+    if (n <= 1) return;
+    Factors f;
+    if (!factor7(static_cast<uint64_t>(n), f)) throw std::invalid_argument("host FFT length is not 7-smooth");
+    std::vector<int> radices;
+    for (int i = 0; i < f.e2; ++i) radices.push_back(2);
+    for (int i = 0; i < f.e3; ++i) radices.push_back(3);
+    for (int i = 0; i < f.e5; ++i) radices.push_back(5);
+    for (int i = 0; i < f.e7; ++i) radices.push_back(7);
+    std::vector<std::complex<double>> y(n);
+    int64_t ns = 1;
+    for (int R : radices) {
+        const int64_t nr = n / R;
+        std::vector<std::complex<double>> dft(R * R);
+        for (int p = 0; p < R; ++p)
+            for (int q = 0; q < R; ++q) {
+                auto w = cis_neg(int64_t(p) * q, R);
+                dft[p * R + q] = sign < 0 ? w : std::conj(w);
+            }
+        std::vector<std::complex<double>> tw(ns * R);
+        for (int64_t jm = 0; jm < ns; ++jm)
+            for (int r = 0; r < R; ++r) {
+                auto w = cis_neg(int64_t(r) * jm, ns * R);
+                tw[jm * R + r] = sign < 0 ? w : std::conj(w);
+            }
+        std::complex<double> v[7], u[7];
+        for (int64_t j = 0; j < nr; ++j) {
+            const int64_t jm = j % ns;
+            for (int r = 0; r < R; ++r) v[r] = a[j + r * nr] * tw[jm * R + r];
+            for (int p = 0; p < R; ++p) {
+                std::complex<double> acc = 0.0;
+                for (int q = 0; q < R; ++q) acc += dft[p * R + q] * v[q];
+                u[p] = acc;
+            }
+            const int64_t base = (j - jm) * R + jm;
+            for (int r = 0; r < R; ++r) y[base + r * ns] = u[r];
+        }
+        a.swap(y);
+        ns *= R;
+    }
+}
+
+PlanSpec make_plan(const PlanRequest& req) {
+    if (req.direction != -1 && req.direction != 1) throw std::invalid_argument("Invalid FFT direction");
+    if (req.normalization < 0 || req.normalization > 3) throw std::invalid_argument("Invalid normalization");
+    PlanSpec plan;
+    plan.req = req;
+    plan.elements = checked_element_count(req.shape, req.batch);
+    plan.transform_size = 1;
+    for (auto v : req.shape) plan.transform_size *= v;
+    plan.scale = normalization_scale(req.normalization, req.direction, plan.transform_size);
+    if (plan.elements > (uint64_t(1) << 40)) throw std::invalid_argument("FFT too large for one device");
+    Builder b{plan, req, req.dbl ? 16 : 8, req.smem_limit > 0 ? req.smem_limit : kSmemDefault, {}};
+    Buf cur = Buf::Input;
+    const int rank = static_cast<int>(req.shape.size());
+    const int64_t E = static_cast<int64_t>(plan.elements);
+    for (int ax = rank - 1; ax >= 0; --ax) {
+        const int64_t L = static_cast<int64_t>(req.shape[ax]);
+        if (L == 1) continue;
+        int64_t s = 1;
+        for (int j = ax + 1; j < rank; ++j) s *= static_cast<int64_t>(req.shape[j]);
+        b.axis(ax, L, s, E / (L * s), cur);
+    }
+    if (plan.passes.empty()) b.copy_pass(cur);
+    plan.passes.back().p.scale = plan.scale;
+    return plan;
+}
+
+std::string describe_plan(const PlanSpec& plan) {
+    std::ostringstream os;
+    os << "{\"elements\":" << plan.elements << ",\"scratch_elements\":" << plan.scratch_elements
+       << ",\"scale\":" << plan.scale << ",\"passes\":[";
+    for (size_t i = 0; i < plan.passes.size(); ++i) {
+        const PassSpec& ps = plan.passes[i];
+        const PassParams& p = ps.p;
+        if (i) os << ",";
+        os << "{\"kind\":\"" << ps.kind << "\",\"axis\":" << ps.axis << ",\"n\":" << p.n << ",\"radices\":[";
+        for (int s = 0; s < p.fft1.nstages; ++s) os << (s ? "," : "") << p.fft1.radix[s];
+        os << "],\"two_ffts\":" << (p.fft2.nstages > 0 ? "true" : "false") << ",\"mode\":\""
+           << (p.mode == kModeK ? "k" : "c") << "\",\"tpl\":" << p.tpl << ",\"w\":" << p.w
+           << ",\"threads\":" << ps.threads << ",\"smem\":" << ps.smem_bytes << ",\"tiles\":" << p.tiles
+           << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
+           << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
+           << ",\"store_via_smem\":" << p.store_via_smem << "}";
+    }
+    os << "]}";
+    return os.str();
+}
+
+}  // namespace sfb

@@ -1,0 +1,95 @@
+// Host-side planner of the B200 FFT provider.
+//
+// Turns (shape, batch, precision, direction, normalization) into a list of
+// fused passes (pass_params.h) plus FP64 tables. It has no CUDA dependency:
+// the provider uploads the tables (cast to the plan precision) and binds the
+// device pointers; tests drive the same plans through a CPU emulator.
+//
+// Decomposition rules (per axis of length L, processed last axis first):
+//   * L == 1                         -> no pass (a copy pass if every axis is 1);
+//   * 7-smooth and fits one CTA      -> one pass (Stockham, shared memory);
+//   * 7-smooth and larger            -> four-step: L = N1 * N2, column pass with the
+//                                       W_L^(n2*k1) twiddle fused into its store, then a
+//                                       row pass storing transposed (two passes);
+//   * otherwise (Bluestein)          -> convolution of length M (the smallest 7-smooth
+//                                       M >= 2L-1): one fused pass when M fits a CTA,
+//                                       else three passes over an M-padded scratch.
+// The normalization scale is fused into the store of the last pass.
+#pragma once
+
+#include <complex>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pass_params.h"
+
+namespace sfb {
+
+enum class Buf : int { Input = 0, Output = 1, Scratch = 2 };
+
+struct TableIds {
+    int tw1 = -1, tw2 = -1, premul = -1, pointwise = -1, postmul = -1, tw4_hi = -1, tw4_lo = -1;
+};
+
+struct KernelChoice {
+    int maxv = 16;   // register capacity (complex values per thread per stage)
+    int maxt = 256;  // __launch_bounds__ of the instantiation
+};
+
+struct PassSpec {
+    PassParams p;
+    TableIds tables;
+    Buf src = Buf::Input, dst = Buf::Output;
+    KernelChoice kc;
+    int threads = 0;         // blockDim.x
+    int64_t smem_bytes = 0;  // dynamic shared memory
+    std::string kind;        // "single", "fourstep_cols", "fourstep_rows", "bluestein_fused", ...
+    int axis = 0;
+    int64_t bytes_moved = 0; // HBM bytes this pass reads + writes (data, not tables)
+};
+
+struct PlanRequest {
+    bool dbl = false;
+    int direction = -1;      // -1 forward, +1 backward
+    int normalization = 0;   // 0 none, 1 forward, 2 backward, 3 orthogonal
+    bool in_place = false;
+    std::vector<uint64_t> shape;
+    uint64_t batch = 1;
+    // tuning knobs (0 = heuristic)
+    int force_maxv = 0;
+    int force_w = 0;
+    int smem_limit = 0;      // bytes, 0 = device default (227 KB)
+};
+
+struct PlanSpec {
+    PlanRequest req;
+    uint64_t elements = 0, transform_size = 0;
+    double scale = 1.0;
+    std::vector<std::vector<std::complex<double>>> tables;
+    std::vector<PassSpec> passes;
+    uint64_t scratch_elements = 0;
+};
+
+// Throws std::invalid_argument / std::runtime_error with a message on failure.
+PlanSpec make_plan(const PlanRequest& req);
+
+// Element count with the reference's validation (rank 1..3, non-zero sizes, overflow).
+uint64_t checked_element_count(const std::vector<uint64_t>& shape, uint64_t batch);
+// Normalization scale as the reference computes it (in double).
+double normalization_scale(int mode, int direction, uint64_t transform_size);
+
+// Helpers exposed for tests.
+bool smooth7(uint64_t n);
+uint64_t bluestein_length(uint64_t len);
+std::vector<int> choose_radices(int n, int maxv);
+int threads_per_line(int n, const std::vector<int>& radices, int maxv);
+std::string describe_plan(const PlanSpec& plan);  // JSON
+
+// exp(-2 pi i num / den), with exact argument reduction (num reduced mod den, octant symmetry).
+std::complex<double> cis_neg(int64_t num, int64_t den);
+
+// Reference-quality FP64 FFT on the host (Stockham, same radices as the device).
+void host_fft_fp64(std::vector<std::complex<double>>& a, int sign);
+
+}  // namespace sfb

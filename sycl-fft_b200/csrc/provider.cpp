@@ -1,0 +1,247 @@
+// The B200 FFT provider module: C ABI v1 (include/syclfft_b200_provider.h).
+//
+// Implements the device-provider contract of the reference's cuFFT module
+// (src/providers/cufft/cufft_provider.cpp:184-248: supports / create / destroy /
+// execute with a 1024-byte error buffer and no exceptions across the boundary) on
+// top of the B200 planner and pass kernels. A plan owns its device tables (twiddles,
+// chirps, chirp spectra; generated in FP64, stored in the plan precision) and one
+// scratch buffer; execute enqueues the plan's passes on the caller's stream.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/syclfft_b200_provider.h"
+#include "launch.hpp"
+#include "planner.hpp"
+
+namespace sfb {
+namespace {
+
+void set_error(char* err, size_t cap, const std::string& msg) {
+    // provider_error_buffer.hpp:10-18 semantics: NUL-terminated, truncated to cap-1
+    if (!err || cap == 0) return;
+    const size_t n = std::min(cap - 1, msg.size());
+    std::memcpy(err, msg.data(), n);
+    err[n] = '\0';
+}
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+class DeviceGuard {
+public:
+    explicit DeviceGuard(int device) {
+        check(cudaGetDevice(&prev_), "cudaGetDevice");
+        if (device >= 0 && device != prev_) {
+            check(cudaSetDevice(device), "cudaSetDevice");
+            switched_ = true;
+        }
+    }
+    ~DeviceGuard() {
+        if (switched_) cudaSetDevice(prev_);
+    }
+
+private:
+    int prev_ = 0;
+    bool switched_ = false;
+};
+
+struct BoundPass {
+    PassParams p;
+    PassSpec spec;
+};
+
+struct DevicePlan {
+    PlanSpec spec;
+    int device = 0;
+    void* table_mem = nullptr;
+    void* scratch = nullptr;
+    std::vector<BoundPass> passes;
+    cudaEvent_t done = nullptr;
+    std::mutex mu;
+
+    ~DevicePlan() {
+        int prev = 0;
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != device) cudaSetDevice(device);
+        if (done) {
+            cudaEventSynchronize(done);
+            cudaEventDestroy(done);
+        }
+        if (scratch) cudaFree(scratch);
+        if (table_mem) cudaFree(table_mem);
+        if (prev != device) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned char>& blob, size_t off) {
+    T* dst = reinterpret_cast<T*>(blob.data() + off);
+    for (size_t i = 0; i < t.size(); ++i) {
+        dst[2 * i] = static_cast<T>(t[i].real());
+        dst[2 * i + 1] = static_cast<T>(t[i].imag());
+    }
+}
+
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
+    if (cfg.abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION) throw std::runtime_error("B200 provider ABI mismatch");
+    if (cfg.scalar != SYCLFFT_B200_SCALAR_FLOAT && cfg.scalar != SYCLFFT_B200_SCALAR_DOUBLE)
+        throw std::invalid_argument("unsupported scalar type");
+    if (cfg.rank == 0 || cfg.rank > 3) throw std::invalid_argument("FFT rank must be between 1 and 3");
+    PlanRequest req;
+    req.dbl = cfg.scalar == SYCLFFT_B200_SCALAR_DOUBLE;
+    req.direction = cfg.direction;
+    req.normalization = static_cast<int>(cfg.normalization);
+    req.in_place = cfg.in_place != 0;
+    req.shape.assign(cfg.lengths, cfg.lengths + cfg.rank);
+    req.batch = cfg.batch_count;
+
+    int device = cfg.device;
+    if (device < 0) check(cudaGetDevice(&device), "cudaGetDevice");
+    DeviceGuard guard(device);
+    int smem_optin = 0;
+    check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "cudaDeviceGetAttribute");
+    req.smem_limit = smem_optin;
+
+    auto plan = std::make_unique<DevicePlan>();
+    plan->device = device;
+    plan->spec = make_plan(req);
+    const size_t cs = req.dbl ? 16 : 8;
+
+    // All tables in one allocation, each 256-byte aligned.
+    std::vector<size_t> offsets(plan->spec.tables.size());
+    size_t total = 0;
+    for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
+        offsets[i] = total;
+        total += (plan->spec.tables[i].size() * cs + 255) / 256 * 256;
+    }
+    std::vector<unsigned char> blob(std::max<size_t>(total, 256), 0);
+    for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
+        if (req.dbl) pack_table<double>(plan->spec.tables[i], blob, offsets[i]);
+        else pack_table<float>(plan->spec.tables[i], blob, offsets[i]);
+    }
+    check(cudaMalloc(&plan->table_mem, blob.size()), "cudaMalloc(tables)");
+    check(cudaMemcpy(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
+    if (plan->spec.scratch_elements) {
+        check(cudaMalloc(&plan->scratch, plan->spec.scratch_elements * cs), "cudaMalloc(scratch)");
+    }
+    check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+
+    auto tab = [&](int id) -> const void* {
+        return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
+    };
+    for (const PassSpec& ps : plan->spec.passes) {
+        if (!has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt)) throw std::runtime_error("no kernel variant for pass");
+        BoundPass bp;
+        bp.spec = ps;
+        bp.p = ps.p;
+        bp.p.fft1.tw = tab(ps.tables.tw1);
+        bp.p.fft2.tw = tab(ps.tables.tw2);
+        bp.p.premul = tab(ps.tables.premul);
+        bp.p.pointwise = tab(ps.tables.pointwise);
+        bp.p.postmul = tab(ps.tables.postmul);
+        bp.p.tw4_hi = tab(ps.tables.tw4_hi);
+        bp.p.tw4_lo = tab(ps.tables.tw4_lo);
+        plan->passes.push_back(bp);
+    }
+    return plan.release();
+}
+
+void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream) {
+    if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
+    const bool in_place = plan->spec.req.in_place;
+    if (in_place && in != out) throw std::invalid_argument("In-place plan must be executed with in == out");
+    if (!in_place && in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
+    std::lock_guard<std::mutex> lock(plan->mu);
+    DeviceGuard guard(plan->device);
+    for (const BoundPass& bp : plan->passes) {
+        auto buf = [&](Buf b) -> void* {
+            if (b == Buf::Input) return const_cast<void*>(in);
+            if (b == Buf::Output) return out;
+            return plan->scratch;
+        };
+        check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec.kc.maxv, bp.spec.kc.maxt, bp.spec.threads,
+                          static_cast<size_t>(bp.spec.smem_bytes), buf(bp.spec.src), buf(bp.spec.dst), stream),
+              "FFT pass launch");
+    }
+    check(cudaEventRecord(plan->done, stream), "cudaEventRecord");
+}
+
+int p_supports(int32_t device, char* err, size_t cap) {
+    try {
+        int count = 0;
+        check(cudaGetDeviceCount(&count), "cudaGetDeviceCount");
+        if (device < 0) check(cudaGetDevice(&device), "cudaGetDevice");
+        if (device >= count) throw std::runtime_error("CUDA device ordinal out of range");
+        cudaDeviceProp prop{};
+        check(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+        if (prop.major != 10 || prop.minor != 0)
+            throw std::runtime_error(std::string("B200 provider needs an sm_100 device, found ") + prop.name);
+        return 1;
+    } catch (const std::exception& e) {
+        set_error(err, cap, e.what());
+        return 0;
+    }
+}
+
+void* p_create(const syclfft_b200_plan_config_v1* cfg, char* err, size_t cap) {
+    try {
+        if (!cfg) throw std::invalid_argument("null plan configuration");
+        return create_plan(*cfg);
+    } catch (const std::exception& e) {
+        set_error(err, cap, e.what());
+        return nullptr;
+    }
+}
+
+void p_destroy(void* plan) { delete static_cast<DevicePlan*>(plan); }
+
+int p_execute(void* plan, const void* in, void* out, void* stream, char* err, size_t cap) {
+    try {
+        execute_plan(static_cast<DevicePlan*>(plan), in, out, static_cast<cudaStream_t>(stream));
+        return 0;
+    } catch (const std::exception& e) {
+        set_error(err, cap, e.what());
+        return 1;
+    }
+}
+
+uint64_t p_scratch_bytes(const void* plan) {
+    const auto* p = static_cast<const DevicePlan*>(plan);
+    return p ? p->spec.scratch_elements * (p->spec.req.dbl ? 16u : 8u) : 0;
+}
+
+const syclfft_b200_provider_v1 kProvider{
+    SYCLFFT_B200_PROVIDER_ABI_VERSION, "b200", &p_supports, &p_create, &p_destroy, &p_execute, &p_scratch_bytes,
+};
+
+}  // namespace
+}  // namespace sfb
+
+SYCLFFT_B200_EXPORT const syclfft_b200_provider_v1* syclfft_b200_get_provider_v1(void) { return &sfb::kProvider; }
+
+SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, size_t cap) {
+    const auto* p = static_cast<const sfb::DevicePlan*>(plan);
+    if (!p || !buf || cap == 0) return -1;
+    const std::string s = sfb::describe_plan(p->spec);
+    if (s.size() + 1 > cap) return -1;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return static_cast<int>(s.size());
+}
+
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
+    const auto* p = static_cast<const sfb::DevicePlan*>(plan);
+    return p ? static_cast<int>(p->passes.size()) : -1;
+}
+
+SYCLFFT_B200_EXPORT const char* syclfft_b200_version(void) { return "syclfft-b200 0.1"; }

@@ -1,0 +1,115 @@
+"""ctypes binding of the B200 provider's C ABI (include/syclfft_b200_provider.h).
+
+This is the raw drop-in boundary: plan configs, the provider table and device
+pointers on a CUDA stream. The higher-level mirror of syclfft's plan API lives in
+``syclfft_b200.api``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.dirname(_HERE)
+LIB_DIR = os.path.join(PKG_ROOT, "lib")
+PROVIDER_DIR = os.path.join(LIB_DIR, "syclfft", "providers")
+PROVIDER_PATH = os.path.join(PROVIDER_DIR, "syclfft_provider_b200.so")
+
+ABI_VERSION = 1
+SCALAR_FLOAT = 1
+SCALAR_DOUBLE = 2
+ERR_CAP = 1024
+
+
+class PlanConfigV1(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32),
+        ("scalar", ctypes.c_uint32),
+        ("direction", ctypes.c_int32),
+        ("rank", ctypes.c_uint32),
+        ("lengths", ctypes.c_uint64 * 3),
+        ("batch_count", ctypes.c_uint64),
+        ("in_place", ctypes.c_uint32),
+        ("normalization", ctypes.c_uint32),
+        ("measure", ctypes.c_uint32),
+        ("device", ctypes.c_int32),
+    ]
+
+
+_SUPPORTS = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t)
+_CREATE = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.POINTER(PlanConfigV1), ctypes.c_char_p, ctypes.c_size_t)
+_DESTROY = ctypes.CFUNCTYPE(None, ctypes.c_void_p)
+_EXECUTE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                            ctypes.c_char_p, ctypes.c_size_t)
+_SCRATCH = ctypes.CFUNCTYPE(ctypes.c_uint64, ctypes.c_void_p)
+
+
+class ProviderV1(ctypes.Structure):
+    _fields_ = [
+        ("abi_version", ctypes.c_uint32),
+        ("name", ctypes.c_char_p),
+        ("supports", _SUPPORTS),
+        ("create", _CREATE),
+        ("destroy", _DESTROY),
+        ("execute", _EXECUTE),
+        ("scratch_bytes", _SCRATCH),
+    ]
+
+
+# Every symbol include/syclfft_b200_provider.h declares.
+EXPORTED_SYMBOLS = (
+    "syclfft_b200_get_provider_v1",
+    "syclfft_b200_describe_plan",
+    "syclfft_b200_plan_launches",
+    "syclfft_b200_version",
+)
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """dlopen the provider module (RTLD_LOCAL, like provider_loader.cpp:209) and bind its symbols."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or PROVIDER_PATH
+    if not os.path.exists(p):
+        raise OSError(f"B200 provider module not built: {p}")
+    lib = ctypes.CDLL(p, mode=ctypes.RTLD_LOCAL)
+    lib.syclfft_b200_get_provider_v1.restype = ctypes.POINTER(ProviderV1)
+    lib.syclfft_b200_get_provider_v1.argtypes = []
+    lib.syclfft_b200_describe_plan.restype = ctypes.c_int
+    lib.syclfft_b200_describe_plan.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_plan_launches.restype = ctypes.c_int
+    lib.syclfft_b200_plan_launches.argtypes = [ctypes.c_void_p]
+    lib.syclfft_b200_version.restype = ctypes.c_char_p
+    lib.syclfft_b200_version.argtypes = []
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def provider(lib=None):
+    lib = lib or load()
+    api = lib.syclfft_b200_get_provider_v1()
+    if not api:
+        raise RuntimeError("syclfft_b200_get_provider_v1 returned NULL")
+    return api.contents
+
+
+def make_config(lengths, batch, direction, double=False, in_place=False, normalization=0, measure=False,
+                device=-1) -> PlanConfigV1:
+    lengths = [int(v) for v in lengths]
+    cfg = PlanConfigV1()
+    cfg.abi_version = ABI_VERSION
+    cfg.scalar = SCALAR_DOUBLE if double else SCALAR_FLOAT
+    cfg.direction = int(direction)
+    cfg.rank = len(lengths)
+    for i in range(3):
+        cfg.lengths[i] = lengths[i] if i < len(lengths) else 0
+    cfg.batch_count = int(batch)
+    cfg.in_place = 1 if in_place else 0
+    cfg.normalization = int(normalization)
+    cfg.measure = 1 if measure else 0
+    cfg.device = int(device)
+    return cfg

@@ -1,0 +1,296 @@
+"""Mirror of syclfft's plan API over the B200 provider's C ABI.
+
+Reference surface and semantics followed here:
+  include/syclfft/common.hpp:34-93    enums (values kept), plan_options, error_code
+  include/syclfft/syclfft.hpp:45-130  plan<Scalar>, plan_many_dft / plan_dft_1d/2d/3d
+  src/sycl/sycl.cpp:424-491           plan construction, direction check, provider selection
+  src/sycl/sycl.cpp:615-641           execute: pointer validation, placement rules,
+                                      per-plan serialisation on the previous execution
+  src/sycl/sycl.cpp:818-874           execute overloads, moved-from plan -> invalid_state
+  src/sycl/sycl.cpp:901-907           scratch_size_bytes
+  src/core/provider_loader.cpp:112-132 checked_element_count errors
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import json
+import threading
+from dataclasses import dataclass
+
+from . import _provider
+
+
+class direction(enum.IntEnum):
+    forward = -1
+    backward = 1
+
+
+class placement(enum.IntEnum):
+    in_place = 0
+    out_of_place = 1
+
+
+class normalization(enum.IntEnum):
+    none = 0
+    forward = 1
+    backward = 2
+    orthogonal = 3
+
+
+class planning_mode(enum.IntEnum):
+    estimate = 0
+    measure = 1
+
+
+class provider(enum.IntEnum):
+    automatic = 0
+    portable_sycl = 1
+    fftw = 2
+    cufft = 3
+    rocfft = 4
+    onemkl = 5
+    b200 = 6
+
+
+class error_code(enum.IntEnum):
+    invalid_argument = 0
+    invalid_state = 1
+    invalid_pointer = 2
+    unsupported_precision = 3
+    provider_unavailable = 4
+    planning_failed = 5
+    execution_failed = 6
+    plugin_error = 7
+
+
+class SyclfftError(RuntimeError):
+    """syclfft::exception: a message plus an error_code."""
+
+    def __init__(self, code: error_code, message: str):
+        super().__init__(message)
+        self.code = error_code(code)
+
+
+@dataclass
+class plan_options:
+    placement: placement = placement.out_of_place
+    normalization: normalization = normalization.none
+    planning: planning_mode = planning_mode.estimate
+    preferred_provider: provider = provider.automatic
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _checked_element_count(lengths, batch):
+    if len(lengths) == 0 or len(lengths) > 3:
+        raise SyclfftError(error_code.invalid_argument, "FFT rank must be between 1 and 3")
+    if batch == 0:
+        raise SyclfftError(error_code.invalid_argument, "FFT batch count must be non-zero")
+    count = int(batch)
+    for n in lengths:
+        if n == 0:
+            raise SyclfftError(error_code.invalid_argument, "FFT dimensions must be non-zero")
+        count *= int(n)
+        if count >= 1 << 64:
+            raise SyclfftError(error_code.invalid_argument, "FFT element count overflows size_t")
+    return count
+
+
+class Plan:
+    """syclfft::plan<Scalar> over the B200 provider. `scalar` is "float" or "double"."""
+
+    def __init__(self, scalar: str, lengths, batch_count: int, dir, options: plan_options | None = None,
+                 device: int | None = None):
+        options = options or plan_options()
+        if scalar not in ("float", "double"):
+            raise SyclfftError(error_code.unsupported_precision, "syclfft supports float and double precision")
+        self._lengths = [int(v) for v in lengths]
+        self._batch = int(batch_count)
+        self._elements = _checked_element_count(self._lengths, self._batch)
+        try:
+            self._direction = direction(int(dir))
+        except ValueError:
+            raise SyclfftError(error_code.invalid_argument, "Invalid FFT direction") from None
+        self._options = options
+        self._double = scalar == "double"
+        if options.preferred_provider not in (provider.automatic, provider.b200):
+            raise SyclfftError(error_code.provider_unavailable,
+                               f"{provider(options.preferred_provider).name} provider is not part of this build")
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise SyclfftError(error_code.provider_unavailable, "no CUDA device is available")
+        self._device = torch.cuda.current_device() if device is None else int(device)
+        try:
+            self._lib = _provider.load()
+        except OSError as e:
+            raise SyclfftError(error_code.provider_unavailable, str(e)) from None
+        self._api = _provider.provider(self._lib)
+        if self._api.abi_version != _provider.ABI_VERSION:
+            raise SyclfftError(error_code.plugin_error, "B200 provider ABI mismatch")
+        err = ctypes.create_string_buffer(_provider.ERR_CAP)
+        if not self._api.supports(self._device, err, _provider.ERR_CAP):
+            raise SyclfftError(error_code.provider_unavailable, err.value.decode() or "device not supported")
+        cfg = _provider.make_config(self._lengths, self._batch, int(self._direction), self._double,
+                                    options.placement == placement.in_place, int(options.normalization),
+                                    options.planning == planning_mode.measure, self._device)
+        self._cfg = cfg
+        h = self._api.create(ctypes.byref(cfg), err, _provider.ERR_CAP)
+        if not h:
+            raise SyclfftError(error_code.planning_failed, err.value.decode() or "B200 plan creation failed")
+        self._handle = h
+        self._lock = threading.Lock()
+        self._last_event = None
+
+    # -- properties (syclfft.hpp:62-66) --
+    def shape(self):
+        return list(self._lengths) if self._handle else []
+
+    def batch_count(self):
+        return self._batch if self._handle else 0
+
+    def direction(self):
+        return self._direction if self._handle else direction.forward
+
+    def selected_provider(self):
+        return provider.b200 if self._handle else provider.automatic
+
+    def scratch_size_bytes(self):
+        return int(self._api.scratch_bytes(self._handle)) if self._handle else 0
+
+    @property
+    def elements(self):
+        return self._elements
+
+    @property
+    def dtype(self):
+        return _torch().complex128 if self._double else _torch().complex64
+
+    def describe(self) -> dict:
+        buf = ctypes.create_string_buffer(1 << 16)
+        n = self._lib.syclfft_b200_describe_plan(self._handle, buf, 1 << 16)
+        if n < 0:
+            raise SyclfftError(error_code.invalid_state, "plan description unavailable")
+        return json.loads(buf.value.decode())
+
+    def launches(self) -> int:
+        return int(self._lib.syclfft_b200_plan_launches(self._handle))
+
+    # -- execution (sycl.cpp:615-641, 818-874) --
+    def _pointer(self, t, name):
+        torch = _torch()
+        if t is None:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
+        if isinstance(t, int):
+            if t == 0:
+                raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
+            return t
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} is not a device allocation in the plan context")
+        if t.device.index != self._device:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
+        if t.dtype != self.dtype:
+            raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {self.dtype}")
+        if not t.is_contiguous() or t.numel() < self._elements:
+            raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {self._elements} elements")
+        return t.data_ptr()
+
+    def execute(self, a, b=None, dependencies=None, stream=None):
+        """execute(inout[, deps]) for in-place plans, execute(input, output[, deps]) otherwise."""
+        if not getattr(self, "_handle", None):
+            raise SyclfftError(error_code.invalid_state, "Cannot execute a moved-from plan")
+        one_pointer = b is None
+        inp = self._pointer(a, "input")
+        out = inp if one_pointer else self._pointer(b, "output")
+        pl = self._options.placement
+        if pl == placement.in_place and not one_pointer:
+            raise SyclfftError(error_code.invalid_argument, "In-place plan must be executed with execute(inout)")
+        if pl == placement.out_of_place and one_pointer:
+            raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires input and output arguments")
+        if pl == placement.out_of_place and inp == out:
+            raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires distinct allocations")
+        torch = _torch()
+        s = stream or torch.cuda.current_stream(self._device)
+        with self._lock:
+            for dep in dependencies or ():
+                s.wait_event(dep)
+            if self._last_event is not None:
+                s.wait_event(self._last_event)
+            err = ctypes.create_string_buffer(_provider.ERR_CAP)
+            rc = self._api.execute(self._handle, inp, out, s.cuda_stream, err, _provider.ERR_CAP)
+            if rc != 0 or err.value:
+                raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
+            ev = torch.cuda.Event()
+            ev.record(s)
+            self._last_event = ev
+            return ev
+
+    def close(self):
+        h = getattr(self, "_handle", None)
+        if h:
+            if self._last_event is not None:
+                self._last_event.synchronize()
+            self._api.destroy(h)
+            self._handle = None
+
+    def move(self) -> "Plan":
+        """C++ move: returns a new owner, leaves this plan moved-from (invalid_state on execute)."""
+        other = object.__new__(Plan)
+        other.__dict__.update(self.__dict__)
+        self._handle = None
+        return other
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def plan_many_dft(scalar, lengths, batch_count, dir, options=None, device=None) -> Plan:
+    return Plan(scalar, lengths, batch_count, dir, options, device)
+
+
+def plan_dft_1d(scalar, n, dir, options=None, device=None) -> Plan:
+    return Plan(scalar, [n], 1, dir, options, device)
+
+
+def plan_dft_2d(scalar, n0, n1, dir, options=None, device=None) -> Plan:
+    return Plan(scalar, [n0, n1], 1, dir, options, device)
+
+
+def plan_dft_3d(scalar, n0, n1, n2, dir, options=None, device=None) -> Plan:
+    return Plan(scalar, [n0, n1, n2], 1, dir, options, device)
+
+
+def query_providers(device: int | None = None):
+    """query_providers (sycl.cpp:909-947): status rows for every provider slot."""
+    rows = []
+    reason = ""
+    available = False
+    try:
+        torch = _torch()
+        lib = _provider.load()
+        api = _provider.provider(lib)
+        if api.abi_version != _provider.ABI_VERSION:
+            reason = "B200 provider ABI mismatch"
+        elif not torch.cuda.is_available():
+            reason = "no CUDA device is available"
+        else:
+            err = ctypes.create_string_buffer(_provider.ERR_CAP)
+            dev = torch.cuda.current_device() if device is None else device
+            available = bool(api.supports(dev, err, _provider.ERR_CAP))
+            reason = "" if available else err.value.decode()
+    except OSError as e:
+        reason = str(e)
+    rows.append(dict(id=provider.b200, name="b200", built=True, available=available, reason=reason))
+    for pid, name, why in ((provider.portable_sycl, "portable_sycl", "not part of this build"),
+                           (provider.cufft, "cufft", "not part of this build"),
+                           (provider.fftw, "fftw", "not part of this build"),
+                           (provider.rocfft, "rocfft", "reserved for a future provider"),
+                           (provider.onemkl, "onemkl", "reserved for a future provider")):
+        rows.append(dict(id=pid, name=name, built=False, available=False, reason=why))
+    return rows

@@ -1,0 +1,154 @@
+// CPU emulator of the B200 provider's pass contract -- TEST INFRASTRUCTURE ONLY.
+//
+// Builds a plan with the product planner (sycl-fft_b200/csrc/planner.cpp) and runs
+// every pass on the host in FP64, following the kernel's semantics step by step:
+// per tile line, load with zero-padding/pre-multiply/conjugation, the Stockham stage
+// sequence with the planner's twiddle tables, the point-wise multiply and second
+// FFT, and the store with conjugation, four-step twiddle, post-multiply, scale and
+// truncation. Used by tests/ to check plan decompositions (four-step, Bluestein,
+// strided axes) without a GPU. Never used by the product library.
+#include <complex>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../sycl-fft_b200/csrc/planner.hpp"
+
+using cd = std::complex<double>;
+using namespace sfb;
+
+namespace {
+
+int64_t line_base(const LineLayout& L, int64_t o, int64_t c) {
+    return (L.d == 1 ? o * L.hi : (o / L.d) * L.hi + (o % L.d) * L.lo) + c * L.cs;
+}
+
+void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, int n) {
+    std::vector<cd> y(n);
+    for (int s = 0; s < S.nstages; ++s) {
+        const int R = S.radix[s], Ns = S.ns[s], nr = n / R;
+        for (int j = 0; j < nr; ++j) {
+            const int jm = j % Ns;
+            cd v[16], u[16];
+            for (int r = 0; r < R; ++r) {
+                v[r] = x[j + r * nr];
+                if (r > 0 && Ns > 1) v[r] *= tw[S.tw_off[s] + jm * (R - 1) + (r - 1)];
+            }
+            for (int p = 0; p < R; ++p) {
+                cd acc = 0.0;
+                for (int q = 0; q < R; ++q) acc += v[q] * cis_neg(int64_t(p) * q, R);
+                u[p] = acc;
+            }
+            const int base = (j - jm) * R + jm;
+            for (int r = 0; r < R; ++r) y[base + r * Ns] = u[r];
+        }
+        x.swap(y);
+    }
+}
+
+void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) {
+    const PassParams& p = ps.p;
+    auto table = [&](int id) -> const std::vector<cd>* { return id < 0 ? nullptr : &plan.tables[id]; };
+    const auto* premul = table(ps.tables.premul);
+    const auto* pointwise = table(ps.tables.pointwise);
+    const auto* postmul = table(ps.tables.postmul);
+    const auto* hi = table(ps.tables.tw4_hi);
+    const auto* lo = table(ps.tables.tw4_lo);
+    // Read every tile line first so in-place passes behave like the kernel (a tile is read
+    // before it is written, and tiles are disjoint).
+    struct Line { int64_t o, c; std::vector<cd> v; };
+    std::vector<Line> lines;
+    for (int64_t o = 0; o < p.n_outer; ++o) {
+        for (int64_t c = 0; c < p.n_cols; ++c) {
+            Line L{o, c, std::vector<cd>(p.n)};
+            const int64_t sel = p.sel_mode == kSelCol ? c : (p.sel_mode == kSelOuterLo ? o % p.sel_d : 0);
+            const int64_t ib = line_base(p.in, o, c);
+            for (int k = 0; k < p.n; ++k) {
+                const int64_t g = int64_t(k) * p.g_k + sel;
+                cd a = 0.0;
+                if (g < p.in_len) {
+                    a = src[ib + int64_t(k) * p.in.ks];
+                    if (premul) a *= (*premul)[g];
+                    if (p.conj_in) a = std::conj(a);
+                }
+                L.v[k] = a;
+            }
+            lines.push_back(std::move(L));
+        }
+    }
+    for (auto& L : lines) {
+        const int64_t sel = p.sel_mode == kSelCol ? L.c : (p.sel_mode == kSelOuterLo ? L.o % p.sel_d : 0);
+        stockham(L.v, p.fft1, plan.tables[ps.tables.tw1], p.n);
+        if (p.fft2.nstages > 0) {
+            for (int k = 0; k < p.n; ++k) {
+                if (pointwise) L.v[k] *= (*pointwise)[k + sel * p.pw_stride];
+                if (p.conj_mid) L.v[k] = std::conj(L.v[k]);
+            }
+            stockham(L.v, p.fft2, plan.tables[ps.tables.tw2], p.n);
+        }
+        const int64_t ob = line_base(p.out, L.o, L.c);
+        for (int k = 0; k < p.n; ++k) {
+            const int64_t g = int64_t(k) * p.g_k + sel;
+            if (g >= p.out_len) continue;
+            cd v = L.v[k];
+            if (p.conj_out) v = std::conj(v);
+            if (p.tw4_sign != 0) {
+                const int64_t m = int64_t(k) * sel;
+                cd w = (*hi)[m >> p.tw4_shift] * (*lo)[m & ((int64_t(1) << p.tw4_shift) - 1)];
+                if (p.tw4_sign > 0) w = std::conj(w);
+                v *= w;
+            }
+            if (postmul) v *= (*postmul)[g];
+            v *= p.scale;
+            dst[ob + int64_t(k) * p.out.ks] = v;
+        }
+    }
+}
+
+void set_err(char* err, size_t cap, const std::string& m) {
+    if (!err || !cap) return;
+    size_t n = std::min(cap - 1, m.size());
+    std::memcpy(err, m.data(), n);
+    err[n] = 0;
+}
+
+}  // namespace
+
+extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
+                       uint64_t batch, int force_maxv, int smem_limit, const double* in, double* out,
+                       char* desc, size_t desc_cap, char* err, size_t cap) {
+    try {
+        PlanRequest req;
+        req.dbl = dbl != 0;
+        req.direction = dir;
+        req.normalization = norm;
+        req.in_place = in_place != 0;
+        req.shape.assign(shape, shape + rank);
+        req.batch = batch;
+        req.force_maxv = force_maxv;
+        req.smem_limit = smem_limit;
+        PlanSpec plan = make_plan(req);
+        set_err(desc, desc_cap, describe_plan(plan));
+        const int64_t E = static_cast<int64_t>(plan.elements);
+        std::vector<cd> input(E), output(E), scratch(plan.scratch_elements);
+        for (int64_t i = 0; i < E; ++i) input[i] = cd(in[2 * i], in[2 * i + 1]);
+        if (req.in_place) output = input;
+        for (const auto& ps : plan.passes) {
+            auto buf = [&](Buf b) -> cd* {
+                if (b == Buf::Input) return req.in_place ? output.data() : input.data();
+                if (b == Buf::Output) return output.data();
+                return scratch.data();
+            };
+            run_pass(plan, ps, buf(ps.src), buf(ps.dst));
+        }
+        for (int64_t i = 0; i < E; ++i) {
+            out[2 * i] = output[i].real();
+            out[2 * i + 1] = output[i].imag();
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, cap, e.what());
+        return 1;
+    }
+}

@@ -1,0 +1,97 @@
+"""Plan API semantics on the GPU: the reference's error-code cases
+(tests/sycl_tests.cpp:508-538, host_tests.cpp:167-195), provider selection and
+query_providers (sycl.cpp:447-475, 909-947), scratch size and the raw C ABI."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+@pytest.fixture(scope="module")
+def sf():
+    import syclfft_b200
+    return syclfft_b200
+
+
+def expect(sf, code, fn):
+    with pytest.raises(sf.SyclfftError) as ei:
+        fn()
+    assert ei.value.code == code, str(ei.value)
+
+
+def test_error_codes(sf, torch):
+    E = sf.error_code
+    fwd = sf.direction.forward
+    expect(sf, E.invalid_argument, lambda: sf.plan_dft_1d("float", 8, 0))
+    expect(sf, E.invalid_argument, lambda: sf.plan_dft_1d("float", 0, fwd))
+    expect(sf, E.invalid_argument, lambda: sf.plan_many_dft("float", [2, 2, 2, 2], 1, fwd))
+    expect(sf, E.invalid_argument, lambda: sf.plan_many_dft("float", [8], 0, fwd))
+    expect(sf, E.invalid_argument, lambda: sf.plan_many_dft("float", [2 ** 63, 4], 1, fwd))
+    expect(sf, E.provider_unavailable, lambda: sf.plan_dft_1d(
+        "float", 8, fwd, sf.plan_options(preferred_provider=sf.provider.cufft)))
+    expect(sf, E.provider_unavailable, lambda: sf.plan_dft_1d(
+        "float", 8, fwd, sf.plan_options(preferred_provider=sf.provider.portable_sycl)))
+    p = sf.plan_dft_1d("float", 8, fwd)
+    expect(sf, E.invalid_pointer, lambda: p.execute(None, None))
+    expect(sf, E.invalid_pointer, lambda: p.execute(torch.zeros(8, dtype=torch.complex64), torch.zeros(8, dtype=torch.complex64)))
+    x = torch.zeros(8, dtype=torch.complex64, device="cuda")
+    expect(sf, E.invalid_argument, lambda: p.execute(x))
+    expect(sf, E.invalid_argument, lambda: p.execute(x, x))
+    expect(sf, E.invalid_argument, lambda: p.execute(x.to(torch.complex128), torch.zeros_like(x)))
+    ip = sf.plan_dft_1d("float", 8, fwd, sf.plan_options(placement=sf.placement.in_place))
+    expect(sf, E.invalid_argument, lambda: ip.execute(x, torch.zeros_like(x)))
+    moved = ip.move()
+    expect(sf, E.invalid_state, lambda: ip.execute(x))
+    moved.execute(x).synchronize()
+    assert ip.shape() == [] and moved.shape() == [8]
+
+
+def test_provider_selection_and_query(sf, torch):
+    p = sf.plan_dft_1d("float", 8, sf.direction.forward)
+    assert p.selected_provider() == sf.provider.b200
+    rows = sf.query_providers()
+    b200 = [r for r in rows if r["name"] == "b200"][0]
+    assert b200["built"] and b200["available"], b200["reason"]
+    assert all(r["reason"] for r in rows if not r["available"])
+
+
+def test_scratch_size(sf, torch):
+    assert sf.plan_many_dft("float", [4096], 16, sf.direction.forward).scratch_size_bytes() == 0
+    assert sf.plan_many_dft("double", [65536], 4, sf.direction.forward).scratch_size_bytes() >= 65536 * 4 * 16
+    assert sf.plan_many_dft("float", [65537], 2, sf.direction.forward).scratch_size_bytes() >= 2 * 131073 * 8
+
+
+def test_raw_c_abi(sf, torch):
+    from syclfft_b200 import _provider
+    api = _provider.provider()
+    err = ctypes.create_string_buffer(1024)
+    assert api.supports(torch.cuda.current_device(), err, 1024) == 1
+    cfg = _provider.make_config([1024], 4, -1, double=False, normalization=3)
+    h = api.create(ctypes.byref(cfg), err, 1024)
+    assert h, err.value
+    x = torch.randn(4096, dtype=torch.complex64, device="cuda")
+    y = torch.empty_like(x)
+    s = torch.cuda.current_stream()
+    assert api.execute(h, x.data_ptr(), y.data_ptr(), s.cuda_stream, err, 1024) == 0, err.value
+    torch.cuda.synchronize()
+    ref = np.fft.fft(x.cpu().numpy().reshape(4, 1024).astype(np.complex128), axis=1, norm="ortho")
+    assert np.abs(y.cpu().numpy().reshape(4, 1024) - ref).max() < 1e-4
+    # in-place plan given distinct pointers -> error status, no exception across the ABI
+    assert api.execute(h, x.data_ptr(), x.data_ptr(), s.cuda_stream, err, 1024) != 0
+    assert b"distinct" in err.value
+    api.destroy(h)
+    bad = _provider.make_config([16], 1, -1)
+    bad.abi_version = 2
+    assert not api.create(ctypes.byref(bad), err, 1024) and b"ABI" in err.value
+    bad = _provider.make_config([16], 1, 0)
+    assert not api.create(ctypes.byref(bad), err, 1024) and b"direction" in err.value

@@ -1,0 +1,65 @@
+"""Host-side checks of the provider's building blocks, no GPU needed:
+register butterflies vs a direct DFT, and every plan decomposition (single pass,
+four-step, fused and three-pass Bluestein, strided axes, copy) run through the FP64
+pass emulator against numpy's FP64 FFT."""
+import numpy as np
+import pytest
+
+from conftest import fp64_fft, gaussian_complex, norm_scale, rel_l2
+from native_libs import butterfly, emulate
+
+
+@pytest.mark.parametrize("radix", [1, 2, 3, 4, 5, 7, 8, 16])
+def test_butterflies_fp64(radix):
+    x = gaussian_complex(radix, radix, np.complex128)
+    assert np.max(np.abs(butterfly(radix, x) - np.fft.fft(x))) < 1e-14 * max(1, radix)
+
+
+@pytest.mark.parametrize("radix", [2, 3, 4, 5, 7, 8, 16])
+def test_butterflies_fp32(radix):
+    x = gaussian_complex(radix, radix + 100, np.complex128)
+    assert np.max(np.abs(butterfly(radix, x, double=False) - np.fft.fft(x))) < 2e-6 * radix
+
+
+SHAPES = [
+    ([8], 2), ([1024], 3), ([4096], 2), ([13440], 1), ([16384], 1), ([11], 3), ([1009], 2), ([4099], 1),
+    ([16, 12, 10], 2), ([11, 3], 1), ([3, 4], 2), ([2, 3, 5], 1), ([1], 5), ([1, 1], 2), ([32768], 2),
+    ([65536], 1), ([65537], 1), ([30000], 2), ([64, 2048], 1), ([3, 40000], 1), ([40000, 3], 1),
+    ([65537, 2], 1), ([257, 5], 2), ([7, 1, 9], 3), ([2048, 2048 // 64], 1),
+]
+
+
+@pytest.mark.parametrize("double", [False, True])
+@pytest.mark.parametrize("shape,batch", SHAPES, ids=lambda v: str(v))
+def test_plan_decompositions_emulated(shape, batch, double):
+    n = int(np.prod(shape))
+    x = gaussian_complex(n * batch, n + batch, np.complex128)
+    for d, norm in ((-1, 3), (1, 2)):
+        y, desc = emulate(x, shape, batch, d, norm, double)
+        ref = fp64_fft(x, shape, batch, d, norm_scale(norm, d, n))
+        assert rel_l2(y, ref) < 1e-13, desc
+
+
+def test_plan_kinds():
+    _, d = emulate(np.zeros(4096 * 2), [4096], 2, -1)
+    assert [p["kind"] for p in d["passes"]] == ["single"]
+    _, d = emulate(np.zeros(65536), [65536], 1, -1, double=True)
+    assert [p["kind"] for p in d["passes"]] == ["fourstep_cols", "fourstep_rows"]
+    _, d = emulate(np.zeros(1009), [1009], 1, -1)
+    assert [p["kind"] for p in d["passes"]] == ["bluestein_fused"]
+    _, d = emulate(np.zeros(65537), [65537], 1, -1)
+    assert [p["kind"] for p in d["passes"]] == ["bluestein_cols_fwd", "bluestein_rows_conv", "bluestein_cols_inv"]
+    assert d["scratch_elements"] >= 2 * 65537 - 1
+
+
+def test_in_place_emulated():
+    x = gaussian_complex(3 * 40000, 5, np.complex128)
+    y, _ = emulate(x, [40000], 3, -1, 0, False, in_place=True)
+    assert rel_l2(y, fp64_fft(x, [40000], 3, -1)) < 1e-13
+
+
+def test_small_smem_limit_forces_fourstep():
+    x = gaussian_complex(4096, 9, np.complex128)
+    y, d = emulate(x, [4096], 1, -1, smem_limit=16 * 1024)
+    assert d["passes"][0]["kind"] == "fourstep_cols"
+    assert rel_l2(y, fp64_fft(x, [4096], 1, -1)) < 1e-13

@@ -252,7 +252,9 @@ def run_ours(args):
 
     opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal)
     plans, bufs, hosts = [], [], []
-    for label, lengths, batch, dbl in WORKLOAD:
+    workload = [w for w in WORKLOAD if not args.only or w[0] == args.only]
+    workload = [(l, s, max(1, b // args.batch_div), d) for l, s, b, d in workload]
+    for label, lengths, batch, dbl in workload:
         n = math.prod(lengths)
         g = torch.Generator(device=dev).manual_seed(1000 * rank + n)
         fdt = torch.float64 if dbl else torch.float32
@@ -302,7 +304,7 @@ def run_ours(args):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     elapsed_ms = float(t.item())
-    total_flops = step_flops() * args.steps * world
+    total_flops = step_flops(workload) * args.steps * world
     value = total_flops / (elapsed_ms / 1e3) / 1e9
 
     # per-plan execute times inside the timed region
@@ -314,8 +316,9 @@ def run_ours(args):
         per_plan[label] = {"fwd_ms": statistics.mean(fw), "bwd_ms": statistics.mean(bw),
                            "launches_per_execute": f.launches(),
                            "gbs_alg": nbytes / (statistics.mean(fw + bw) / 1e3) / 1e9}
-    dom = per_plan[DOMINANT]
-    dom_plan = [p for p in plans if p[0] == DOMINANT][0]
+    dom_label = DOMINANT if DOMINANT in per_plan else plans[0][0]
+    dom = per_plan[dom_label]
+    dom_plan = [p for p in plans if p[0] == dom_label][0]
     dom_bytes = 2 * math.prod(dom_plan[1]) * dom_plan[2] * (16 if dom_plan[3] else 8)
     dom_ms = (dom["fwd_ms"] + dom["bwd_ms"]) / 2 / dom["launches_per_execute"]
     peak, peak_kind = measured_peaks()
@@ -323,7 +326,7 @@ def run_ours(args):
     traffic = dram_traffic_record()
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "kernel": f"fft_pass_kernel<float,16,256,plain> ({DOMINANT}, radix 16^3, 1 launch per execute)",
+                "kernel": f"fft_pass_kernel ({dom_label}, {dom['launches_per_execute']} launch(es) per execute)",
                 "alg_bytes_per_launch": dom_bytes,
                 "traffic": traffic.get("bytes_per_launch") if traffic else None}
 
@@ -357,22 +360,23 @@ def run_ours(args):
         if world > 1:
             dist.all_reduce(t2, op=dist.ReduceOp.MAX)
         e2e_ms = float(t2.item())
-        e2e = {"value": step_flops() * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
+        e2e = {"value": step_flops(workload) * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": args.e2e_steps,
                "ms_per_step": e2e_ms / args.e2e_steps}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not args.only and args.batch_div == 1:
         cpu = cpu_baseline()
 
     if rank == 0:
-        alg_bytes_step = sum(2 * 2 * math.prod(l) * b * (16 if d else 8) for _, l, b, d in WORKLOAD)
+        alg_bytes_step = sum(2 * 2 * math.prod(l) * b * (16 if d else 8) for _, l, b, d in workload)
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (complex64, complex128)",
             "data": "synthetic (seeded uniform[-1,1) complex)",
-            "config": {"workload": "config2_batched_c2c", "plans": [w[0] for w in WORKLOAD],
+            "config": {"workload": "config2_batched_c2c" if len(workload) == len(WORKLOAD) and args.batch_div == 1
+                       else "subset", "plans": [f"{w[0]} (batch {w[2]})" for w in workload],
                        "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
                        "parallelism": f"replicas x{world} (independent batches per GPU)",
                        "l2": "inputs larger than L2 (no flush)"},
@@ -400,6 +404,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--only", default="", help="run one plan of the workload (profiling)")
+    ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

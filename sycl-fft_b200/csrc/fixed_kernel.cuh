@@ -1,0 +1,197 @@
+// Size-specialised pass kernels: the same Stockham register/shared-memory scheme as
+// pass_kernel.cuh, with the FFT length, radix sequence, threads per line and the
+// shared-memory layout fixed at compile time. Every stage's strides, twiddle-table
+// offsets and shared-memory offsets then fold into immediates, so a thread's work is
+// loads, butterflies and stores with almost no index arithmetic.
+//
+// Only plain passes use them: a whole line per CTA row (no zero padding, tables or
+// four-step twiddle), conjugation for inverse transforms and the normalization scale
+// fused into the store.
+//   kModeK: lines are contiguous (line pitch `in_pitch`), threads walk elements;
+//   kModeC: lines are strided columns (element stride `in_ks`, columns contiguous),
+//           threads walk W adjacent columns so every access is a W-wide segment.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "butterfly.cuh"
+
+namespace sfb {
+
+struct FixedParams {
+    int64_t n_cols = 1;     // lines (kModeK) or columns per outer index (kModeC)
+    int64_t col_tiles = 1;  // ceil(n_cols / w)
+    int w = 1;              // lines per CTA (kModeK; kModeC uses the compile-time W)
+    int64_t in_hi = 0, out_hi = 0;      // outer stride (kModeC)
+    int64_t in_pitch = 0, out_pitch = 0;  // line pitch (kModeK)
+    int64_t in_ks = 1, out_ks = 1;      // element stride (kModeC)
+    const void* tw = nullptr;           // concatenated per-stage twiddles [ns][R-1]
+    int conj_in = 0, conj_out = 0;
+    double scale = 1.0;
+};
+
+template <class T>
+struct FixedCtx {
+    using C = cplx<T>;
+    C* sm;           // this thread's line (kModeK) or column (kModeC) in shared memory
+    const C* gin;    // this thread's line / column in the input
+    C* gout;
+    const C* twb;    // twiddle table base
+    int t;
+    bool active;
+    bool line_ok;
+    int64_t in_ks, out_ks;
+    T scale;
+    bool conj_in, conj_out;
+};
+
+template <class T> __host__ __device__ constexpr int pad_shift_c() { return sizeof(T) == 4 ? 4 : 3; }
+template <class T, int N> __host__ __device__ constexpr int kpitch() {
+    constexpr int p = N + (N >> pad_shift_c<T>());
+    return (p & 1) ? p : p + 1;
+}
+
+template <class T>
+__device__ __forceinline__ int pidx(int k) {
+    return k + (k >> pad_shift_c<T>());
+}
+
+template <class T, int N, int TPL, bool MODEC, int W, int NS, int TWOFF, int R, bool FIRST, bool LAST>
+__device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
+    using C = cplx<T>;
+    constexpr int PS = pad_shift_c<T>();
+    constexpr int PAD = 1 << PS;
+    constexpr int NR = N / R;
+    constexpr int NB = (NR + TPL - 1) / TPL;
+    constexpr bool EXACT = (NR % TPL) == 0;
+    C v[NB * R];
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const int j = X.t + i * TPL;
+        if (X.active && (EXACT || j < NR)) {
+            if constexpr (FIRST) {
+                if (X.line_ok) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        C a = MODEC ? X.gin[(int64_t)(j + r * NR) * X.in_ks] : X.gin[j + r * NR];
+                        if (X.conj_in) a.y = -a.y;
+                        v[i * R + r] = a;
+                    }
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) v[i * R + r] = cmake<C>(T(0), T(0));
+                }
+            } else if constexpr (MODEC) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[i * R + r] = X.sm[(j + r * NR) * W];
+            } else if constexpr (NR % PAD == 0) {
+                const C* p = X.sm + pidx<T>(j);
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[i * R + r] = p[r * (NR + NR / PAD)];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[i * R + r] = X.sm[pidx<T>(j + r * NR)];
+            }
+        }
+    }
+    if constexpr (!FIRST) __syncthreads();
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const int j = X.t + i * TPL;
+        if (X.active && (EXACT || j < NR)) {
+            C* u = &v[i * R];
+            const int jm = j % NS;
+            if constexpr (NS > 1 && R > 1) {
+                const C* twp = X.twb + TWOFF + jm * (R - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], __ldg(twp + (r - 1)));
+            }
+            dft<R, T>(u);
+            if constexpr (LAST) {
+                // last stage: base == j, outputs at j + r * NR
+                if (X.line_ok) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        C a = u[r];
+                        if (X.conj_out) a.y = -a.y;
+                        a.x *= X.scale;
+                        a.y *= X.scale;
+                        if constexpr (MODEC) X.gout[(int64_t)(j + r * NR) * X.out_ks] = a;
+                        else X.gout[j + r * NR] = a;
+                    }
+                }
+            } else {
+                const int base = (j - jm) * R + jm;
+                if constexpr (MODEC) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) X.sm[(base + r * NS) * W] = u[r];
+                } else if constexpr (NS % PAD == 0 || (R * NS <= PAD && PAD % (R * NS) == 0)) {
+                    C* p = X.sm + pidx<T>(base);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) p[r * NS + (r * NS) / PAD] = u[r];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) X.sm[pidx<T>(base + r * NS)] = u[r];
+                }
+            }
+        }
+    }
+    if constexpr (!LAST) __syncthreads();
+}
+
+template <class T, int N, int TPL, bool MODEC, int W, int NS, int TWOFF, bool FIRST, int R, int... Rest>
+__device__ __forceinline__ void fixed_stages(FixedCtx<T>& X) {
+    constexpr bool LAST = sizeof...(Rest) == 0;
+    fixed_stage<T, N, TPL, MODEC, W, NS, TWOFF, R, FIRST, LAST>(X);
+    if constexpr (!LAST) fixed_stages<T, N, TPL, MODEC, W, NS * R, TWOFF + NS * (R - 1), false, Rest...>(X);
+}
+
+// Register budget: 64 per thread (16 float or 8 double complex values per stage).
+template <class T, int MAXT, int REGS>
+__host__ __device__ constexpr int fixed_min_blocks() {
+    return 65536 / (MAXT * REGS) > 0 ? 65536 / (MAXT * REGS) : 1;
+}
+
+// kModeK: grid = ceil(lines / w), block = w * TPL (<= MAXT), dynamic smem = w * kpitch<T,N>() * sizeof(C).
+// kModeC: grid = n_outer * col_tiles, block = W * TPL, dynamic smem = N * W * sizeof(C).
+template <class T, int N, int TPL, bool MODEC, int W, int MAXT, int REGS, int... Rs>
+__global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
+    fft_fixed_kernel(const __grid_constant__ FixedParams P, const cplx<T>* in, cplx<T>* out) {
+    using C = cplx<T>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    FixedCtx<T> X;
+    X.twb = static_cast<const C*>(P.tw);
+    X.scale = static_cast<T>(P.scale);
+    X.conj_in = P.conj_in != 0;
+    X.conj_out = P.conj_out != 0;
+    const int tid = threadIdx.x;
+    if constexpr (MODEC) {
+        const int w = tid % W;
+        X.t = tid / W;
+        X.active = X.t < TPL;
+        const int64_t tile = blockIdx.x;
+        const int64_t o = tile / P.col_tiles;
+        const int64_t c = (tile - o * P.col_tiles) * W + w;
+        X.line_ok = X.active && c < P.n_cols;
+        X.sm = sm + w;
+        X.gin = in + o * P.in_hi + c;
+        X.gout = out + o * P.out_hi + c;
+        X.in_ks = P.in_ks;
+        X.out_ks = P.out_ks;
+    } else {
+        const int w = tid / TPL;
+        X.t = tid - w * TPL;
+        X.active = w < P.w;
+        const int64_t c = (int64_t)blockIdx.x * P.w + w;
+        X.line_ok = X.active && c < P.n_cols;
+        X.sm = sm + w * kpitch<T, N>();
+        X.gin = in + c * P.in_pitch;
+        X.gout = out + c * P.out_pitch;
+        X.in_ks = 1;
+        X.out_ks = 1;
+    }
+    fixed_stages<T, N, TPL, MODEC, W, 1, 0, true, Rs...>(X);
+}
+
+}  // namespace sfb

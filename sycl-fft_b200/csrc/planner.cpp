@@ -1,5 +1,7 @@
 #include "planner.hpp"
 
+#include "fixed_catalog.h"
+
 #include <algorithm>
 #include <cmath>
 #include <limits>
@@ -172,6 +174,38 @@ struct Builder {
         p.tiles = p.n_outer * p.col_tiles;
     }
 
+    // Switch a plain single pass to its size-specialised kernel when the catalog has one.
+    void try_fixed(PassSpec& ps, const SingleCfg& cfg) {
+        if (req.no_fixed || (req.force_maxv && req.force_maxv != cfg.kc.maxv)) return;
+        PassParams& p = ps.p;
+        const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n);
+        if (!e) return;
+        if (e->nstages != p.fft1.nstages) return;
+        for (int i = 0; i < e->nstages; ++i)
+            if (e->radices[i] != p.fft1.radix[i]) return;
+        if (p.mode == kModeK) {
+            if (p.in.ks != 1 || p.out.ks != 1 || p.n_outer != 1) return;
+            int w = std::max(1, 256 / e->tpl);
+            w = static_cast<int>(std::min<int64_t>(w, p.n_cols));
+            while (w > 1 && (w * e->tpl > e->maxt || static_cast<int64_t>(w) * p.pitch * cs > smem_limit)) --w;
+            p.w = w;
+            ps.threads = round_up(w * e->tpl, 32);
+            ps.smem_bytes = static_cast<int64_t>(w) * p.pitch * cs;
+        } else {
+            if (p.in.cs != 1 || p.out.cs != 1 || p.in.d != 1 || p.out.d != 1) return;
+            p.w = e->w;
+            ps.threads = round_up(e->w * e->tpl, 32);
+            ps.smem_bytes = static_cast<int64_t>(e->w) * p.n * cs;
+            if (ps.smem_bytes > smem_limit) return;
+        }
+        if (ps.threads > e->maxt) return;
+        p.tpl = e->tpl;
+        p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+        p.tiles = p.n_outer * p.col_tiles;
+        ps.kc.maxt = e->maxt;
+        ps.fixed_id = e->id;
+    }
+
     bool fits(int64_t n, int mode) {
         SingleCfg cfg = single_cfg(n, req.dbl, req.force_maxv);
         if (!cfg.ok) return false;
@@ -226,6 +260,7 @@ struct Builder {
                 SingleCfg cfg = single_cfg(L, req.dbl, req.force_maxv);
                 set_fft(ps, p.fft1, &ps.tables.tw1, p.n, cfg);
                 geometry(ps, cfg, req.force_w);
+                try_fixed(ps, cfg);
                 ps.src = cur;
                 ps.dst = Buf::Output;
                 ps.bytes_moved = 2 * E * cs;
@@ -485,6 +520,15 @@ struct Builder {
     }
 };
 
+template <class... A>
+constexpr int count_args(A...) {
+    return static_cast<int>(sizeof...(A));
+}
+#define SFB_ENTRY(ID, DBL, MODEC, N, TPL, W, MAXT, ...) \
+    FixedEntry{ID, DBL, MODEC, N, TPL, W, MAXT, {__VA_ARGS__}, count_args(__VA_ARGS__)},
+const FixedEntry kFixed[] = {SFB_FIXED_CATALOG(SFB_ENTRY)};
+#undef SFB_ENTRY
+
 long double two_pi_l() { return 6.283185307179586476925286766559005768L; }
 
 }  // namespace
@@ -600,6 +644,12 @@ void host_fft_fp64(std::vector<std::complex<double>>& a, int sign) {
     }
 }
 
+const FixedEntry* find_fixed(bool dbl, int mode, int n) {
+    for (const FixedEntry& e : kFixed)
+        if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n) return &e;
+    return nullptr;
+}
+
 PlanSpec make_plan(const PlanRequest& req) {
     if (req.direction != -1 && req.direction != 1) throw std::invalid_argument("Invalid FFT direction");
     if (req.normalization < 0 || req.normalization > 3) throw std::invalid_argument("Invalid normalization");
@@ -641,7 +691,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"threads\":" << ps.threads << ",\"smem\":" << ps.smem_bytes << ",\"tiles\":" << p.tiles
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
-           << ",\"store_via_smem\":" << p.store_via_smem << "}";
+           << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id << "}";
     }
     os << "]}";
     return os.str();

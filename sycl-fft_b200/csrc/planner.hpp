@@ -47,7 +47,16 @@ struct PassSpec {
     std::string kind;        // "single", "fourstep_cols", "fourstep_rows", "bluestein_fused", ...
     int axis = 0;
     int64_t bytes_moved = 0; // HBM bytes this pass reads + writes (data, not tables)
+    int fixed_id = -1;       // size-specialised kernel (fixed_catalog.h), -1 = generic kernel
 };
+
+// One entry of fixed_catalog.h as seen by the host.
+struct FixedEntry {
+    int id, dbl, modec, n, tpl, w, maxt;
+    int radices[kMaxStages];
+    int nstages;
+};
+const FixedEntry* find_fixed(bool dbl, int mode, int n);
 
 struct PlanRequest {
     bool dbl = false;
@@ -60,6 +69,7 @@ struct PlanRequest {
     int force_maxv = 0;
     int force_w = 0;
     int smem_limit = 0;      // bytes, 0 = device default (227 KB)
+    bool no_fixed = false;   // force the generic kernel (tests, tuning)
 };
 
 struct PlanSpec {

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -17,6 +18,7 @@
 #include <vector>
 
 #include "../../include/syclfft_b200_provider.h"
+#include "fixed_launch.hpp"
 #include "launch.hpp"
 #include "planner.hpp"
 
@@ -60,7 +62,26 @@ private:
 struct BoundPass {
     PassParams p;
     PassSpec spec;
+    FixedParams fp;  // used when spec.fixed_id >= 0
 };
+
+FixedParams to_fixed(const PassParams& p) {
+    FixedParams f;
+    f.n_cols = p.n_cols;
+    f.col_tiles = p.col_tiles;
+    f.w = p.w;
+    f.in_hi = p.in.hi;
+    f.out_hi = p.out.hi;
+    f.in_pitch = p.in.cs;
+    f.out_pitch = p.out.cs;
+    f.in_ks = p.in.ks;
+    f.out_ks = p.out.ks;
+    f.tw = p.fft1.tw;
+    f.conj_in = p.conj_in;
+    f.conj_out = p.conj_out;
+    f.scale = p.scale;
+    return f;
+}
 
 struct DevicePlan {
     PlanSpec spec;
@@ -105,6 +126,9 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     req.in_place = cfg.in_place != 0;
     req.shape.assign(cfg.lengths, cfg.lengths + cfg.rank);
     req.batch = cfg.batch_count;
+    // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
+    // (used to test and compare it against the size-specialised kernels).
+    if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
 
     int device = cfg.device;
     if (device < 0) check(cudaGetDevice(&device), "cudaGetDevice");
@@ -152,6 +176,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         bp.p.postmul = tab(ps.tables.postmul);
         bp.p.tw4_hi = tab(ps.tables.tw4_hi);
         bp.p.tw4_lo = tab(ps.tables.tw4_lo);
+        bp.fp = to_fixed(bp.p);
         plan->passes.push_back(bp);
     }
     return plan.release();
@@ -170,9 +195,16 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
             if (b == Buf::Output) return out;
             return plan->scratch;
         };
-        check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec.kc.maxv, bp.spec.kc.maxt, bp.spec.threads,
-                          static_cast<size_t>(bp.spec.smem_bytes), buf(bp.spec.src), buf(bp.spec.dst), stream),
-              "FFT pass launch");
+        if (bp.spec.fixed_id >= 0) {
+            check(launch_fixed(bp.spec.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, bp.spec.threads,
+                               static_cast<size_t>(bp.spec.smem_bytes), bp.p.tiles, buf(bp.spec.src),
+                               buf(bp.spec.dst), stream),
+                  "FFT pass launch");
+        } else {
+            check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec.kc.maxv, bp.spec.kc.maxt, bp.spec.threads,
+                              static_cast<size_t>(bp.spec.smem_bytes), buf(bp.spec.src), buf(bp.spec.dst), stream),
+                  "FFT pass launch");
+        }
     }
     check(cudaEventRecord(plan->done, stream), "cudaEventRecord");
 }

@@ -164,6 +164,23 @@ def test_parity_vs_oracle_and_fp64(sf, torch, oracle_mod, shape, batch, dbl, gau
         assert e_or <= max(tol, 2 * e_or64), f"vs oracle {e_or:.3e} (oracle vs FP64 {e_or64:.3e})"
 
 
+GENERIC = [([4096], 16, False), ([13440], 2, False), ([256, 64], 2, True), ([64, 48, 40], 1, False),
+           ([2048], 8, True), ([128, 256], 2, False)]
+
+
+@pytest.mark.parametrize("shape,batch,dbl", GENERIC, ids=lambda v: str(v))
+def test_generic_kernel_path(sf, torch, oracle_mod, shape, batch, dbl, monkeypatch):
+    """The runtime-parameterised kernel (the fallback for sizes without a specialised
+    kernel) on sizes that normally take the specialised one."""
+    monkeypatch.setenv("SYCLFFT_B200_KERNELS", "generic")
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 77 + n, dt)
+    out, p = run(sf, torch, x, shape, batch, 1, 2, dbl)
+    assert all(ps["fixed_id"] == -1 for ps in p.describe()["passes"])
+    assert rel_l2(out, fp64_fft(x, shape, batch, 1, 1.0 / n)) <= spec_tol(n, dbl)
+
+
 def test_in_place_multi_axis(sf, torch):
     x = uniform_complex(2 * 12 * 40 * 9, 3)
     out, _ = run(sf, torch, x.copy(), [12, 40, 9], 2, -1, 0, False, in_place=True)

@@ -1,5 +1,6 @@
 #include "planner.hpp"
 
+#include "cluster_catalog.h"
 #include "fixed_catalog.h"
 
 #include <algorithm>
@@ -83,7 +84,7 @@ struct Builder {
     const PlanRequest& req;
     int cs;
     int smem_limit;
-    std::map<std::pair<int, int>, int> seq_tables;  // (n, maxv) -> table id
+    std::map<std::vector<int>, int> seq_tables;  // radix sequence -> twiddle table id
 
     int add_table(std::vector<std::complex<double>> t) {
         plan.tables.push_back(std::move(t));
@@ -104,7 +105,8 @@ struct Builder {
             ns *= radices[i];
         }
         if (ns != n) throw std::runtime_error("radix product mismatch");
-        auto key = std::make_pair(n, maxv);
+        (void)maxv;
+        const std::vector<int>& key = radices;
         auto it = seq_tables.find(key);
         if (it != seq_tables.end()) {
             *table_id = it->second;
@@ -267,6 +269,12 @@ struct Builder {
                 plan.passes.push_back(ps);
                 cur = Buf::Output;
                 return;
+            }
+            if (s == 1 && !req.no_cluster) {
+                if (const ClusterEntry* ce = find_cluster(req.dbl, L, req.cluster_p)) {
+                    cluster_pass(ax, L, O, *ce, cur);
+                    return;
+                }
             }
             int64_t n1, n2;
             if (!split(L, n1, n2)) throw std::runtime_error("FFT length too large for this provider");
@@ -494,6 +502,43 @@ struct Builder {
         cur = Buf::Output;
     }
 
+    // Whole line of length L = n1*n2 on one thread-block cluster (single HBM round trip).
+    void cluster_pass(int ax, int64_t L, int64_t O, const ClusterEntry& ce, Buf& cur) {
+        PassSpec ps;
+        ps.kind = "cluster";
+        ps.axis = ax;
+        PassParams& p = ps.p;
+        p.n = static_cast<int>(L);
+        p.mode = kModeK;
+        p.n_outer = 1;
+        p.n_cols = O;
+        p.in.cs = L; p.in.ks = 1;
+        p.out = p.in;
+        p.in_len = p.out_len = L;
+        p.conj_in = p.conj_out = req.direction == 1;
+        std::vector<int> r1(ce.r1, ce.r1 + ce.ns1), r2(ce.r2, ce.r2 + ce.ns2);
+        p.fft1 = make_seq(ce.n1, r1, 0, &ps.tables.tw1);
+        p.fft2 = make_seq(ce.n2, r2, 0, &ps.tables.tw2);
+        add_tw4(ps, L, -1);
+        ps.cluster_id = ce.id;
+        ps.cl_n1 = ce.n1;
+        ps.cl_n2 = ce.n2;
+        ps.cl_p = ce.p;
+        const int cw = ce.n2 / ce.p, rw = ce.n1 / ce.p;
+        ps.threads = std::max(cw * ce.tpl1, rw * ce.tpl2);
+        ps.smem_bytes = L / ce.p * cs;
+        if (ps.smem_bytes > smem_limit) throw std::runtime_error("cluster pass exceeds shared memory");
+        ps.kc.maxt = ce.maxt;
+        p.w = 1;
+        p.col_tiles = O;
+        p.tiles = O * ce.p;
+        ps.src = cur;
+        ps.dst = Buf::Output;
+        ps.bytes_moved = 2 * static_cast<int64_t>(plan.elements) * cs;
+        plan.passes.push_back(ps);
+        cur = Buf::Output;
+    }
+
     void copy_pass(Buf& cur) {
         PassSpec ps;
         ps.kind = "copy";
@@ -644,6 +689,24 @@ void host_fft_fp64(std::vector<std::complex<double>>& a, int sign) {
     }
 }
 
+#define SFB_CENTRY(ID, DBL, N1, N2, P, TPL1, TPL2, MAXT, MINB, R1, R2)                                      \
+    ClusterEntry{ID, DBL, N1, N2, P, TPL1, TPL2, MAXT, MINB, {SFB_EXPAND R1}, {SFB_EXPAND R2}, count_args(SFB_EXPAND R1), \
+                 count_args(SFB_EXPAND R2)},
+#define SFB_EXPAND(...) __VA_ARGS__
+const ClusterEntry kCluster[] = {SFB_CLUSTER_CATALOG(SFB_CENTRY)};
+#undef SFB_CENTRY
+#undef SFB_EXPAND
+
+const ClusterEntry* find_cluster(bool dbl, int64_t n, int prefer_p) {
+    const ClusterEntry* first = nullptr;
+    for (const ClusterEntry& e : kCluster) {
+        if (e.dbl != (dbl ? 1 : 0) || static_cast<int64_t>(e.n1) * e.n2 != n) continue;
+        if (!first) first = &e;
+        if (prefer_p == 0 || e.p == prefer_p) return &e;
+    }
+    return first;
+}
+
 const FixedEntry* find_fixed(bool dbl, int mode, int n) {
     for (const FixedEntry& e : kFixed)
         if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n) return &e;
@@ -691,7 +754,9 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"threads\":" << ps.threads << ",\"smem\":" << ps.smem_bytes << ",\"tiles\":" << p.tiles
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
-           << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id << "}";
+           << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
+           << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ps.cl_p << "]}";
     }
     os << "]}";
     return os.str();

@@ -48,7 +48,18 @@ struct PassSpec {
     int axis = 0;
     int64_t bytes_moved = 0; // HBM bytes this pass reads + writes (data, not tables)
     int fixed_id = -1;       // size-specialised kernel (fixed_catalog.h), -1 = generic kernel
+    int cluster_id = -1;     // cluster kernel (cluster_catalog.h) for a whole long line
+    int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
 };
+
+// One entry of cluster_catalog.h as seen by the host.
+struct ClusterEntry {
+    int id, dbl, n1, n2, p, tpl1, tpl2, maxt, minb;
+    int r1[kMaxStages], r2[kMaxStages];
+    int ns1, ns2;
+};
+// Entries for a line length; `prefer_p` (0 = catalog order) picks the cluster size.
+const ClusterEntry* find_cluster(bool dbl, int64_t n, int prefer_p);
 
 // One entry of fixed_catalog.h as seen by the host.
 struct FixedEntry {
@@ -70,6 +81,8 @@ struct PlanRequest {
     int force_w = 0;
     int smem_limit = 0;      // bytes, 0 = device default (227 KB)
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
+    bool no_cluster = false; // force the two-pass four-step for long lines
+    int cluster_p = 0;       // preferred cluster size (0 = catalog order)
 };
 
 struct PlanSpec {

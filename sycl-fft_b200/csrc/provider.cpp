@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/syclfft_b200_provider.h"
+#include "cluster_launch.hpp"
 #include "fixed_launch.hpp"
 #include "launch.hpp"
 #include "planner.hpp"
@@ -62,8 +63,25 @@ private:
 struct BoundPass {
     PassParams p;
     PassSpec spec;
-    FixedParams fp;  // used when spec.fixed_id >= 0
+    FixedParams fp;    // used when spec.fixed_id >= 0
+    ClusterParams cp;  // used when spec.cluster_id >= 0
 };
+
+ClusterParams to_cluster(const PassParams& p) {
+    ClusterParams c;
+    c.lines = p.n_cols;
+    c.in_pitch = p.in.cs;
+    c.out_pitch = p.out.cs;
+    c.tw1 = p.fft1.tw;
+    c.tw2 = p.fft2.tw;
+    c.tw4_hi = p.tw4_hi;
+    c.tw4_lo = p.tw4_lo;
+    c.tw4_shift = p.tw4_shift;
+    c.conj_in = p.conj_in;
+    c.conj_out = p.conj_out;
+    c.scale = p.scale;
+    return c;
+}
 
 FixedParams to_fixed(const PassParams& p) {
     FixedParams f;
@@ -129,6 +147,11 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
+    // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
+    if (const char* k = std::getenv("SYCLFFT_B200_CLUSTER")) {
+        if (std::strcmp(k, "off") == 0) req.no_cluster = true;
+        else req.cluster_p = std::atoi(k);
+    }
 
     int device = cfg.device;
     if (device < 0) check(cudaGetDevice(&device), "cudaGetDevice");
@@ -177,6 +200,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         bp.p.tw4_hi = tab(ps.tables.tw4_hi);
         bp.p.tw4_lo = tab(ps.tables.tw4_lo);
         bp.fp = to_fixed(bp.p);
+        bp.cp = to_cluster(bp.p);
         plan->passes.push_back(bp);
     }
     return plan.release();
@@ -195,7 +219,10 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
             if (b == Buf::Output) return out;
             return plan->scratch;
         };
-        if (bp.spec.fixed_id >= 0) {
+        if (bp.spec.cluster_id >= 0) {
+            check(launch_cluster(bp.spec.cluster_id, bp.cp, buf(bp.spec.src), buf(bp.spec.dst), stream),
+                  "FFT cluster pass launch");
+        } else if (bp.spec.fixed_id >= 0) {
             check(launch_fixed(bp.spec.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, bp.spec.threads,
                                static_cast<size_t>(bp.spec.smem_bytes), bp.p.tiles, buf(bp.spec.src),
                                buf(bp.spec.dst), stream),

@@ -47,7 +47,44 @@ void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, 
     }
 }
 
+// Cluster pass: columns (length n1, stride n2) with the n1 stage table, four-step twiddle,
+// rows (length n2) with the n2 stage table, stored transposed -- per line.
+void run_cluster(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) {
+    const PassParams& p = ps.p;
+    const int n1 = ps.cl_n1, n2 = ps.cl_n2, N = n1 * n2;
+    const auto& hi = plan.tables[ps.tables.tw4_hi];
+    const auto& lo = plan.tables[ps.tables.tw4_lo];
+    std::vector<cd> line(N), y(N), col(n1), row(n2);
+    for (int64_t c = 0; c < p.n_cols; ++c) {
+        for (int k = 0; k < N; ++k) {
+            line[k] = src[c * p.in.cs + k];
+            if (p.conj_in) line[k] = std::conj(line[k]);
+        }
+        for (int b = 0; b < n2; ++b) {
+            for (int a = 0; a < n1; ++a) col[a] = line[int64_t(a) * n2 + b];
+            stockham(col, p.fft1, plan.tables[ps.tables.tw1], n1);
+            for (int k1 = 0; k1 < n1; ++k1) {
+                const int64_t m = int64_t(k1) * b;
+                y[int64_t(k1) * n2 + b] = col[k1] * hi[m >> p.tw4_shift] * lo[m & ((int64_t(1) << p.tw4_shift) - 1)];
+            }
+        }
+        for (int k1 = 0; k1 < n1; ++k1) {
+            for (int b = 0; b < n2; ++b) row[b] = y[int64_t(k1) * n2 + b];
+            stockham(row, p.fft2, plan.tables[ps.tables.tw2], n2);
+            for (int k2 = 0; k2 < n2; ++k2) {
+                cd v = row[k2];
+                if (p.conj_out) v = std::conj(v);
+                dst[c * p.out.cs + k1 + int64_t(n1) * k2] = v * p.scale;
+            }
+        }
+    }
+}
+
 void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) {
+    if (ps.cluster_id >= 0) {
+        run_cluster(plan, ps, src, dst);
+        return;
+    }
     const PassParams& p = ps.p;
     auto table = [&](int id) -> const std::vector<cd>* { return id < 0 ? nullptr : &plan.tables[id]; };
     const auto* premul = table(ps.tables.premul);

@@ -165,7 +165,29 @@ def test_parity_vs_oracle_and_fp64(sf, torch, oracle_mod, shape, batch, dbl, gau
 
 
 GENERIC = [([4096], 16, False), ([13440], 2, False), ([256, 64], 2, True), ([64, 48, 40], 1, False),
-           ([2048], 8, True), ([128, 256], 2, False)]
+           ([2048], 8, True), ([128, 256], 2, False), ([65536], 4, True)]
+
+
+@pytest.mark.parametrize("cluster", ["8", "16", "off"])
+@pytest.mark.parametrize("shape,batch,dbl", [([65536], 6, True), ([65536], 3, False), ([131072], 2, False),
+                                             ([32768], 5, True), ([32768], 4, False)], ids=lambda v: str(v))
+def test_long_line_paths(sf, torch, shape, batch, dbl, cluster, monkeypatch):
+    """Long lines on the cluster kernel (cluster sizes 8 and 16) and on the two-pass four-step."""
+    monkeypatch.setenv("SYCLFFT_B200_CLUSTER", cluster)
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 5 + n, dt)
+    for d, norm in ((-1, 3), (1, 1)):
+        out, p = run(sf, torch, x, shape, batch, d, norm, dbl)
+        kinds = [ps["kind"] for ps in p.describe()["passes"]]
+        assert kinds == (["fourstep_cols", "fourstep_rows"] if cluster == "off" else ["cluster"]), kinds
+        assert rel_l2(out, fp64_fft(x, shape, batch, d, norm_scale(norm, d, n))) <= spec_tol(n, dbl)
+    xt = torch.from_numpy(x).cuda()
+    keep = xt.clone()
+    ip = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward,
+                          sf.plan_options(placement=sf.placement.in_place))
+    ip.execute(xt).synchronize()
+    assert rel_l2(xt.cpu().numpy(), fp64_fft(keep.cpu().numpy(), shape, batch, -1)) <= spec_tol(n, dbl)
 
 
 @pytest.mark.parametrize("shape,batch,dbl", GENERIC, ids=lambda v: str(v))
@@ -173,6 +195,7 @@ def test_generic_kernel_path(sf, torch, oracle_mod, shape, batch, dbl, monkeypat
     """The runtime-parameterised kernel (the fallback for sizes without a specialised
     kernel) on sizes that normally take the specialised one."""
     monkeypatch.setenv("SYCLFFT_B200_KERNELS", "generic")
+    monkeypatch.setenv("SYCLFFT_B200_CLUSTER", "off")
     n = int(np.prod(shape))
     dt = np.complex128 if dbl else np.complex64
     x = uniform_complex(n * batch, 77 + n, dt)

@@ -25,7 +25,7 @@ SHAPES = [
     ([8], 2), ([1024], 3), ([4096], 2), ([13440], 1), ([16384], 1), ([11], 3), ([1009], 2), ([4099], 1),
     ([16, 12, 10], 2), ([11, 3], 1), ([3, 4], 2), ([2, 3, 5], 1), ([1], 5), ([1, 1], 2), ([32768], 2),
     ([65536], 1), ([65537], 1), ([30000], 2), ([64, 2048], 1), ([3, 40000], 1), ([40000, 3], 1),
-    ([65537, 2], 1), ([257, 5], 2), ([7, 1, 9], 3), ([2048, 2048 // 64], 1),
+    ([65537, 2], 1), ([257, 5], 2), ([7, 1, 9], 3), ([2048, 2048 // 64], 1), ([131072], 1), ([65536, 3], 1),
 ]
 
 
@@ -44,7 +44,9 @@ def test_plan_kinds():
     _, d = emulate(np.zeros(4096 * 2), [4096], 2, -1)
     assert [p["kind"] for p in d["passes"]] == ["single"]
     _, d = emulate(np.zeros(65536), [65536], 1, -1, double=True)
-    assert [p["kind"] for p in d["passes"]] == ["fourstep_cols", "fourstep_rows"]
+    assert [p["kind"] for p in d["passes"]] == ["cluster"]
+    _, d = emulate(np.zeros(2 * 65536), [65536, 2], 1, -1, double=True)
+    assert [p["kind"] for p in d["passes"]][1:] == ["fourstep_cols", "fourstep_rows"]
     _, d = emulate(np.zeros(1009), [1009], 1, -1)
     assert [p["kind"] for p in d["passes"]] == ["bluestein_fused"]
     _, d = emulate(np.zeros(65537), [65537], 1, -1)

@@ -28,7 +28,17 @@ struct FixedParams {
     const void* tw = nullptr;           // concatenated per-stage twiddles [ns][R-1]
     int conj_in = 0, conj_out = 0;
     double scale = 1.0;
+    // kFeatTw4 (kModeC column pass of a four-step): multiply output k of column c by
+    // W_L^(k*c) = tw4_hi[m >> tw4_shift] * tw4_lo[m & mask], m = k * c.
+    const void* tw4_hi = nullptr;
+    const void* tw4_lo = nullptr;
+    int tw4_shift = 0;
+    // kFeatTStore (kModeK row pass of a four-step): row l = o*rows + k1 of length N is
+    // stored transposed at o * line + k1 + k2 * rows (coalesced over consecutive rows).
+    int64_t rows = 1, line = 0;
 };
+
+enum : int { kFeatPlain = 0, kFeatTw4 = 1, kFeatTStore = 2 };
 
 template <class T>
 struct FixedCtx {
@@ -43,6 +53,9 @@ struct FixedCtx {
     int64_t in_ks, out_ks;
     T scale;
     bool conj_in, conj_out;
+    int sel;              // column index (kFeatTw4)
+    const C *tw4_hi, *tw4_lo;
+    int tw4_shift;
 };
 
 template <class T> __host__ __device__ constexpr int pad_shift_c() { return sizeof(T) == 4 ? 4 : 3; }
@@ -56,7 +69,7 @@ __device__ __forceinline__ int pidx(int k) {
     return k + (k >> pad_shift_c<T>());
 }
 
-template <class T, int N, int TPL, bool MODEC, int W, int NS, int TWOFF, int R, bool FIRST, bool LAST>
+template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int NS, int TWOFF, int R, bool FIRST, bool LAST>
 __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
     using C = cplx<T>;
     constexpr int PS = pad_shift_c<T>();
@@ -107,13 +120,28 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 for (int r = 1; r < R; ++r) u[r] = cmul(u[r], __ldg(twp + (r - 1)));
             }
             dft<R, T>(u);
-            if constexpr (LAST) {
+            if constexpr (LAST && FEAT == kFeatTStore) {
+                // natural order into shared memory; the transposed store follows the stages
+                if constexpr (NR % PAD == 0) {
+                    C* p = X.sm + pidx<T>(j);
+#pragma unroll
+                    for (int r = 0; r < R; ++r) p[r * (NR + NR / PAD)] = u[r];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) X.sm[pidx<T>(j + r * NR)] = u[r];
+                }
+            } else if constexpr (LAST) {
                 // last stage: base == j, outputs at j + r * NR
                 if (X.line_ok) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         C a = u[r];
                         if (X.conj_out) a.y = -a.y;
+                        if constexpr (FEAT == kFeatTw4) {
+                            const int m = (j + r * NR) * X.sel;
+                            a = cmul(a, cmul(__ldg(X.tw4_hi + (m >> X.tw4_shift)),
+                                             __ldg(X.tw4_lo + (m & ((1 << X.tw4_shift) - 1)))));
+                        }
                         a.x *= X.scale;
                         a.y *= X.scale;
                         if constexpr (MODEC) X.gout[(int64_t)(j + r * NR) * X.out_ks] = a;
@@ -136,14 +164,15 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             }
         }
     }
-    if constexpr (!LAST) __syncthreads();
+    if constexpr (!LAST || FEAT == kFeatTStore) __syncthreads();
 }
 
-template <class T, int N, int TPL, bool MODEC, int W, int NS, int TWOFF, bool FIRST, int R, int... Rest>
+template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int NS, int TWOFF, bool FIRST, int R, int... Rest>
 __device__ __forceinline__ void fixed_stages(FixedCtx<T>& X) {
     constexpr bool LAST = sizeof...(Rest) == 0;
-    fixed_stage<T, N, TPL, MODEC, W, NS, TWOFF, R, FIRST, LAST>(X);
-    if constexpr (!LAST) fixed_stages<T, N, TPL, MODEC, W, NS * R, TWOFF + NS * (R - 1), false, Rest...>(X);
+    fixed_stage<T, N, TPL, MODEC, W, FEAT, NS, TWOFF, R, FIRST, LAST>(X);
+    if constexpr (!LAST)
+        fixed_stages<T, N, TPL, MODEC, W, FEAT, NS * R, TWOFF + NS * (R - 1), false, Rest...>(X);
 }
 
 // Register budget: 64 per thread (16 float or 8 double complex values per stage).
@@ -154,7 +183,7 @@ __host__ __device__ constexpr int fixed_min_blocks() {
 
 // kModeK: grid = ceil(lines / w), block = w * TPL (<= MAXT), dynamic smem = w * kpitch<T,N>() * sizeof(C).
 // kModeC: grid = n_outer * col_tiles, block = W * TPL, dynamic smem = N * W * sizeof(C).
-template <class T, int N, int TPL, bool MODEC, int W, int MAXT, int REGS, int... Rs>
+template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int MAXT, int REGS, int... Rs>
 __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
     fft_fixed_kernel(const __grid_constant__ FixedParams P, const cplx<T>* in, cplx<T>* out) {
     using C = cplx<T>;
@@ -174,6 +203,10 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         const int64_t o = tile / P.col_tiles;
         const int64_t c = (tile - o * P.col_tiles) * W + w;
         X.line_ok = X.active && c < P.n_cols;
+        X.sel = static_cast<int>(c);
+        X.tw4_hi = static_cast<const C*>(P.tw4_hi);
+        X.tw4_lo = static_cast<const C*>(P.tw4_lo);
+        X.tw4_shift = P.tw4_shift;
         X.sm = sm + w;
         X.gin = in + o * P.in_hi + c;
         X.gout = out + o * P.out_hi + c;
@@ -191,7 +224,25 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         X.in_ks = 1;
         X.out_ks = 1;
     }
-    fixed_stages<T, N, TPL, MODEC, W, 1, 0, true, Rs...>(X);
+    fixed_stages<T, N, TPL, MODEC, W, FEAT, 1, 0, true, Rs...>(X);
+    if constexpr (FEAT == kFeatTStore && !MODEC) {
+        // Rows blockIdx.x*w .. +w-1 are consecutive k1 of one line when rows % w == 0:
+        // walk (row fastest, element) so every store is a w-wide segment.
+        const int64_t row0 = (int64_t)blockIdx.x * P.w;
+        const T sc = X.scale;
+        for (int idx = tid; idx < P.w * N; idx += blockDim.x) {
+            const int k = idx / P.w;
+            const int w = idx - k * P.w;
+            const int64_t l = row0 + w;
+            if (l >= P.n_cols) continue;
+            C a = sm[w * kpitch<T, N>() + pidx<T>(k)];
+            if (X.conj_out) a.y = -a.y;
+            a.x *= sc;
+            a.y *= sc;
+            const int64_t o = l / P.rows;
+            out[o * P.line + (l - o * P.rows) + (int64_t)k * P.rows] = a;
+        }
+    }
 }
 
 }  // namespace sfb

@@ -18,18 +18,18 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 
-template <bool ENABLED, class T, int N, int TPL, bool MODEC, int W, int MAXT, int... Rs>
+template <bool ENABLED, class T, int N, int TPL, bool MODEC, int W, int FEAT, int MAXT, int... Rs>
 struct FixedLauncher {
     static cudaError_t run(const FixedParams&, int, size_t, int64_t, const void*, void*, cudaStream_t) {
         return cudaErrorInvalidDeviceFunction;
     }
 };
 
-template <class T, int N, int TPL, bool MODEC, int W, int MAXT, int... Rs>
-struct FixedLauncher<true, T, N, TPL, MODEC, W, MAXT, Rs...> {
+template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int MAXT, int... Rs>
+struct FixedLauncher<true, T, N, TPL, MODEC, W, FEAT, MAXT, Rs...> {
     static cudaError_t run(const FixedParams& p, int threads, size_t smem, int64_t grid, const void* in, void* out,
                            cudaStream_t stream) {
-        auto kernel = fft_fixed_kernel<T, N, TPL, MODEC, W, MAXT, 64, Rs...>;
+        auto kernel = fft_fixed_kernel<T, N, TPL, MODEC, W, FEAT, MAXT, 64, Rs...>;
         static std::atomic<int> configured[kMaxDevices];
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -57,10 +57,11 @@ struct FixedLauncher<true, T, N, TPL, MODEC, W, MAXT, Rs...> {
 cudaError_t SFB_FIXED_FN(int id, const FixedParams& p, int threads, size_t smem, int64_t grid, const void* in,
                          void* out, cudaStream_t stream) {
     switch (id) {
-#define SFB_X(ID, DBL, MODEC, N, TPL, W, MAXT, ...)                                                            \
+#define SFB_X(ID, DBL, MODEC, FEAT, N, TPL, W, MAXT, ...)                                                     \
     case ID:                                                                                                  \
         return FixedLauncher<((DBL) * 2 + (MODEC)) == SFB_FIXED_PART, std::conditional_t<(DBL) != 0, double, float>, \
-                             N, TPL, (MODEC) != 0, W, MAXT, __VA_ARGS__>::run(p, threads, smem, grid, in, out, stream);
+                             N, TPL, (MODEC) != 0, W, FEAT, MAXT, __VA_ARGS__>::run(p, threads, smem, grid, in, out,   \
+                                                                                    stream);
         SFB_FIXED_CATALOG(SFB_X)
 #undef SFB_X
         default:

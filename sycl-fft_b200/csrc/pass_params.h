@@ -74,6 +74,9 @@ struct PassParams {
     const void* postmul = nullptr;    // indexed by g on store
     double scale = 1.0;
     int store_via_smem = 0;           // transpose through shared memory before storing
+    // Size-specialised four-step row pass: row l (= o*ts_rows + k1) stored at
+    // (l / ts_rows) * ts_line + l % ts_rows + k * ts_rows.
+    int64_t ts_rows = 0, ts_line = 0;
 };
 
 }  // namespace sfb

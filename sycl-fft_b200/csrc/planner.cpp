@@ -180,7 +180,7 @@ struct Builder {
     void try_fixed(PassSpec& ps, const SingleCfg& cfg) {
         if (req.no_fixed || (req.force_maxv && req.force_maxv != cfg.kc.maxv)) return;
         PassParams& p = ps.p;
-        const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n);
+        const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n, kFixedPlain);
         if (!e) return;
         if (e->nstages != p.fft1.nstages) return;
         for (int i = 0; i < e->nstages; ++i)
@@ -206,6 +206,46 @@ struct Builder {
         p.tiles = p.n_outer * p.col_tiles;
         ps.kc.maxt = e->maxt;
         ps.fixed_id = e->id;
+        ps.fixed_feat = kFixedPlain;
+    }
+
+    // Four-step passes of a contiguous axis on their size-specialised kernels.
+    void try_fixed_fourstep(PassSpec& ps, int feat, int64_t rows = 0, int64_t line = 0) {
+        if (req.no_fixed) return;
+        PassParams& p = ps.p;
+        const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n, feat);
+        if (!e || e->nstages != p.fft1.nstages) return;
+        for (int i = 0; i < e->nstages; ++i)
+            if (e->radices[i] != p.fft1.radix[i]) return;
+        const int threads = round_up(e->w * e->tpl, 32);
+        if (threads > e->maxt) return;
+        if (feat == kFixedTw4) {
+            const int64_t smem = static_cast<int64_t>(e->w) * p.n * cs;
+            if (smem > smem_limit || p.in.d != 1 || p.out.d != 1 || p.in.cs != 1 || p.out.cs != 1) return;
+            p.w = e->w;
+            ps.smem_bytes = smem;
+        } else {
+            if (rows % e->w != 0) return;
+            const int64_t smem = static_cast<int64_t>(e->w) * p.pitch * cs;
+            if (smem > smem_limit) return;
+            // flat row index l = o * rows + k1 with pitch n
+            p.n_cols = p.n_outer * p.n_cols;
+            p.n_outer = 1;
+            p.in.hi = 0;
+            p.in.cs = p.n;
+            p.in.ks = 1;
+            p.ts_rows = rows;
+            p.ts_line = line;
+            p.w = e->w;
+            ps.smem_bytes = smem;
+        }
+        ps.threads = threads;
+        p.tpl = e->tpl;
+        p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+        p.tiles = p.n_outer * p.col_tiles;
+        ps.kc.maxt = e->maxt;
+        ps.fixed_id = e->id;
+        ps.fixed_feat = feat;
     }
 
     bool fits(int64_t n, int mode) {
@@ -216,7 +256,7 @@ struct Builder {
         return bytes <= smem_limit;
     }
 
-    void set_fft(PassSpec& ps, StageSeq& seq, int* tid, int n, const SingleCfg& cfg) {
+    void set_fft(PassSpec&, StageSeq& seq, int* tid, int n, const SingleCfg& cfg) {
         seq = make_seq(n, cfg.radices, cfg.kc.maxv, tid);
     }
 
@@ -270,7 +310,9 @@ struct Builder {
                 cur = Buf::Output;
                 return;
             }
-            if (s == 1 && !req.no_cluster) {
+            // The cluster kernel is opt-in (cluster_p > 0, chosen by the autotuner or the caller):
+            // measured slower than the size-specialised two-pass four-step on B200.
+            if (s == 1 && !req.no_cluster && req.cluster_p > 0) {
                 if (const ClusterEntry* ce = find_cluster(req.dbl, L, req.cluster_p)) {
                     cluster_pass(ax, L, O, *ce, cur);
                     return;
@@ -304,6 +346,7 @@ struct Builder {
                 set_fft(a, p.fft1, &a.tables.tw1, p.n, cfg);
                 add_tw4(a, L, -1);
                 geometry(a, cfg, 0);
+                if (s == 1) try_fixed_fourstep(a, kFixedTw4);
                 a.src = cur;
                 a.dst = Buf::Scratch;
                 a.bytes_moved = 2 * E * cs;
@@ -333,6 +376,7 @@ struct Builder {
                 set_fft(b, p.fft1, &b.tables.tw1, p.n, cfg);
                 // rows per CTA: enough for 128-byte segments of the transposed store
                 geometry(b, cfg, s == 1 ? std::max(1, 128 / cs) : 0);
+                if (s == 1) try_fixed_fourstep(b, kFixedTStore, n1, L);
                 b.src = Buf::Scratch;
                 b.dst = Buf::Output;
                 b.bytes_moved = 2 * E * cs;
@@ -569,8 +613,8 @@ template <class... A>
 constexpr int count_args(A...) {
     return static_cast<int>(sizeof...(A));
 }
-#define SFB_ENTRY(ID, DBL, MODEC, N, TPL, W, MAXT, ...) \
-    FixedEntry{ID, DBL, MODEC, N, TPL, W, MAXT, {__VA_ARGS__}, count_args(__VA_ARGS__)},
+#define SFB_ENTRY(ID, DBL, MODEC, FEAT, N, TPL, W, MAXT, ...) \
+    FixedEntry{ID, DBL, MODEC, FEAT, N, TPL, W, MAXT, {__VA_ARGS__}, count_args(__VA_ARGS__)},
 const FixedEntry kFixed[] = {SFB_FIXED_CATALOG(SFB_ENTRY)};
 #undef SFB_ENTRY
 
@@ -707,9 +751,9 @@ const ClusterEntry* find_cluster(bool dbl, int64_t n, int prefer_p) {
     return first;
 }
 
-const FixedEntry* find_fixed(bool dbl, int mode, int n) {
+const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
     for (const FixedEntry& e : kFixed)
-        if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n) return &e;
+        if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n && e.feat == feat) return &e;
     return nullptr;
 }
 

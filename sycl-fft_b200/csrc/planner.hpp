@@ -48,6 +48,7 @@ struct PassSpec {
     int axis = 0;
     int64_t bytes_moved = 0; // HBM bytes this pass reads + writes (data, not tables)
     int fixed_id = -1;       // size-specialised kernel (fixed_catalog.h), -1 = generic kernel
+    int fixed_feat = 0;      // its feature (kFixedPlain / kFixedTw4 / kFixedTStore)
     int cluster_id = -1;     // cluster kernel (cluster_catalog.h) for a whole long line
     int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
 };
@@ -62,12 +63,13 @@ struct ClusterEntry {
 const ClusterEntry* find_cluster(bool dbl, int64_t n, int prefer_p);
 
 // One entry of fixed_catalog.h as seen by the host.
+enum : int { kFixedPlain = 0, kFixedTw4 = 1, kFixedTStore = 2 };
 struct FixedEntry {
-    int id, dbl, modec, n, tpl, w, maxt;
+    int id, dbl, modec, feat, n, tpl, w, maxt;
     int radices[kMaxStages];
     int nstages;
 };
-const FixedEntry* find_fixed(bool dbl, int mode, int n);
+const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat);
 
 struct PlanRequest {
     bool dbl = false;
@@ -82,7 +84,7 @@ struct PlanRequest {
     int smem_limit = 0;      // bytes, 0 = device default (227 KB)
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
     bool no_cluster = false; // force the two-pass four-step for long lines
-    int cluster_p = 0;       // preferred cluster size (0 = catalog order)
+    int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size
 };
 
 struct PlanSpec {

@@ -98,6 +98,11 @@ FixedParams to_fixed(const PassParams& p) {
     f.conj_in = p.conj_in;
     f.conj_out = p.conj_out;
     f.scale = p.scale;
+    f.tw4_hi = p.tw4_hi;
+    f.tw4_lo = p.tw4_lo;
+    f.tw4_shift = p.tw4_shift;
+    f.rows = p.ts_rows;
+    f.line = p.ts_line;
     return f;
 }
 
@@ -188,7 +193,8 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
     };
     for (const PassSpec& ps : plan->spec.passes) {
-        if (!has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt)) throw std::runtime_error("no kernel variant for pass");
+        if (ps.fixed_id < 0 && ps.cluster_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
+            throw std::runtime_error("no kernel variant for pass");
         BoundPass bp;
         bp.spec = ps;
         bp.p = ps.p;

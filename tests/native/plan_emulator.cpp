@@ -125,6 +125,7 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
             stockham(L.v, p.fft2, plan.tables[ps.tables.tw2], p.n);
         }
         const int64_t ob = line_base(p.out, L.o, L.c);
+        const bool tstore = ps.fixed_id >= 0 && ps.fixed_feat == kFixedTStore;
         for (int k = 0; k < p.n; ++k) {
             const int64_t g = int64_t(k) * p.g_k + sel;
             if (g >= p.out_len) continue;
@@ -138,6 +139,12 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
             }
             if (postmul) v *= (*postmul)[g];
             v *= p.scale;
+            if (tstore) {
+                // size-specialised row pass: flat row l stored transposed
+                const int64_t l = L.c, o = l / p.ts_rows;
+                dst[o * p.ts_line + (l - o * p.ts_rows) + int64_t(k) * p.ts_rows] = v;
+                continue;
+            }
             dst[ob + int64_t(k) * p.out.ks] = v;
         }
     }

@@ -65,9 +65,13 @@ def test_provider_selection_and_query(sf, torch):
     assert all(r["reason"] for r in rows if not r["available"])
 
 
-def test_scratch_size(sf, torch):
+def test_scratch_size(sf, torch, monkeypatch):
     assert sf.plan_many_dft("float", [4096], 16, sf.direction.forward).scratch_size_bytes() == 0
     assert sf.plan_many_dft("double", [65536], 4, sf.direction.forward).scratch_size_bytes() >= 65536 * 4 * 16
+    monkeypatch.setenv("SYCLFFT_B200_CLUSTER", "8")
+    assert sf.plan_many_dft("double", [65536], 4, sf.direction.forward).scratch_size_bytes() == 0  # cluster kernel
+    monkeypatch.delenv("SYCLFFT_B200_CLUSTER")
+    assert sf.plan_many_dft("double", [65536, 3], 1, sf.direction.forward).scratch_size_bytes() >= 65536 * 3 * 16
     assert sf.plan_many_dft("float", [65537], 2, sf.direction.forward).scratch_size_bytes() >= 2 * 131073 * 8
 
 

@@ -44,7 +44,8 @@ def test_plan_kinds():
     _, d = emulate(np.zeros(4096 * 2), [4096], 2, -1)
     assert [p["kind"] for p in d["passes"]] == ["single"]
     _, d = emulate(np.zeros(65536), [65536], 1, -1, double=True)
-    assert [p["kind"] for p in d["passes"]] == ["cluster"]
+    assert [p["kind"] for p in d["passes"]] == ["fourstep_cols", "fourstep_rows"]
+    assert all(p["fixed_id"] >= 0 for p in d["passes"])
     _, d = emulate(np.zeros(2 * 65536), [65536, 2], 1, -1, double=True)
     assert [p["kind"] for p in d["passes"]][1:] == ["fourstep_cols", "fourstep_rows"]
     _, d = emulate(np.zeros(1009), [1009], 1, -1)

@@ -95,4 +95,26 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
 /* Library version string. */
 SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
 
+/* ---- Transform without device allocation (no counterpart in the reference). ----
+ *
+ * For callers that cannot allocate device memory at the point they need a transform:
+ * a framework whose memory planner owns the device and hands out only planned buffers,
+ * a real-time loop that must not call cudaMalloc (it may synchronize the device), or a
+ * process whose free memory already belongs to its own pool. Plans allocate their
+ * twiddle tables and four-step scratch; this call instead uses two fixed arrays in the
+ * library's device memory (a 32 MiB scratch and a small twiddle table, held by every
+ * GPU that loads the library until the process exits) and calls no allocator.
+ *
+ * Batched 1-D complex<float> C2C of power-of-two length n in [2^15, 2^20] over `batch`
+ * contiguous lines, n * batch <= 4194304 (4 Mi) elements; larger sizes are rejected with
+ * an error message. in == out (in place) is allowed. direction -1 / +1,
+ * normalization SYCLFFT_B200_NORM_*. Enqueued on `stream` (cudaStream_t, NULL = legacy
+ * default stream); returns 0, or writes err and returns non-zero.
+ * All calls share the arrays: calls that overlap on the GPU race and must be ordered by
+ * the caller. The first call on a device looks up the arrays' device addresses and
+ * should come before any stream capture. */
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void *in, void *out, uint64_t n, uint64_t batch,
+                                                             int32_t direction, uint32_t normalization,
+                                                             void *stream, char *err, size_t cap);
+
 #endif /* SYCLFFT_B200_PROVIDER_H */

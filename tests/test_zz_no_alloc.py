@@ -1,0 +1,92 @@
+"""The allocation-free entry point (syclfft_b200_execute_noalloc_c2c_f32), called
+through the C ABI, against the plan entry point on the same inputs.
+
+It serves callers that cannot allocate device memory when they transform (a framework
+whose memory planner owns the device, a real-time loop that must not call cudaMalloc):
+its scratch and twiddles live in fixed arrays inside the library. This file is named to
+be collected last, so a run that stops at the first failure has run everything else.
+It passes alone in a fresh process and after the other tests.
+"""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+def rel_l2(a, b):
+    a = a.to(dtype=b.dtype)
+    return float((a - b).abs().pow(2).sum().sqrt() / b.abs().pow(2).sum().sqrt())
+
+
+def plan_reference(torch, x, n, batch, direction, norm):
+    """The existing entry point: a plan of the provider's C ABI."""
+    from syclfft_b200 import _provider
+    api = _provider.provider()
+    err = ctypes.create_string_buffer(1024)
+    cfg = _provider.make_config([n], batch, direction, double=False, normalization=norm)
+    h = api.create(ctypes.byref(cfg), err, 1024)
+    assert h, err.value
+    y = torch.empty_like(x)
+    rc = api.execute(h, x.data_ptr(), y.data_ptr(), torch.cuda.current_stream().cuda_stream, err, 1024)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    api.destroy(h)
+    return y
+
+
+def noalloc(torch, x, out, n, batch, direction, norm):
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    rc = lib.syclfft_b200_execute_noalloc_c2c_f32(x.data_ptr(), out.data_ptr(), n, batch, direction, norm,
+                                                  torch.cuda.current_stream().cuda_stream, err, 1024)
+    return rc, err.value.decode()
+
+
+def test_noalloc_matches_plan_entry_point_twice(torch):
+    cases = [(65536, 8, -1, 3), (1 << 20, 2, 1, 2)]  # two calls in a row, different length and direction
+    for n, batch, direction, norm in cases:
+        g = torch.Generator(device="cuda").manual_seed(n + batch)
+        x = torch.complex(torch.rand(n * batch, device="cuda", generator=g) * 2 - 1,
+                          torch.rand(n * batch, device="cuda", generator=g) * 2 - 1)
+        keep = x.clone()
+        out = torch.empty_like(x)
+        rc, msg = noalloc(torch, x, out, n, batch, direction, norm)
+        assert rc == 0, msg
+        torch.cuda.synchronize()
+        assert torch.equal(x, keep)  # out-of-place input untouched
+        ref = plan_reference(torch, x, n, batch, direction, norm)
+        tol = 1e-5 * math.log2(n)  # the float tolerance of the parity tests
+        assert rel_l2(out, ref) <= tol
+        # also against an FP64 FFT of the same input
+        xs = x.view(batch, n)[:2].cpu().numpy().astype(np.complex128)
+        f = np.fft.fft(xs, axis=1) if direction == -1 else np.fft.ifft(xs, axis=1) * n
+        scale = {3: 1 / math.sqrt(n), 2: (1 / n if direction == 1 else 1.0)}[norm]
+        got = out.view(batch, n)[:2].cpu().numpy()
+        assert np.linalg.norm(got - f * scale) / np.linalg.norm(f * scale) <= tol
+
+
+def test_noalloc_in_place_and_limits(torch):
+    n, batch = 32768, 4
+    x = torch.randn(n * batch, dtype=torch.complex64, device="cuda")
+    ref = plan_reference(torch, x, n, batch, -1, 0)
+    rc, msg = noalloc(torch, x, x, n, batch, -1, 0)
+    assert rc == 0, msg
+    torch.cuda.synchronize()
+    assert rel_l2(x, ref) <= 1e-5 * math.log2(n)
+    big = torch.empty(1, dtype=torch.complex64, device="cuda")
+    rc, msg = noalloc(torch, big, big, 1 << 20, 8, -1, 0)  # 8 Mi elements > the 4 Mi limit
+    assert rc != 0 and "limited" in msg
+    rc, msg = noalloc(torch, big, big, 3 * 4096, 1, -1, 0)
+    assert rc != 0 and "power-of-two" in msg

@@ -45,7 +45,6 @@ WORKLOAD = [
 ]
 METRIC = "batched C2C GFLOP/s (5N log2N), 1D fwd+bwd in-place orthogonal: c64 4096x16384, c64 13440x4096, c128 65536x512"
 UNIT = "GFLOP/s"
-DOMINANT = "c64_4096x16384"  # its plan is one kernel launch per execute
 
 
 def flops(lengths, batch):
@@ -67,6 +66,7 @@ def measured_peaks():
 
 
 def dram_traffic_record():
+    """DRAM bytes per launch from an ncu capture, summarised in profiles/dram_traffic.json."""
     p = os.path.join(ROOT, "profiles", "dram_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
@@ -137,7 +137,7 @@ def dist_env():
     return world, rank, local
 
 
-def cpu_baseline(sample_div: int = 16, repeats: int = 3):
+def cpu_baseline(sample_div: int = 2, repeats: int = 10):
     """Oracle (CPU restatement of the portable provider) on 1/sample_div of each batch."""
     import numpy as np
     from oracle import portable
@@ -316,19 +316,33 @@ def run_ours(args):
         per_plan[label] = {"fwd_ms": statistics.mean(fw), "bwd_ms": statistics.mean(bw),
                            "launches_per_execute": f.launches(),
                            "gbs_alg": nbytes / (statistics.mean(fw + bw) / 1e3) / 1e9}
-    dom_label = DOMINANT if DOMINANT in per_plan else plans[0][0]
-    dom = per_plan[dom_label]
-    dom_plan = [p for p in plans if p[0] == dom_label][0]
-    dom_bytes = 2 * math.prod(dom_plan[1]) * dom_plan[2] * (16 if dom_plan[3] else 8)
-    dom_ms = (dom["fwd_ms"] + dom["bwd_ms"]) / 2 / dom["launches_per_execute"]
+    # Dominant kernel: the launch with the largest device time per step. A plan with L
+    # launches per execute is split evenly over its L kernels (its passes move equal bytes).
     peak, peak_kind = measured_peaks()
-    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    step_ms = elapsed_ms / args.steps
+    kernels = []
+    for label, lengths, batch, dbl, f, b in plans:
+        pp = per_plan[label]
+        L = pp["launches_per_execute"]
+        launch_ms = (pp["fwd_ms"] + pp["bwd_ms"]) / 2 / L
+        nbytes = 2 * math.prod(lengths) * batch * (16 if dbl else 8)  # one launch reads + writes every element
+        kinds = [ps["kind"] for ps in f.describe()["passes"]]
+        for k in kinds:
+            kernels.append({"plan": label, "pass": k, "launch_ms": launch_ms, "bytes": nbytes,
+                            "share": 2 * launch_ms / step_ms,
+                            "gbs": nbytes / (launch_ms / 1e3) / 1e9})
+    dom = max(kernels, key=lambda k: k["launch_ms"])
     traffic = dram_traffic_record()
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                "kernel": f"fft_pass_kernel ({dom_label}, {dom['launches_per_execute']} launch(es) per execute)",
-                "alg_bytes_per_launch": dom_bytes,
-                "traffic": traffic.get("bytes_per_launch") if traffic else None}
+    tr = None
+    if traffic:
+        tr = traffic.get("kernels", {}).get(f"{dom['plan']}:{dom['pass']}")
+    roofline = {"bound": "hbm", "achieved": round(dom["gbs"], 1), "peak": peak, "unit": "GB/s",
+                "frac": round(dom["gbs"] / peak, 4), "peak_source": peak_kind,
+                "kernel": f"{dom['plan']} {dom['pass']} pass (largest device-time share, {dom['share']:.2f})",
+                "alg_bytes_per_launch": dom["bytes"], "launch_ms": round(dom["launch_ms"], 4),
+                "traffic": tr,
+                "kernels": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in kk.items()}
+                            for kk in kernels]}
 
     # e2e through the public API with pinned host buffers
     e2e = None
@@ -380,7 +394,7 @@ def run_ours(args):
                        "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
                        "parallelism": f"replicas x{world} (independent batches per GPU)",
                        "l2": "inputs larger than L2 (no flush)"},
-            "gbs_alg": round(alg_bytes_step * world / (elapsed_ms / 1e3) / 1e9, 1),
+            "gbs_alg": round(alg_bytes_step * world * args.steps / (elapsed_ms / 1e3) / 1e9, 1),
             "per_plan": per_plan,
             "roofline": roofline,
             "e2e": e2e,

@@ -1,0 +1,306 @@
+// The reference's portable-provider test program (tests/sycl_tests.cpp), restated for the
+// C++ front end of the B200 provider (include/syclfft_b200.hpp). Same cases, inputs,
+// direct-DFT oracles, tolerances and error-code checks; device buffers come from
+// cudaMalloc instead of SYCL USM, events are CUDA events. Needs a GPU; run by
+// tests/test_frontend.py. Exit status 0 = every check passed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../../include/syclfft_b200.hpp"
+
+namespace sf = syclfft_b200;
+
+namespace {
+
+void check(bool condition, const std::string& message) {
+    if (!condition) throw std::runtime_error(message);
+}
+
+sf::plan_options make_plan_options(sf::placement placement = sf::placement::out_of_place,
+                                   sf::normalization normalization = sf::normalization::none,
+                                   sf::provider provider = sf::provider::automatic) {
+    sf::plan_options o;
+    o.placement = placement;
+    o.normalization = normalization;
+    o.preferred_provider = provider;
+    return o;
+}
+
+template <class F>
+void expect_error(sf::error_code code, F&& fn) {
+    try {
+        fn();
+    } catch (const sf::exception& ex) {
+        check(ex.code() == code, std::string("wrong exception code: ") + ex.what());
+        return;
+    }
+    throw std::runtime_error("expected syclfft_b200::exception");
+}
+
+template <class T>
+class device_buffer {
+public:
+    explicit device_buffer(std::size_t count) : count_(count) {
+        if (cudaMalloc(&ptr_, count * sizeof(T)) != cudaSuccess) throw std::runtime_error("cudaMalloc failed");
+    }
+    ~device_buffer() { cudaFree(ptr_); }
+    device_buffer(const device_buffer&) = delete;
+    device_buffer& operator=(const device_buffer&) = delete;
+    T* get() const { return static_cast<T*>(ptr_); }
+    void write(const std::vector<T>& v) {
+        check(v.size() == count_, "upload size mismatch");
+        check(cudaMemcpy(ptr_, v.data(), count_ * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess, "upload");
+    }
+    std::vector<T> read() const {
+        std::vector<T> v(count_);
+        check(cudaMemcpy(v.data(), ptr_, count_ * sizeof(T), cudaMemcpyDeviceToHost) == cudaSuccess, "download");
+        return v;
+    }
+
+private:
+    std::size_t count_;
+    void* ptr_ = nullptr;
+};
+
+// sycl_tests.cpp:91-112
+template <class Scalar>
+std::vector<std::complex<Scalar>> direct_dft(const std::vector<std::complex<Scalar>>& input, sf::direction dir,
+                                             sf::normalization norm) {
+    const auto count = input.size();
+    std::vector<std::complex<Scalar>> output(count);
+    const auto sign = dir == sf::direction::forward ? Scalar{-1} : Scalar{1};
+    const auto pi = std::acos(Scalar{-1});
+    for (std::size_t k = 0; k < count; ++k)
+        for (std::size_t n = 0; n < count; ++n) {
+            const auto angle = sign * Scalar{2} * pi * static_cast<Scalar>(k * n) / static_cast<Scalar>(count);
+            output[k] += input[n] * std::complex<Scalar>{std::cos(angle), std::sin(angle)};
+        }
+    const auto scale = static_cast<Scalar>(sf::detail::normalization_scale(norm, dir, count));
+    for (auto& v : output) v *= scale;
+    return output;
+}
+
+// sycl_tests.cpp:115-151
+template <class Scalar>
+std::vector<std::complex<Scalar>> reference_many(std::vector<std::complex<Scalar>> values,
+                                                 const std::vector<std::size_t>& shape, std::size_t batch,
+                                                 sf::direction dir) {
+    std::size_t transform = 1;
+    for (auto n : shape) transform *= n;
+    const auto sign = dir == sf::direction::forward ? Scalar{-1} : Scalar{1};
+    const auto pi = std::acos(Scalar{-1});
+    for (std::size_t axis = 0; axis < shape.size(); ++axis) {
+        auto output = values;
+        std::size_t stride = 1;
+        for (std::size_t i = axis + 1; i < shape.size(); ++i) stride *= shape[i];
+        const auto length = shape[axis];
+        for (std::size_t b = 0; b < batch; ++b) {
+            const auto offset = b * transform;
+            for (std::size_t linear = 0; linear < transform; ++linear) {
+                const auto coordinate = (linear / stride) % length;
+                const auto base = linear - coordinate * stride;
+                std::complex<Scalar> sum{};
+                for (std::size_t k = 0; k < length; ++k) {
+                    const auto angle = sign * Scalar{2} * pi * static_cast<Scalar>(coordinate * k) /
+                                       static_cast<Scalar>(length);
+                    sum += values[offset + base + k * stride] * std::complex<Scalar>{std::cos(angle), std::sin(angle)};
+                }
+                output[offset + linear] = sum;
+            }
+        }
+        values = std::move(output);
+    }
+    return values;
+}
+
+template <class Scalar>
+void run_many(const std::vector<std::size_t>& shape, std::size_t batch) {
+    std::size_t count = batch;
+    for (auto n : shape) count *= n;
+    std::vector<std::complex<Scalar>> source(count);
+    for (std::size_t i = 0; i < count; ++i)
+        source[i] = {static_cast<Scalar>((i * 11 + 2) % 17) / Scalar{8}, static_cast<Scalar>((i * 3 + 1) % 13) / Scalar{7}};
+    const auto expected = reference_many(source, shape, batch, sf::direction::forward);
+    device_buffer<std::complex<Scalar>> input(count), output(count);
+    input.write(source);
+    auto fft = sf::plan_many_dft<Scalar>(sf::queue{}, shape, batch, sf::direction::forward,
+                                         make_plan_options(sf::placement::out_of_place, sf::normalization::none,
+                                                           sf::provider::b200));
+    fft.execute(input.get(), output.get()).wait_and_throw();
+    const auto actual = output.read();
+    const auto tol = std::is_same_v<Scalar, float> ? Scalar{8e-4} : Scalar{5e-11};
+    for (std::size_t i = 0; i < count; ++i)
+        check(std::abs(actual[i] - expected[i]) <= tol * (Scalar{1} + std::abs(expected[i])),
+              "multidimensional or batch mismatch at element " + std::to_string(i));
+}
+
+template <class Scalar>
+void run_1d(std::size_t count, sf::direction dir, sf::normalization norm, sf::placement pl) {
+    std::vector<std::complex<Scalar>> source(count);
+    for (std::size_t i = 0; i < count; ++i)
+        source[i] = {static_cast<Scalar>((i * 5 + 1) % 9) / Scalar{4}, static_cast<Scalar>((i * 3 + 2) % 7) / Scalar{5}};
+    const auto expected = direct_dft(source, dir, norm);
+    device_buffer<std::complex<Scalar>> input(count);
+    std::unique_ptr<device_buffer<std::complex<Scalar>>> out_storage, repeat_storage;
+    if (pl == sf::placement::out_of_place) {
+        out_storage = std::make_unique<device_buffer<std::complex<Scalar>>>(count);
+        repeat_storage = std::make_unique<device_buffer<std::complex<Scalar>>>(count);
+    }
+    input.write(source);
+    auto fft = sf::plan_dft_1d<Scalar>(sf::queue{}, count, dir, make_plan_options(pl, norm, sf::provider::b200));
+    auto dependency = sf::event::record(nullptr);
+    auto ev = pl == sf::placement::in_place ? fft.execute(input.get(), dependency)
+                                            : fft.execute(input.get(), out_storage->get(), dependency);
+    sf::event repeated;
+    if (repeat_storage) repeated = fft.execute(input.get(), repeat_storage->get());
+    ev.wait_and_throw();
+    repeated.wait_and_throw();
+    const auto actual = out_storage ? out_storage->read() : input.read();
+    const auto again = repeat_storage ? repeat_storage->read() : std::vector<std::complex<Scalar>>{};
+    const auto tol = std::is_same_v<Scalar, float> ? Scalar{4e-4} : Scalar{2e-11};
+    for (std::size_t i = 0; i < count; ++i) {
+        if (std::abs(actual[i] - expected[i]) > tol * (Scalar{1} + std::abs(expected[i])))
+            throw std::runtime_error("b200 mismatch at element " + std::to_string(i));
+        if (repeat_storage)
+            check(std::abs(again[i] - expected[i]) <= tol * (Scalar{1} + std::abs(expected[i])),
+                  "serialized repeated execution mismatch");
+    }
+    check(fft.selected_provider() == sf::provider::b200, "wrong provider");
+}
+
+}  // namespace
+
+int main()
+try {
+    static_assert(sizeof(sf::complex<float>) == 2 * sizeof(float));
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+        std::cerr << "no CUDA device\n";
+        return 2;
+    }
+    for (auto norm : {sf::normalization::none, sf::normalization::forward, sf::normalization::backward,
+                      sf::normalization::orthogonal})
+        run_1d<float>(8, sf::direction::forward, norm, sf::placement::out_of_place);
+    run_1d<float>(7, sf::direction::backward, sf::normalization::none, sf::placement::in_place);
+    run_1d<float>(6, sf::direction::forward, sf::normalization::none, sf::placement::out_of_place);
+    run_1d<float>(15, sf::direction::backward, sf::normalization::none, sf::placement::out_of_place);
+    run_1d<float>(35, sf::direction::forward, sf::normalization::none, sf::placement::out_of_place);
+    run_1d<float>(11, sf::direction::backward, sf::normalization::none, sf::placement::in_place);
+    run_many<float>({3, 4}, 2);
+    run_many<float>({2, 3, 5}, 1);
+    run_many<float>({11, 3}, 1);
+    run_1d<double>(11, sf::direction::forward, sf::normalization::orthogonal, sf::placement::out_of_place);
+
+    {  // sycl_tests.cpp:367-399: N=13 round trip chained by an event
+        device_buffer<std::complex<float>> input(13), spectrum(13), restored(13);
+        std::vector<std::complex<float>> source(13);
+        for (std::size_t i = 0; i < 13; ++i) source[i] = {static_cast<float>(i) / 7.0f, static_cast<float>(i % 3) / 5.0f};
+        input.write(source);
+        auto forward = sf::plan_dft_1d<float>(sf::queue{}, 13, sf::direction::forward);
+        auto backward = sf::plan_dft_1d<float>(sf::queue{}, 13, sf::direction::backward,
+                                               make_plan_options(sf::placement::out_of_place, sf::normalization::backward));
+        const auto forward_done = forward.execute(input.get(), spectrum.get());
+        backward.execute(spectrum.get(), restored.get(), forward_done).wait_and_throw();
+        const auto actual = restored.read();
+        for (std::size_t i = 0; i < 13; ++i) check(std::abs(actual[i] - source[i]) < 2e-3f, "round trip mismatch");
+    }
+
+    const auto providers = sf::query_providers(sf::queue{});
+    check(!providers.empty() && providers.front().available, "b200 provider unavailable");
+    {
+        auto automatic = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward);
+        check(automatic.selected_provider() == sf::provider::b200, "automatic selection did not pick b200");
+    }
+    {  // sycl_tests.cpp:410-435: two plans on two streams
+        device_buffer<std::complex<float>> ia(8), ib(8), oa(8), ob(8);
+        std::vector<std::complex<float>> sa(8), sb(8);
+        sa[0] = {1.0f, 0.0f};
+        sb[1] = {1.0f, 0.0f};
+        ia.write(sa);
+        ib.write(sb);
+        cudaStream_t s2;
+        check(cudaStreamCreate(&s2) == cudaSuccess, "stream");
+        auto first = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward);
+        auto second = sf::plan_dft_1d<float>(sf::queue{-1, reinterpret_cast<CUstream_st*>(s2)}, 8, sf::direction::forward);
+        auto d1 = first.execute(ia.get(), oa.get());
+        auto d2 = second.execute(ib.get(), ob.get());
+        d1.wait_and_throw();
+        d2.wait_and_throw();
+        const auto a = oa.read();
+        const auto b = ob.read();
+        check(std::abs(a[0].real() - 1.0f) < 1e-5f && std::abs(b[0].real() - 1.0f) < 1e-5f, "concurrent plans failed");
+        cudaStreamDestroy(s2);
+    }
+    {  // sycl_tests.cpp:437-449: memory the plan's device cannot see -> invalid_pointer
+        std::vector<std::complex<float>> host(8);
+        device_buffer<std::complex<float>> output(8);
+        expect_error(sf::error_code::invalid_pointer, [&] {
+            auto fft = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward);
+            fft.execute(host.data(), output.get());
+        });
+    }
+    {  // sycl_tests.cpp:483-506: two producers on another stream, the FFT waits on both events
+        device_buffer<std::complex<float>> input(8), output(8);
+        cudaStream_t producer;
+        check(cudaStreamCreate(&producer) == cudaSuccess, "stream");
+        std::vector<std::complex<float>> impulse(4);
+        impulse[0] = {1.0f, 0.0f};
+        cudaMemcpyAsync(input.get(), impulse.data(), 4 * sizeof(std::complex<float>), cudaMemcpyHostToDevice, producer);
+        auto first_half = sf::event::record(reinterpret_cast<CUstream_st*>(producer));
+        cudaMemsetAsync(input.get() + 4, 0, 4 * sizeof(std::complex<float>), producer);
+        auto second_half = sf::event::record(reinterpret_cast<CUstream_st*>(producer));
+        auto fft = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward);
+        fft.execute(input.get(), output.get(), std::vector<sf::event>{first_half, second_half}).wait_and_throw();
+        const auto actual = output.read();
+        for (std::size_t i = 0; i < 8; ++i)
+            check(std::abs(actual[i].real() - 1.0f) < 1e-5f && std::abs(actual[i].imag()) < 1e-5f,
+                  "event-span dependency ordering failed");
+        cudaStreamDestroy(producer);
+    }
+    // sycl_tests.cpp:508-538
+    expect_error(sf::error_code::provider_unavailable, [&] {
+        (void)sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward,
+                                     make_plan_options(sf::placement::out_of_place, sf::normalization::none,
+                                                       sf::provider::cufft));
+    });
+    expect_error(sf::error_code::invalid_argument,
+                 [&] { (void)sf::plan_dft_1d<float>(sf::queue{}, 8, static_cast<sf::direction>(0)); });
+    expect_error(sf::error_code::invalid_pointer, [&] {
+        auto fft = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward);
+        fft.execute(nullptr, nullptr);
+    });
+    expect_error(sf::error_code::invalid_argument, [&] {
+        auto fft = sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward,
+                                          make_plan_options(sf::placement::in_place));
+        device_buffer<std::complex<float>> a(8), b(8);
+        fft.execute(a.get(), b.get());
+    });
+    expect_error(sf::error_code::invalid_state, [&] {
+        auto original = sf::plan_dft_1d<float>(sf::queue{}, 4, sf::direction::forward);
+        auto moved = std::move(original);
+        (void)moved;
+        original.execute(nullptr, nullptr);  // NOLINT(bugprone-use-after-move)
+    });
+    // host_tests.cpp:167-195: planning errors
+    expect_error(sf::error_code::invalid_argument, [] { (void)sf::plan_dft_1d<float>(sf::queue{}, 0, sf::direction::forward); });
+    expect_error(sf::error_code::invalid_argument, [] {
+        (void)sf::plan_many_dft<float>(sf::queue{}, {static_cast<std::size_t>(-1), 2}, 1, sf::direction::forward);
+    });
+    expect_error(sf::error_code::invalid_argument,
+                 [] { (void)sf::plan_many_dft<float>(sf::queue{}, {2, 2, 2, 2}, 1, sf::direction::forward); });
+    std::cout << "front-end tests passed\n";
+    return 0;
+} catch (const std::exception& ex) {
+    std::cerr << "front-end tests failed: " << ex.what() << '\n';
+    return 1;
+}

@@ -253,6 +253,13 @@ def run_ours(args):
     opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal)
     plans, bufs, hosts = [], [], []
     workload = [w for w in WORKLOAD if not args.only or w[0] == args.only]
+    if args.plan:
+        # ad-hoc plans "N[xM[xK]]:batch:c64|c128", comma separated (profiling and tuning runs)
+        workload = []
+        for spec in args.plan.split(","):
+            shape, batch, kind = spec.split(":")
+            lengths = [int(v) for v in shape.split("x")]
+            workload.append((f"{kind}_{shape}x{batch}", lengths, int(batch), kind == "c128"))
     workload = [(l, s, max(1, b // args.batch_div), d) for l, s, b, d in workload]
     for label, lengths, batch, dbl in workload:
         n = math.prod(lengths)
@@ -379,7 +386,7 @@ def run_ours(args):
                "ms_per_step": e2e_ms / args.e2e_steps}
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu and not args.only and args.batch_div == 1:
+    if rank == 0 and world == 1 and not args.no_cpu and not args.only and not args.plan and args.batch_div == 1:
         cpu = cpu_baseline()
 
     if rank == 0:
@@ -390,6 +397,7 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (complex64, complex128)",
             "data": "synthetic (seeded uniform[-1,1) complex)",
             "config": {"workload": "config2_batched_c2c" if len(workload) == len(WORKLOAD) and args.batch_div == 1
+                       and not args.plan
                        else "subset", "plans": [f"{w[0]} (batch {w[2]})" for w in workload],
                        "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
                        "parallelism": f"replicas x{world} (independent batches per GPU)",
@@ -420,6 +428,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--only", default="", help="run one plan of the workload (profiling)")
     ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
+    ap.add_argument("--plan", default="", help="replace the workload: N[xM[xK]]:batch:c64|c128[,...]")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -94,6 +94,9 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void *plan, char *buf, 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
 /* Library version string. */
 SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
+/* Device status word of the plan: 0 = healthy; 1 = a kernel's bounded wait on an
+ * asynchronous copy gave up (the execution's output is incomplete). Synchronous. -1 on error. */
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void *plan);
 
 /* ---- Transform without device allocation (no counterpart in the reference). ----
  *

@@ -182,6 +182,21 @@ template <class T, class C> SFB_HD void bfly16(C* v) {
     t = v[11]; v[11] = v[14]; v[14] = t;
 }
 
+// u[r] *= w^r for r = 1..R-1, the powers formed by a balanced product tree
+// (w^r = w^h * w^(r-h), h the largest power of two <= r): at most log2(R)+1 roundings deep.
+template <int R, class C> SFB_HD void twiddle_powers(C* u, C w) {
+    C p[R > 1 ? R : 1];
+    p[0] = w;  // p[k] holds w^(k+1)
+#pragma unroll
+    for (int r = 2; r < R; ++r) {
+        int h = 1;
+        while (h * 2 <= r) h *= 2;
+        p[r - 1] = (h == r) ? cmul(p[h / 2 - 1], p[h / 2 - 1]) : cmul(p[h - 1], p[r - h - 1]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; ++r) u[r] = cmul(u[r], p[r - 1]);
+}
+
 template <int R, class T, class C> SFB_HD void dft(C* v) {
     if constexpr (R == 1) {
         (void)v;

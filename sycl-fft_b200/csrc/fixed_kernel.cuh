@@ -25,7 +25,7 @@ struct FixedParams {
     int64_t in_hi = 0, out_hi = 0;      // outer stride (kModeC)
     int64_t in_pitch = 0, out_pitch = 0;  // line pitch (kModeK)
     int64_t in_ks = 1, out_ks = 1;      // element stride (kModeC)
-    const void* tw = nullptr;           // concatenated per-stage twiddles [ns][R-1]
+    const void* tw = nullptr;           // base twiddles: per stage, W_(ns*R)^jm for jm < ns, concatenated
     int conj_in = 0, conj_out = 0;
     double scale = 1.0;
     // kFeatTw4 (kModeC column pass of a four-step): multiply output k of column c by
@@ -115,9 +115,8 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             C* u = &v[i * R];
             const int jm = j % NS;
             if constexpr (NS > 1 && R > 1) {
-                const C* twp = X.twb + TWOFF + jm * (R - 1);
-#pragma unroll
-                for (int r = 1; r < R; ++r) u[r] = cmul(u[r], __ldg(twp + (r - 1)));
+                // base-twiddle table: one W_(NS*R)^jm per butterfly, powers in registers
+                twiddle_powers<R>(u, __ldg(X.twb + TWOFF + jm));
             }
             dft<R, T>(u);
             if constexpr (LAST && FEAT == kFeatTStore) {
@@ -172,7 +171,7 @@ __device__ __forceinline__ void fixed_stages(FixedCtx<T>& X) {
     constexpr bool LAST = sizeof...(Rest) == 0;
     fixed_stage<T, N, TPL, MODEC, W, FEAT, NS, TWOFF, R, FIRST, LAST>(X);
     if constexpr (!LAST)
-        fixed_stages<T, N, TPL, MODEC, W, FEAT, NS * R, TWOFF + NS * (R - 1), false, Rest...>(X);
+        fixed_stages<T, N, TPL, MODEC, W, FEAT, NS * R, TWOFF + NS, false, Rest...>(X);
 }
 
 // Register budget: 64 per thread (16 float or 8 double complex values per stage).

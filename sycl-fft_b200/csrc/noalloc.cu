@@ -69,18 +69,16 @@ struct TableJob {
 // two-level four-step twiddle W_N^m = hi[m >> shift] * lo[m & (2^shift - 1)].
 __global__ void noalloc_fill_tables(const __grid_constant__ TableJob job, float2* tab) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // base twiddles of the size-specialised kernels: per stage, W_(ns*R)^jm for jm < ns
     auto stage_entry = [](int idx, const int* r, int nr, float2* out) -> bool {
         int ns = 1, off = 0;
         for (int s = 0; s < nr; ++s) {
             const int R = r[s];
-            const int cnt = ns * (R - 1);
-            if (idx < off + cnt) {
-                const int e = idx - off;
-                const int jm = e / (R - 1), rr = e % (R - 1) + 1;
-                *out = cis_neg_f(static_cast<long long>(rr) * jm, static_cast<long long>(ns) * R);
+            if (idx < off + ns) {
+                *out = cis_neg_f(idx - off, static_cast<long long>(ns) * R);
                 return true;
             }
-            off += cnt;
+            off += ns;
             ns *= R;
         }
         return false;
@@ -108,7 +106,7 @@ void set_error(char* err, size_t cap, const std::string& msg) {
 int stage_table_size(const FixedEntry& e) {
     int ns = 1, off = 0;
     for (int s = 0; s < e.nstages; ++s) {
-        off += ns * (e.radices[s] - 1);
+        off += ns;
         ns *= e.radices[s];
     }
     return off;

@@ -1,0 +1,149 @@
+// Persistent, copy-engine-pipelined pass kernel for long contiguous lines.
+//
+// For lines so long that one line fills most of a CTA's shared memory (float N=13440 is
+// 105 KB), only one CTA fits per SM and a plain kernel alternates load -> exchanges ->
+// store with the HBM idle during the exchanges. Here each CTA is persistent (one per SM)
+// and owns two buffers: a copy buffer, filled by the bulk-copy engine (cp.async.bulk,
+// completion on an mbarrier) with the next line as it is in HBM, and a padded work buffer
+// for the exchanges (the conflict-free layout of fixed_kernel.cuh). The first stage reads
+// the copy buffer into registers and writes the work buffer; right after it, the copy
+// engine is told to fetch the following line into the copy buffer, so that load hides
+// behind the remaining stages, and the last stage's stores drain during the next line.
+//
+// Waits on the copy are bounded: after kSpinLimit polls the CTA records a timeout in the
+// plan's status word and stops (all threads agree through a barrier first).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "butterfly.cuh"
+#include "fixed_kernel.cuh"
+
+namespace sfb {
+
+struct PipedParams {
+    int64_t lines = 0;
+    int64_t in_pitch = 0, out_pitch = 0;  // elements; pitch * sizeof(C) is a multiple of 16
+    const void* tw = nullptr;
+    int conj_in = 0, conj_out = 0;
+    double scale = 1.0;
+    int* status = nullptr;  // set to 1 if a copy wait timed out
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+constexpr long long kSpinLimit = 1ll << 26;
+constexpr int kCopyChunks = 4;
+
+// Stages 2..: the plain padded-layout stages of fixed_kernel.cuh.
+template <class T, int N, int TPL, int R0, int... Rest>
+__device__ __forceinline__ void piped_rest(FixedCtx<T>& X) {
+    if constexpr (sizeof...(Rest) > 0) fixed_stages<T, N, TPL, false, 1, kFeatPlain, R0, 1, false, Rest...>(X);
+}
+
+template <class T, int N, int TPL, int R0, int... Rest>
+__device__ __forceinline__ void piped_first(FixedCtx<T>& X) {
+    fixed_stage<T, N, TPL, false, 1, kFeatPlain, 1, 0, R0, true, sizeof...(Rest) == 0>(X);
+}
+
+// grid = min(lines, SMs); block = TPL threads;
+// dynamic smem = N * sizeof(C) (copy buffer) + kpitch<T,N>() * sizeof(C) (work buffer) + 16.
+template <class T, int N, int TPL, int MAXT, int... Rs>
+__global__ void __launch_bounds__(MAXT, 1)
+    fft_piped_kernel(const __grid_constant__ PipedParams P, const cplx<T>* in, cplx<T>* out) {
+    using C = cplx<T>;
+    static_assert((N * sizeof(C)) % (16 * kCopyChunks) == 0, "line must split into 16-byte multiples");
+    constexpr uint32_t kLineBytes = N * sizeof(C);
+    constexpr uint32_t kChunk = kLineBytes / kCopyChunks;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* const copy = reinterpret_cast<C*>(smem_raw);
+    C* const work = copy + N;
+    uint64_t* const bar = reinterpret_cast<uint64_t*>(smem_raw + kLineBytes + kpitch<T, N>() * sizeof(C));
+    const int t = threadIdx.x;
+
+    FixedCtx<T> X;
+    X.sm = work;
+    X.gin = copy;
+    X.twb = static_cast<const C*>(P.tw);
+    X.t = t;
+    X.active = t < TPL;
+    X.line_ok = true;
+    X.in_ks = 1;
+    X.out_ks = 1;
+    X.scale = static_cast<T>(P.scale);
+    X.conj_in = P.conj_in != 0;
+    X.conj_out = P.conj_out != 0;
+    X.sel = 0;
+
+    auto fetch = [&](int64_t line) {
+        mbar_expect_tx(bar, kLineBytes);
+        const unsigned char* src = reinterpret_cast<const unsigned char*>(in + line * P.in_pitch);
+#pragma unroll
+        for (int c = 0; c < kCopyChunks; ++c)
+            bulk_g2s(reinterpret_cast<unsigned char*>(copy) + c * kChunk, src + c * kChunk, kChunk, bar);
+    };
+    if (t == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (blockIdx.x < P.lines) fetch(blockIdx.x);
+    }
+    __syncthreads();
+
+    uint32_t parity = 0;
+    for (int64_t line = blockIdx.x; line < P.lines; line += gridDim.x) {
+        bool ok = false;
+        for (long long spin = 0; spin < kSpinLimit; ++spin) {
+            if (mbar_try_wait(bar, parity)) {
+                ok = true;
+                break;
+            }
+        }
+        if (__syncthreads_or(!ok)) {
+            if (t == 0 && P.status) atomicExch(P.status, 1);
+            return;  // the only copy in flight is the one that never completed
+        }
+        parity ^= 1u;
+        X.gout = out + line * P.out_pitch;
+        piped_first<T, N, TPL, Rs...>(X);  // ends with a barrier: the copy buffer is consumed
+        const int64_t next = line + gridDim.x;
+        if (t == 0 && next < P.lines) {
+            fence_proxy_async();  // order the generic reads of the copy buffer before the copy
+            fetch(next);
+        }
+        piped_rest<T, N, TPL, Rs...>(X);
+        __syncthreads();  // the work buffer is free for the next line's first stage
+    }
+}
+
+}  // namespace sfb

@@ -2,6 +2,7 @@
 
 #include "cluster_catalog.h"
 #include "fixed_catalog.h"
+#include "piped_catalog.h"
 
 #include <algorithm>
 #include <cmath>
@@ -129,6 +130,30 @@ struct Builder {
         return s;
     }
 
+    // Base-twiddle table of the size-specialised kernels: for each stage, W_(ns*R)^jm, jm < ns.
+    int base_table(const std::vector<int>& radices) {
+        std::vector<int> key = radices;
+        key.push_back(-1);  // distinct from the full-table key
+        auto it = seq_tables.find(key);
+        if (it != seq_tables.end()) return it->second;
+        std::vector<std::complex<double>> tw;
+        int64_t ns = 1;
+        for (int R : radices) {
+            for (int64_t jm = 0; jm < ns; ++jm) tw.push_back(cis_neg(jm, ns * R));
+            ns *= R;
+        }
+        if (tw.empty()) tw.push_back(1.0);
+        const int id = add_table(std::move(tw));
+        seq_tables[key] = id;
+        return id;
+    }
+
+    void use_base_table(PassSpec& ps) {
+        std::vector<int> r(ps.p.fft1.radix, ps.p.fft1.radix + ps.p.fft1.nstages);
+        ps.tables.tw1 = base_table(r);
+        ps.tw_base = true;
+    }
+
     void add_tw4(PassSpec& ps, int64_t ntot, int sign) {
         int shift = 0;
         while ((int64_t(1) << (2 * shift)) < ntot) ++shift;  // 2^shift >= sqrt(ntot)
@@ -207,6 +232,14 @@ struct Builder {
         ps.kc.maxt = e->maxt;
         ps.fixed_id = e->id;
         ps.fixed_feat = kFixedPlain;
+        use_base_table(ps);
+        if (p.mode == kModeK && !req.no_piped && (p.in.cs * cs) % 16 == 0 && (p.out.cs * cs) % 16 == 0) {
+            if (const PipedEntry* pe = find_piped(req.dbl, p.n)) {
+                bool same = pe->nstages == p.fft1.nstages;
+                for (int i = 0; same && i < pe->nstages; ++i) same = pe->radices[i] == p.fft1.radix[i];
+                if (same) ps.piped_id = pe->id;
+            }
+        }
     }
 
     // Four-step passes of a contiguous axis on their size-specialised kernels.
@@ -246,6 +279,7 @@ struct Builder {
         ps.kc.maxt = e->maxt;
         ps.fixed_id = e->id;
         ps.fixed_feat = feat;
+        use_base_table(ps);
     }
 
     bool fits(int64_t n, int mode) {
@@ -751,6 +785,16 @@ const ClusterEntry* find_cluster(bool dbl, int64_t n, int prefer_p) {
     return first;
 }
 
+#define SFB_PENTRY(ID, DBL, N, TPL, MAXT, ...) PipedEntry{ID, DBL, N, TPL, MAXT, {__VA_ARGS__}, count_args(__VA_ARGS__)},
+const PipedEntry kPiped[] = {SFB_PIPED_CATALOG(SFB_PENTRY)};
+#undef SFB_PENTRY
+
+const PipedEntry* find_piped(bool dbl, int n) {
+    for (const PipedEntry& e : kPiped)
+        if (e.dbl == (dbl ? 1 : 0) && e.n == n) return &e;
+    return nullptr;
+}
+
 const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
     for (const FixedEntry& e : kFixed)
         if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n && e.feat == feat) return &e;
@@ -799,7 +843,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
-           << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ",\"piped_id\":" << ps.piped_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
            << ps.cl_p << "]}";
     }
     os << "]}";

@@ -49,7 +49,10 @@ struct PassSpec {
     int64_t bytes_moved = 0; // HBM bytes this pass reads + writes (data, not tables)
     int fixed_id = -1;       // size-specialised kernel (fixed_catalog.h), -1 = generic kernel
     int fixed_feat = 0;      // its feature (kFixedPlain / kFixedTw4 / kFixedTStore)
+    bool tw_base = false;    // tables.tw1 holds base twiddles W_(ns*R)^jm (size-specialised kernels)
     int cluster_id = -1;     // cluster kernel (cluster_catalog.h) for a whole long line
+    int piped_id = -1;       // copy-engine-pipelined kernel (piped_catalog.h), used when the
+                             // buffers are 16-byte aligned; otherwise fixed_id runs
     int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
 };
 
@@ -71,6 +74,14 @@ struct FixedEntry {
 };
 const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat);
 
+// One entry of piped_catalog.h as seen by the host.
+struct PipedEntry {
+    int id, dbl, n, tpl, maxt;
+    int radices[kMaxStages];
+    int nstages;
+};
+const PipedEntry* find_piped(bool dbl, int n);
+
 struct PlanRequest {
     bool dbl = false;
     int direction = -1;      // -1 forward, +1 backward
@@ -84,6 +95,7 @@ struct PlanRequest {
     int smem_limit = 0;      // bytes, 0 = device default (227 KB)
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
     bool no_cluster = false; // force the two-pass four-step for long lines
+    bool no_piped = false;   // never use the copy-engine-pipelined kernels
     int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size
 };
 

@@ -21,6 +21,7 @@
 #include "cluster_launch.hpp"
 #include "fixed_launch.hpp"
 #include "launch.hpp"
+#include "piped_launch.hpp"
 #include "planner.hpp"
 
 namespace sfb {
@@ -65,7 +66,21 @@ struct BoundPass {
     PassSpec spec;
     FixedParams fp;    // used when spec.fixed_id >= 0
     ClusterParams cp;  // used when spec.cluster_id >= 0
+    PipedParams pp;    // used when spec.piped_id >= 0 and the buffers are 16-byte aligned
 };
+
+PipedParams to_piped(const PassParams& p, int* status) {
+    PipedParams q;
+    q.lines = p.n_cols;
+    q.in_pitch = p.in.cs;
+    q.out_pitch = p.out.cs;
+    q.tw = p.fft1.tw;
+    q.conj_in = p.conj_in;
+    q.conj_out = p.conj_out;
+    q.scale = p.scale;
+    q.status = status;
+    return q;
+}
 
 ClusterParams to_cluster(const PassParams& p) {
     ClusterParams c;
@@ -111,6 +126,8 @@ struct DevicePlan {
     int device = 0;
     void* table_mem = nullptr;
     void* scratch = nullptr;
+    int* status = nullptr;  // device word: non-zero after a bounded wait in a kernel timed out
+    int sms = 148;
     std::vector<BoundPass> passes;
     cudaEvent_t done = nullptr;
     std::mutex mu;
@@ -152,6 +169,8 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
+    // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
+    if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
     // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
     if (const char* k = std::getenv("SYCLFFT_B200_CLUSTER")) {
         if (std::strcmp(k, "off") == 0) req.no_cluster = true;
@@ -177,13 +196,17 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         offsets[i] = total;
         total += (plan->spec.tables[i].size() * cs + 255) / 256 * 256;
     }
-    std::vector<unsigned char> blob(std::max<size_t>(total, 256), 0);
+    const size_t status_off = total;
+    total += 256;  // status word(s), zero-initialised with the tables
+    std::vector<unsigned char> blob(total, 0);
     for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
         if (req.dbl) pack_table<double>(plan->spec.tables[i], blob, offsets[i]);
         else pack_table<float>(plan->spec.tables[i], blob, offsets[i]);
     }
     check(cudaMalloc(&plan->table_mem, blob.size()), "cudaMalloc(tables)");
     check(cudaMemcpy(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
+    plan->status = reinterpret_cast<int*>(static_cast<unsigned char*>(plan->table_mem) + status_off);
+    check(cudaDeviceGetAttribute(&plan->sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     if (plan->spec.scratch_elements) {
         check(cudaMalloc(&plan->scratch, plan->spec.scratch_elements * cs), "cudaMalloc(scratch)");
     }
@@ -207,6 +230,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         bp.p.tw4_lo = tab(ps.tables.tw4_lo);
         bp.fp = to_fixed(bp.p);
         bp.cp = to_cluster(bp.p);
+        bp.pp = to_piped(bp.p, plan->status);
         plan->passes.push_back(bp);
     }
     return plan.release();
@@ -225,7 +249,14 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
             if (b == Buf::Output) return out;
             return plan->scratch;
         };
-        if (bp.spec.cluster_id >= 0) {
+        const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec.src)) % 16 == 0) &&
+                             (reinterpret_cast<uintptr_t>(buf(bp.spec.dst)) % 16 == 0);
+        if (bp.spec.piped_id >= 0 && aligned) {
+            const int64_t lines = bp.pp.lines;
+            const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
+            check(launch_piped(bp.spec.piped_id, bp.pp, grid, buf(bp.spec.src), buf(bp.spec.dst), stream),
+                  "FFT pipelined pass launch");
+        } else if (bp.spec.cluster_id >= 0) {
             check(launch_cluster(bp.spec.cluster_id, bp.cp, buf(bp.spec.src), buf(bp.spec.dst), stream),
                   "FFT cluster pass launch");
         } else if (bp.spec.fixed_id >= 0) {
@@ -310,3 +341,15 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
 }
 
 SYCLFFT_B200_EXPORT const char* syclfft_b200_version(void) { return "syclfft-b200 0.1"; }
+
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void* plan) {
+    const auto* p = static_cast<const sfb::DevicePlan*>(plan);
+    if (!p || !p->status) return -1;
+    int value = 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != p->device) cudaSetDevice(p->device);
+    const cudaError_t e = cudaMemcpy(&value, p->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (prev != p->device) cudaSetDevice(prev);
+    return e == cudaSuccess ? value : -1;
+}

@@ -62,6 +62,7 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_describe_plan",
     "syclfft_b200_plan_launches",
     "syclfft_b200_version",
+    "syclfft_b200_plan_status",
     "syclfft_b200_execute_noalloc_c2c_f32",
 )
 
@@ -85,6 +86,8 @@ def load(path: str | None = None):
     lib.syclfft_b200_plan_launches.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_version.restype = ctypes.c_char_p
     lib.syclfft_b200_version.argtypes = []
+    lib.syclfft_b200_plan_status.restype = ctypes.c_int
+    lib.syclfft_b200_plan_status.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_execute_noalloc_c2c_f32.restype = ctypes.c_int
     lib.syclfft_b200_execute_noalloc_c2c_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                          ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32,

@@ -24,8 +24,11 @@ int64_t line_base(const LineLayout& L, int64_t o, int64_t c) {
     return (L.d == 1 ? o * L.hi : (o / L.d) * L.hi + (o % L.d) * L.lo) + c * L.cs;
 }
 
-void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, int n) {
+// base == true: the table holds, per stage, W_(Ns*R)^jm (size-specialised kernels), and the
+// stage twiddle W^(r*jm) is its r-th power; otherwise the full [Ns][R-1] layout at tw_off.
+void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, int n, bool base = false) {
     std::vector<cd> y(n);
+    int64_t boff = 0;
     for (int s = 0; s < S.nstages; ++s) {
         const int R = S.radix[s], Ns = S.ns[s], nr = n / R;
         for (int j = 0; j < nr; ++j) {
@@ -33,7 +36,7 @@ void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, 
             cd v[16], u[16];
             for (int r = 0; r < R; ++r) {
                 v[r] = x[j + r * nr];
-                if (r > 0 && Ns > 1) v[r] *= tw[S.tw_off[s] + jm * (R - 1) + (r - 1)];
+                if (r > 0 && Ns > 1) v[r] *= base ? std::pow(tw[boff + jm], r) : tw[S.tw_off[s] + jm * (R - 1) + (r - 1)];
             }
             for (int p = 0; p < R; ++p) {
                 cd acc = 0.0;
@@ -44,6 +47,7 @@ void stockham(std::vector<cd>& x, const StageSeq& S, const std::vector<cd>& tw, 
             for (int r = 0; r < R; ++r) y[base + r * Ns] = u[r];
         }
         x.swap(y);
+        boff += Ns;
     }
 }
 
@@ -116,7 +120,7 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
     }
     for (auto& L : lines) {
         const int64_t sel = p.sel_mode == kSelCol ? L.c : (p.sel_mode == kSelOuterLo ? L.o % p.sel_d : 0);
-        stockham(L.v, p.fft1, plan.tables[ps.tables.tw1], p.n);
+        stockham(L.v, p.fft1, plan.tables[ps.tables.tw1], p.n, ps.tw_base);
         if (p.fft2.nstages > 0) {
             for (int k = 0; k < p.n; ++k) {
                 if (pointwise) L.v[k] *= (*pointwise)[k + sel * p.pw_stride];

@@ -204,6 +204,39 @@ def test_generic_kernel_path(sf, torch, oracle_mod, shape, batch, dbl, monkeypat
     assert rel_l2(out, fp64_fft(x, shape, batch, 1, 1.0 / n)) <= spec_tol(n, dbl)
 
 
+@pytest.mark.parametrize("piped", ["1", "0"])
+@pytest.mark.parametrize("shape,batch,dbl", [([13440], 300, False), ([8192], 200, False), ([13440], 3, False)],
+                         ids=lambda v: str(v))
+def test_pipelined_kernel(sf, torch, shape, batch, dbl, piped, monkeypatch):
+    """Persistent copy-engine-pipelined kernel (many lines per CTA) vs the plain kernel, both
+    directions, in place and out of place, with unaligned buffers falling back to the plain kernel."""
+    monkeypatch.setenv("SYCLFFT_B200_PIPED", piped)
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 31 + n, dt)
+    for d, norm in ((-1, 3), (1, 1)):
+        out, p = run(sf, torch, x, shape, batch, d, norm, dbl)
+        ids = [ps["piped_id"] for ps in p.describe()["passes"]]
+        assert (ids[0] >= 0) == (piped == "1"), ids
+        assert rel_l2(out, fp64_fft(x, shape, batch, d, norm_scale(norm, d, n))) <= spec_tol(n, dbl)
+    out, _ = run(sf, torch, x, shape, batch, -1, 0, dbl, in_place=True)
+    assert rel_l2(out, fp64_fft(x, shape, batch, -1)) <= spec_tol(n, dbl)
+    # 8-byte-aligned (not 16) buffers: the provider must take the plain kernel
+    xt = torch.from_numpy(np.concatenate([np.zeros(1, dt), x])).cuda()
+    yt = torch.empty_like(xt)
+    p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)
+    from syclfft_b200 import _provider
+    import ctypes
+    err = ctypes.create_string_buffer(1024)
+    es = xt.element_size()
+    rc = p._api.execute(p._handle, xt.data_ptr() + es, yt.data_ptr() + es, torch.cuda.current_stream().cuda_stream,
+                        err, 1024)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    assert rel_l2(yt[1:].cpu().numpy(), fp64_fft(x, shape, batch, -1)) <= spec_tol(n, dbl)
+    assert p._lib.syclfft_b200_plan_status(p._handle) == 0
+
+
 def test_in_place_multi_axis(sf, torch):
     x = uniform_complex(2 * 12 * 40 * 9, 3)
     out, _ = run(sf, torch, x.copy(), [12, 40, 9], 2, -1, 0, False, in_place=True)

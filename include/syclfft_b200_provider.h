@@ -94,9 +94,38 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void *plan, char *buf, 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
 /* Library version string. */
 SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
+/* Like execute, for the first `batch` transforms only (1 <= batch <= the plan's
+ * batch_count): a plan made for up to B transforms serves any smaller batch with the same
+ * resident tables and scratch. */
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_batch(void *plan, const void *in, void *out, uint64_t batch,
+                                                   void *stream, char *err, size_t cap);
 /* Device status word of the plan: 0 = healthy; 1 = a kernel's bounded wait on an
  * asynchronous copy gave up (the execution's output is incomplete). Synchronous. -1 on error. */
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void *plan);
+
+/* ---- Grouped execution (no reference counterpart): the serving path's batched launch. ----
+ *
+ * A group serves one length family: 1-D C2C transforms of length n and one precision over
+ * contiguous lines. One execute runs many requests -- each with its own buffers, batch
+ * count, direction and normalization -- in a single kernel launch (up to 192 requests per
+ * launch; more are split). The request table is passed as kernel parameters, so executes
+ * are stream-ordered, need no device staging and can be captured in a CUDA graph.
+ * Available for the lengths of the size-specialised single-pass kernels
+ * (syclfft_b200_group_supports). in == out is allowed per request. */
+typedef struct syclfft_b200_group_item_v1 {
+    const void *in;
+    void *out;
+    uint64_t batch;          /* lines of length n */
+    int32_t direction;       /* -1 / +1 */
+    uint32_t normalization;  /* SYCLFFT_B200_NORM_* */
+} syclfft_b200_group_item_v1;
+
+SYCLFFT_B200_EXPORT int syclfft_b200_group_supports(uint32_t scalar, uint64_t n);
+SYCLFFT_B200_EXPORT void *syclfft_b200_group_create(uint32_t scalar, uint64_t n, int32_t device, char *err,
+                                                    size_t cap);
+SYCLFFT_B200_EXPORT int syclfft_b200_group_execute(void *group, const syclfft_b200_group_item_v1 *items,
+                                                   uint32_t count, void *stream, char *err, size_t cap);
+SYCLFFT_B200_EXPORT void syclfft_b200_group_destroy(void *group);
 
 /* ---- Transform without device allocation (no counterpart in the reference). ----
  *

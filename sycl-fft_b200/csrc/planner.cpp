@@ -425,16 +425,18 @@ struct Builder {
         const int64_t M = static_cast<int64_t>(bluestein_length(static_cast<uint64_t>(L)));
         const int sgn = req.direction;  // -1 forward, +1 backward
         std::vector<std::complex<double>> chirp(L), kern(M, 0.0);
-        for (int64_t n = 0; n < L; ++n) {
-            const uint64_t r = (static_cast<unsigned __int128>(n) * n) % static_cast<uint64_t>(2 * L);
-            // h_n = exp(-i*sgn*pi*r/L) = exp(-2 pi i * (sgn*r) / (2L))
-            const std::complex<double> h = cis_neg(sgn * static_cast<int64_t>(r), 2 * L);
-            kern[n] = h;
-            if (n) kern[M - n] = h;
-            chirp[n] = std::conj(h);
+        if (!req.device_spectrum) {
+            for (int64_t n = 0; n < L; ++n) {
+                const uint64_t r = (static_cast<unsigned __int128>(n) * n) % static_cast<uint64_t>(2 * L);
+                // h_n = exp(-i*sgn*pi*r/L) = exp(-2 pi i * (sgn*r) / (2L))
+                const std::complex<double> h = cis_neg(sgn * static_cast<int64_t>(r), 2 * L);
+                kern[n] = h;
+                if (n) kern[M - n] = h;
+                chirp[n] = std::conj(h);
+            }
+            host_fft_fp64(kern, -1);
+            for (auto& v : kern) v /= static_cast<double>(M);
         }
-        host_fft_fp64(kern, -1);
-        for (auto& v : kern) v /= static_cast<double>(M);
         const int chirp_id = add_table(std::move(chirp));
         const int mode = s == 1 ? kModeK : kModeC;
         if (fits(M, mode)) {
@@ -456,6 +458,15 @@ struct Builder {
             ps.tables.premul = chirp_id;
             ps.tables.postmul = chirp_id;
             ps.tables.pointwise = add_table(std::move(kern));
+            if (req.device_spectrum) {
+                BluesteinJob job;
+                job.L = L;
+                job.M = M;
+                job.sgn = sgn;
+                job.chirp_table = chirp_id;
+                job.spectrum_table = ps.tables.pointwise;
+                plan.bluestein_jobs.push_back(job);
+            }
             p.conj_mid = 1;
             p.conj_out = 1;
             SingleCfg cfg = single_cfg(M, req.dbl, req.force_maxv);
@@ -473,9 +484,23 @@ struct Builder {
         if (!split(M, n1, n2)) throw std::runtime_error("Bluestein length too large for this provider");
         // K'[k1*N2 + k2] = K[k1 + N1*k2]
         std::vector<std::complex<double>> kp(M);
-        for (int64_t k1 = 0; k1 < n1; ++k1)
-            for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = kern[k1 + n1 * k2];
+        if (!req.device_spectrum) {
+            for (int64_t k1 = 0; k1 < n1; ++k1)
+                for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = kern[k1 + n1 * k2];
+        }
         const int kp_id = add_table(std::move(kp));
+        if (req.device_spectrum) {
+            BluesteinJob job;
+            job.L = L;
+            job.M = M;
+            job.n1 = n1;
+            job.n2 = n2;
+            job.sgn = sgn;
+            job.large = true;
+            job.chirp_table = chirp_id;
+            job.spectrum_table = kp_id;
+            plan.bluestein_jobs.push_back(job);
+        }
         const int64_t lines = E / L;
         plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(lines * M));
         // pass 1: columns of the zero-padded, chirp-multiplied line
@@ -718,10 +743,30 @@ int threads_per_line(int n, const std::vector<int>& radices, int maxv) {
 }
 
 std::complex<double> cis_neg(int64_t num, int64_t den) {
+    // exp(-2 pi i m / den) with the argument reduced to |x| <= 1/4 turn-halves by symmetry:
+    // x = 2m/den in [0, 2) -> [-1, 1) -> quadrant folding, so cos/sin see |angle| <= pi/4.
     int64_t m = num % den;
     if (m < 0) m += den;
-    const long double a = two_pi_l() * static_cast<long double>(m) / static_cast<long double>(den);
-    return {static_cast<double>(std::cos(a)), static_cast<double>(-std::sin(a))};
+    // work in units of 1/(4 den) of a half-turn: t = 8m / den eighths
+    const int64_t m8 = 8 * m;
+    const int64_t oct = m8 / den;                      // 0..7 octant of the full turn
+    const int64_t rem = m8 - oct * den;                // remainder in [0, den)
+    const double f = static_cast<double>(rem) / static_cast<double>(den);  // [0,1) of an octant
+    const double pi4 = 0.78539816339744830961566084581987572;
+    double c, sn;
+    // angle within the octant pair: theta = (oct + f) * pi/4
+    switch (oct) {
+        case 0: c = std::cos(f * pi4); sn = std::sin(f * pi4); break;
+        case 1: c = std::sin((1 - f) * pi4); sn = std::cos((1 - f) * pi4); break;
+        case 2: c = -std::sin(f * pi4); sn = std::cos(f * pi4); break;
+        case 3: c = -std::cos((1 - f) * pi4); sn = std::sin((1 - f) * pi4); break;
+        case 4: c = -std::cos(f * pi4); sn = -std::sin(f * pi4); break;
+        case 5: c = -std::sin((1 - f) * pi4); sn = -std::cos((1 - f) * pi4); break;
+        case 6: c = std::sin(f * pi4); sn = -std::cos(f * pi4); break;
+        default: c = std::cos((1 - f) * pi4); sn = -std::sin((1 - f) * pi4); break;
+    }
+    (void)two_pi_l;
+    return {c, -sn};
 }
 
 void host_fft_fp64(std::vector<std::complex<double>>& a, int sign) {
@@ -824,6 +869,14 @@ PlanSpec make_plan(const PlanRequest& req) {
     }
     if (plan.passes.empty()) b.copy_pass(cur);
     plan.passes.back().p.scale = plan.scale;
+    // The batch is the outermost index of every pass: the pass's outer count when it has
+    // one (n_outer > 1 or strided columns), else its line count.
+    for (auto& ps : plan.passes) {
+        const bool outer = ps.p.n_outer > 1 || (ps.p.n_outer == 1 && ps.p.mode == kModeC && req.batch == 1);
+        ps.batch_dim = outer ? 0 : 1;
+        const int64_t v = ps.batch_dim == 0 ? ps.p.n_outer : ps.p.n_cols;
+        if (v % static_cast<int64_t>(req.batch) != 0) ps.batch_dim = -1;  // cannot rescale
+    }
     return plan;
 }
 

@@ -50,6 +50,9 @@ struct PassSpec {
     int fixed_id = -1;       // size-specialised kernel (fixed_catalog.h), -1 = generic kernel
     int fixed_feat = 0;      // its feature (kFixedPlain / kFixedTw4 / kFixedTStore)
     bool tw_base = false;    // tables.tw1 holds base twiddles W_(ns*R)^jm (size-specialised kernels)
+    // Which line count is proportional to the plan's batch: 0 = n_outer, 1 = n_cols
+    // (lets a plan for up to B transforms run the first b <= B).
+    int batch_dim = 1;
     int cluster_id = -1;     // cluster kernel (cluster_catalog.h) for a whole long line
     int piped_id = -1;       // copy-engine-pipelined kernel (piped_catalog.h), used when the
                              // buffers are 16-byte aligned; otherwise fixed_id runs
@@ -97,10 +100,22 @@ struct PlanRequest {
     bool no_cluster = false; // force the two-pass four-step for long lines
     bool no_piped = false;   // never use the copy-engine-pipelined kernels
     int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size
+    bool device_spectrum = false;  // leave Bluestein chirp/spectrum tables to the device (zeroed here)
+};
+
+// A Bluestein axis whose chirp and chirp spectrum the provider generates on the device
+// (PlanRequest::device_spectrum): chirp[n] = conj(h_n), h_n = exp(-i*sgn*pi*(n^2 mod 2L)/L),
+// spectrum = FFT_M(h zero-padded, mirrored) / M, permuted K'[k1*n2+k2] = K[k1+n1*k2] when large.
+struct BluesteinJob {
+    int64_t L = 0, M = 0, n1 = 0, n2 = 0;
+    int sgn = -1;
+    bool large = false;
+    int chirp_table = -1, spectrum_table = -1;
 };
 
 struct PlanSpec {
     PlanRequest req;
+    std::vector<BluesteinJob> bluestein_jobs;
     uint64_t elements = 0, transform_size = 0;
     double scale = 1.0;
     std::vector<std::vector<std::complex<double>>> tables;

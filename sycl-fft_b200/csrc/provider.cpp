@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -18,6 +19,7 @@
 #include <vector>
 
 #include "../../include/syclfft_b200_provider.h"
+#include "bluestein_init.hpp"
 #include "cluster_launch.hpp"
 #include "fixed_launch.hpp"
 #include "launch.hpp"
@@ -154,6 +156,30 @@ void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned
     }
 }
 
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg);
+void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch);
+
+// FP64 forward in-place FFT plans of length M used to make chirp spectra; kept for the process.
+DevicePlan* spectrum_plan(int device, int64_t M) {
+    static std::mutex mu;
+    static std::map<std::pair<int, int64_t>, DevicePlan*> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({device, M});
+    if (it != cache.end()) return it->second;
+    syclfft_b200_plan_config_v1 c{};
+    c.abi_version = SYCLFFT_B200_PROVIDER_ABI_VERSION;
+    c.scalar = SYCLFFT_B200_SCALAR_DOUBLE;
+    c.direction = -1;
+    c.rank = 1;
+    c.lengths[0] = static_cast<uint64_t>(M);
+    c.batch_count = 1;
+    c.in_place = 1;
+    c.device = device;
+    DevicePlan* p = create_plan(c);
+    cache[{device, M}] = p;
+    return p;
+}
+
 DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     if (cfg.abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION) throw std::runtime_error("B200 provider ABI mismatch");
     if (cfg.scalar != SYCLFFT_B200_SCALAR_FLOAT && cfg.scalar != SYCLFFT_B200_SCALAR_DOUBLE)
@@ -183,6 +209,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     int smem_optin = 0;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "cudaDeviceGetAttribute");
     req.smem_limit = smem_optin;
+    req.device_spectrum = true;
 
     auto plan = std::make_unique<DevicePlan>();
     plan->device = device;
@@ -211,6 +238,27 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         check(cudaMalloc(&plan->scratch, plan->spec.scratch_elements * cs), "cudaMalloc(scratch)");
     }
     check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+    if (!plan->spec.bluestein_jobs.empty()) {
+        // chirps and chirp spectra on the device: exact-integer chirp, FP64 FFT of length M
+        int64_t maxM = 0;
+        for (const auto& j : plan->spec.bluestein_jobs) maxM = std::max(maxM, j.M);
+        void* kern = nullptr;
+        check(cudaMalloc(&kern, static_cast<size_t>(maxM) * 16), "cudaMalloc(chirp kernel)");
+        try {
+            for (const auto& j : plan->spec.bluestein_jobs) {
+                void* chirp = static_cast<unsigned char*>(plan->table_mem) + offsets[j.chirp_table];
+                void* spec = static_cast<unsigned char*>(plan->table_mem) + offsets[j.spectrum_table];
+                check(bluestein_chirp(req.dbl, chirp, kern, j.L, j.M, j.sgn, nullptr), "chirp kernel");
+                execute_plan(spectrum_plan(device, j.M), kern, kern, nullptr, 0);
+                check(bluestein_spectrum(req.dbl, spec, kern, j.M, j.n1, j.n2, j.large, nullptr), "spectrum kernel");
+            }
+            check(cudaStreamSynchronize(nullptr), "chirp spectrum");
+        } catch (...) {
+            cudaFree(kern);
+            throw;
+        }
+        cudaFree(kern);
+    }
 
     auto tab = [&](int id) -> const void* {
         return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
@@ -236,14 +284,37 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     return plan.release();
 }
 
-void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream) {
+// Line counts of a pass for the first `batch` transforms of a plan made for `planned`.
+BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
+    if (batch == planned) return bp;
+    if (bp.spec.batch_dim < 0) throw std::invalid_argument("plan cannot run a smaller batch");
+    BoundPass r = bp;
+    PassParams& p = r.p;
+    const int64_t b = static_cast<int64_t>(batch), B = static_cast<int64_t>(planned);
+    if (bp.spec.batch_dim == 0) p.n_outer = p.n_outer / B * b;
+    else p.n_cols = p.n_cols / B * b;
+    p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+    p.tiles = p.n_outer * p.col_tiles;
+    r.fp.n_cols = p.n_cols;
+    r.fp.col_tiles = p.col_tiles;
+    r.cp.lines = p.n_cols;
+    r.pp.lines = p.n_cols;
+    if (bp.spec.cluster_id >= 0) p.tiles = p.n_cols * bp.spec.cl_p;
+    return r;
+}
+
+void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch = 0) {
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
+    const uint64_t planned = plan->spec.req.batch;
+    if (batch == 0) batch = planned;
+    if (batch > planned) throw std::invalid_argument("batch exceeds the plan's batch count");
     const bool in_place = plan->spec.req.in_place;
     if (in_place && in != out) throw std::invalid_argument("In-place plan must be executed with in == out");
     if (!in_place && in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
     std::lock_guard<std::mutex> lock(plan->mu);
     DeviceGuard guard(plan->device);
-    for (const BoundPass& bp : plan->passes) {
+    for (const BoundPass& planned_pass : plan->passes) {
+        const BoundPass bp = rescale(planned_pass, batch, planned);
         auto buf = [&](Buf b) -> void* {
             if (b == Buf::Input) return const_cast<void*>(in);
             if (b == Buf::Output) return out;
@@ -341,6 +412,18 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
 }
 
 SYCLFFT_B200_EXPORT const char* syclfft_b200_version(void) { return "syclfft-b200 0.1"; }
+
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_batch(void* plan, const void* in, void* out, uint64_t batch, void* stream,
+                                                   char* err, size_t cap) {
+    try {
+        if (batch == 0) throw std::invalid_argument("batch must be non-zero");
+        sfb::execute_plan(static_cast<sfb::DevicePlan*>(plan), in, out, static_cast<cudaStream_t>(stream), batch);
+        return 0;
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return 1;
+    }
+}
 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);

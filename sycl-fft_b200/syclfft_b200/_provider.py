@@ -44,6 +44,16 @@ _EXECUTE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctyp
 _SCRATCH = ctypes.CFUNCTYPE(ctypes.c_uint64, ctypes.c_void_p)
 
 
+class GroupItemV1(ctypes.Structure):
+    _fields_ = [
+        ("in_", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("batch", ctypes.c_uint64),
+        ("direction", ctypes.c_int32),
+        ("normalization", ctypes.c_uint32),
+    ]
+
+
 class ProviderV1(ctypes.Structure):
     _fields_ = [
         ("abi_version", ctypes.c_uint32),
@@ -63,6 +73,11 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_plan_launches",
     "syclfft_b200_version",
     "syclfft_b200_plan_status",
+    "syclfft_b200_execute_batch",
+    "syclfft_b200_group_supports",
+    "syclfft_b200_group_create",
+    "syclfft_b200_group_execute",
+    "syclfft_b200_group_destroy",
     "syclfft_b200_execute_noalloc_c2c_f32",
 )
 
@@ -86,8 +101,21 @@ def load(path: str | None = None):
     lib.syclfft_b200_plan_launches.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_version.restype = ctypes.c_char_p
     lib.syclfft_b200_version.argtypes = []
+    lib.syclfft_b200_execute_batch.restype = ctypes.c_int
+    lib.syclfft_b200_execute_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                               ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
     lib.syclfft_b200_plan_status.restype = ctypes.c_int
     lib.syclfft_b200_plan_status.argtypes = [ctypes.c_void_p]
+    lib.syclfft_b200_group_supports.restype = ctypes.c_int
+    lib.syclfft_b200_group_supports.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
+    lib.syclfft_b200_group_create.restype = ctypes.c_void_p
+    lib.syclfft_b200_group_create.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_char_p,
+                                              ctypes.c_size_t]
+    lib.syclfft_b200_group_execute.restype = ctypes.c_int
+    lib.syclfft_b200_group_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(GroupItemV1), ctypes.c_uint32,
+                                               ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_group_destroy.restype = None
+    lib.syclfft_b200_group_destroy.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_execute_noalloc_c2c_f32.restype = ctypes.c_int
     lib.syclfft_b200_execute_noalloc_c2c_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                          ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32,

@@ -1,0 +1,289 @@
+"""Continuous-batching FFT serving loop over the B200 provider.
+
+Requests of mixed lengths, batch counts, precisions, directions and normalizations arrive
+over time. The server keeps plans and their tables resident on the device, admits waiting
+requests while their buffers (and any new plan's scratch) fit an HBM budget, and launches
+everything admitted so far without waiting for earlier work: requests whose length has a
+size-specialised single-pass kernel are packed into one grouped launch per length family
+(syclfft_b200_group_execute), the others run on resident plans made for up to a
+power-of-two batch (syclfft_b200_execute_batch). Families are spread over several CUDA
+streams so independent work overlaps on the device. Latency is measured from a request's
+arrival to the CUDA event that completes it; the per-request plain mode executes one
+request at a time with one plan execute each and waits for it, for comparison.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import statistics
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _provider
+
+ERR = 1024
+
+
+@dataclass
+class Request:
+    rid: int
+    lengths: tuple
+    batch: int
+    double: bool
+    direction: int  # -1 forward, +1 backward
+    normalization: int
+    seed: int
+    arrival: float  # seconds after the start of the run
+    # filled while serving
+    nbytes: int = 0
+    t_done: float = 0.0
+    inp: object = None
+    out: object = None
+    result: object = None
+
+    @property
+    def elements(self):
+        return self.batch * math.prod(self.lengths)
+
+    @property
+    def flops(self):
+        n = math.prod(self.lengths)
+        return 5.0 * n * math.log2(n) * self.batch if n > 1 else 0.0
+
+
+def _smooth7(n):
+    for p in (2, 3, 5, 7):
+        while n % p == 0:
+            n //= p
+    return n == 1
+
+
+def _primes(lo, hi):
+    sieve = np.ones(hi + 1, dtype=bool)
+    sieve[:2] = False
+    for i in range(2, int(hi ** 0.5) + 1):
+        if sieve[i]:
+            sieve[i * i::i] = False
+    return [int(p) for p in np.nonzero(sieve)[0] if p >= lo]
+
+
+def make_request_stream(count=20000, rate=50000.0, seed=5, max_batch=512, float_share=0.8):
+    """The mixed request stream of the serving configuration: Poisson arrivals; lengths one
+    third each from powers of two 2^6..2^20 (log-uniform), 7-smooth lengths and primes
+    257..65537; batch log-uniform 1..512; 80% complex<float>; random direction and
+    normalization; a per-request seed for the uniform[-1, 1) input."""
+    rng = np.random.default_rng(seed)
+    smooth = [n for n in range(64, 1 << 20) if _smooth7(n) and (n & (n - 1))]
+    primes = _primes(257, 65537)
+    t = 0.0
+    reqs = []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        fam = rng.integers(0, 3)
+        if fam == 0:
+            n = 1 << int(rng.integers(6, 21))
+        elif fam == 1:
+            n = int(smooth[int(np.exp(rng.uniform(0, np.log(len(smooth)))) - 1)])
+        else:
+            n = int(primes[int(rng.integers(0, len(primes)))])
+        batch = int(np.clip(np.exp(rng.uniform(0, np.log(max_batch))), 1, max_batch))
+        reqs.append(Request(i, (n,), batch, bool(rng.random() >= float_share), int(rng.choice([-1, 1])),
+                            int(rng.integers(0, 4)), int(rng.integers(0, 2 ** 31)), t))
+    return reqs
+
+
+def _pow2_ceil(v):
+    return 1 << max(0, (int(v) - 1).bit_length())
+
+
+class Server:
+    def __init__(self, device=None, budget_bytes=120e9, streams=4, torch_module=None):
+        import torch
+        self.torch = torch
+        self.dev = torch.cuda.current_device() if device is None else device
+        self.lib = _provider.load()
+        self.api = _provider.provider(self.lib)
+        self.budget = float(budget_bytes)
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(streams)]
+        self.plans = {}   # (lengths, double, direction, norm, cap) -> (handle, scratch bytes)
+        self.groups = {}  # (n, double) -> handle
+        self.err = ctypes.create_string_buffer(ERR)
+        self.plan_bytes = 0
+
+    # ---------------------------------------------------------------- resident state
+    def _plan(self, r: Request):
+        cap = _pow2_ceil(r.batch)
+        key = (r.lengths, r.double, r.direction, r.normalization, cap)
+        h = self.plans.get(key)
+        if h is None:
+            cfg = _provider.make_config(list(r.lengths), cap, r.direction, r.double, False, r.normalization,
+                                        False, self.dev)
+            handle = self.api.create(ctypes.byref(cfg), self.err, ERR)
+            if not handle:
+                raise RuntimeError(self.err.value.decode())
+            scratch = int(self.api.scratch_bytes(handle))
+            self.plan_bytes += scratch
+            h = (handle, scratch)
+            self.plans[key] = h
+        return h[0]
+
+    def _group(self, n, double):
+        key = (n, double)
+        g = self.groups.get(key)
+        if g is None:
+            g = self.lib.syclfft_b200_group_create(2 if double else 1, n, self.dev, self.err, ERR)
+            if not g:
+                raise RuntimeError(self.err.value.decode())
+            self.groups[key] = g
+        return g
+
+    def groupable(self, r: Request):
+        return len(r.lengths) == 1 and bool(self.lib.syclfft_b200_group_supports(2 if r.double else 1, r.lengths[0]))
+
+    def close(self):
+        self.torch.cuda.synchronize(self.dev)
+        for handle, _ in self.plans.values():
+            self.api.destroy(handle)
+        for g in self.groups.values():
+            self.lib.syclfft_b200_group_destroy(g)
+        self.plans.clear()
+        self.groups.clear()
+
+    # ---------------------------------------------------------------- data
+    def _fill(self, r: Request, stream):
+        torch = self.torch
+        fdt = torch.float64 if r.double else torch.float32
+        with torch.cuda.stream(stream):
+            g = torch.Generator(device=f"cuda:{self.dev}")
+            g.manual_seed(r.seed)
+            ri = torch.rand(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt, generator=g) * 2 - 1
+            r.inp = torch.view_as_complex(ri.view(-1, 2))
+            r.out = torch.empty_like(r.inp)
+
+    def _execute_one(self, r: Request, stream):
+        h = self._plan(r)
+        rc = self.lib.syclfft_b200_execute_batch(h, r.inp.data_ptr(), r.out.data_ptr(), r.batch, stream.cuda_stream,
+                                                 self.err, ERR)
+        if rc:
+            raise RuntimeError(self.err.value.decode())
+
+    def _execute_group(self, key, reqs, stream):
+        n, double = key
+        g = self._group(n, double)
+        items = (_provider.GroupItemV1 * len(reqs))()
+        for i, r in enumerate(reqs):
+            items[i].in_ = r.inp.data_ptr()
+            items[i].out = r.out.data_ptr()
+            items[i].batch = r.batch
+            items[i].direction = r.direction
+            items[i].normalization = r.normalization
+        rc = self.lib.syclfft_b200_group_execute(g, items, len(reqs), stream.cuda_stream, self.err, ERR)
+        if rc:
+            raise RuntimeError(self.err.value.decode())
+
+    # ---------------------------------------------------------------- loops
+    def run(self, requests, mode="served", keep_results=False):
+        """Serve `requests` (sorted by arrival); returns statistics. mode 'served' or 'plain'."""
+        torch = self.torch
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        for r in reqs:
+            r.nbytes = 2 * r.elements * (16 if r.double else 8)
+        start = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(self.dev)
+        t0 = time.perf_counter()
+        start.record(self.streams[0])
+        done_events = []
+        if mode == "plain":
+            s = self.streams[0]
+            for r in reqs:
+                while time.perf_counter() - t0 < r.arrival:
+                    pass
+                self._fill(r, s)
+                with torch.cuda.stream(s):
+                    self._execute_one(r, s)
+                    ev = torch.cuda.Event(enable_timing=True)
+                    ev.record(s)
+                ev.synchronize()
+                r.t_done = start.elapsed_time(ev) / 1e3
+                if keep_results:
+                    r.result = r.out.cpu()
+                r.inp = r.out = None
+        else:
+            self._serve(reqs, t0, start, keep_results)
+        torch.cuda.synchronize(self.dev)
+        lat = [r.t_done - r.arrival for r in reqs]
+        makespan = max(r.t_done for r in reqs) - min(r.arrival for r in reqs)
+        total_flops = sum(r.flops for r in reqs)
+        total_bytes = sum(r.nbytes for r in reqs)
+        lat_sorted = sorted(lat)
+        return {
+            "mode": mode, "requests": len(reqs), "makespan_s": makespan,
+            "throughput_gflops": total_flops / makespan / 1e9, "throughput_gbs": total_bytes / makespan / 1e9,
+            "requests_per_s": len(reqs) / makespan,
+            "p50_ms": 1e3 * lat_sorted[len(lat) // 2], "p99_ms": 1e3 * lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "mean_ms": 1e3 * statistics.mean(lat), "plans": len(self.plans), "groups": len(self.groups),
+            "plan_scratch_bytes": self.plan_bytes,
+        }
+
+    def _serve(self, reqs, t0, start, keep_results):
+        torch = self.torch
+        nxt = 0
+        waiting = deque()
+        in_flight = deque()  # (event, [requests])
+        used = 0.0
+        S = len(self.streams)
+        completed = 0
+        while completed < len(reqs):
+            now = time.perf_counter() - t0
+            while nxt < len(reqs) and reqs[nxt].arrival <= now:
+                waiting.append(reqs[nxt])
+                nxt += 1
+            # admission by HBM budget (FIFO; a request larger than the budget runs alone)
+            bins = {}
+            while waiting:
+                r = waiting[0]
+                if used + r.nbytes > self.budget and (used > 0 or in_flight):
+                    break
+                waiting.popleft()
+                used += r.nbytes
+                key = ("g", r.lengths[0], r.double) if self.groupable(r) else ("p", r.lengths, r.double)
+                bins.setdefault(key, []).append(r)
+            # launch everything admitted: one grouped launch per length family
+            for key, rs in bins.items():
+                s = self.streams[hash(key) % S]
+                for r in rs:
+                    self._fill(r, s)
+                with torch.cuda.stream(s):
+                    if key[0] == "g":
+                        self._execute_group((key[1], key[2]), rs, s)
+                    else:
+                        for r in rs:
+                            self._execute_one(r, s)
+                    ev = torch.cuda.Event(enable_timing=True)
+                    ev.record(s)
+                in_flight.append((ev, rs))
+            # completions
+            progressed = False
+            while in_flight and in_flight[0][0].query():
+                ev, rs = in_flight.popleft()
+                t = start.elapsed_time(ev) / 1e3
+                for r in rs:
+                    r.t_done = t
+                    if keep_results:
+                        r.result = r.out.cpu()
+                    r.inp = r.out = None
+                    used -= r.nbytes
+                completed += len(rs)
+                progressed = True
+            if not progressed and not bins:
+                if in_flight and (waiting or nxt >= len(reqs)):
+                    # blocked on memory or draining: wait for the oldest launch
+                    in_flight[0][0].synchronize()
+                elif nxt < len(reqs):
+                    # idle until the next arrival (short sleeps keep arrival times honest)
+                    gap = reqs[nxt].arrival - (time.perf_counter() - t0)
+                    if gap > 2e-4:
+                        time.sleep(min(gap, 1e-3))

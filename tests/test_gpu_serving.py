@@ -1,0 +1,127 @@
+"""Serving-path features on the GPU: grouped launches (many requests of a length family in
+one launch), plans that run a smaller batch than planned, device-generated Bluestein
+tables, and the continuous-batching loop, whose results must be the same for a request
+served alone and in the mix."""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from conftest import fp64_fft, norm_scale, rel_l2, uniform_complex
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    if not t.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return t
+
+
+def spec_tol(n, dbl):
+    return (1e-12 if dbl else 1e-5) * max(1.0, math.log2(max(n, 2)))
+
+
+def test_grouped_launch_matches_fp64(torch):
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    rng = np.random.default_rng(3)
+    for n, dbl in ((4096, False), (256, True), (13440, False), (64, False)):
+        assert lib.syclfft_b200_group_supports(2 if dbl else 1, n) == 1
+        g = lib.syclfft_b200_group_create(2 if dbl else 1, n, -1, err, 1024)
+        assert g, err.value
+        dt = np.complex128 if dbl else np.complex64
+        reqs = []
+        for i in range(7):
+            b = int(rng.integers(1, 40))
+            d = int(rng.choice([-1, 1]))
+            nm = int(rng.integers(0, 4))
+            x = uniform_complex(n * b, 100 * i + n, dt)
+            xi = torch.from_numpy(x).cuda()
+            xo = xi if i % 3 == 0 else torch.empty_like(xi)  # some in place
+            reqs.append((x, xi, xo, b, d, nm))
+        items = (_provider.GroupItemV1 * len(reqs))()
+        for k, (x, xi, xo, b, d, nm) in enumerate(reqs):
+            items[k].in_, items[k].out, items[k].batch = xi.data_ptr(), xo.data_ptr(), b
+            items[k].direction, items[k].normalization = d, nm
+        rc = lib.syclfft_b200_group_execute(g, items, len(reqs), torch.cuda.current_stream().cuda_stream, err, 1024)
+        assert rc == 0, err.value
+        torch.cuda.synchronize()
+        for x, xi, xo, b, d, nm in reqs:
+            ref = fp64_fft(x, [n], b, d, norm_scale(nm, d, n))
+            assert rel_l2(xo.cpu().numpy(), ref) <= spec_tol(n, dbl)
+        lib.syclfft_b200_group_destroy(g)
+    assert lib.syclfft_b200_group_supports(1, 1009) == 0
+
+
+@pytest.mark.parametrize("shape,dbl", [([4096], False), ([65536], True), ([65537], False), ([1009], True),
+                                       ([13440], False), ([24, 40], False), ([30000], True)], ids=str)
+def test_execute_smaller_batch(torch, shape, dbl):
+    """A plan for up to 8 transforms runs the first 3 (same tables and scratch)."""
+    from syclfft_b200 import _provider
+    api = _provider.provider()
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    cfg = _provider.make_config(shape, 8, 1, double=dbl, normalization=2)
+    h = api.create(ctypes.byref(cfg), err, 1024)
+    assert h, err.value
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(3 * n, 7 + n, dt)
+    xi = torch.from_numpy(x).cuda()
+    out = torch.zeros(8 * n, dtype=xi.dtype, device="cuda")
+    rc = lib.syclfft_b200_execute_batch(h, xi.data_ptr(), out.data_ptr(), 3, torch.cuda.current_stream().cuda_stream,
+                                        err, 1024)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert rel_l2(got[: 3 * n], fp64_fft(x, shape, 3, 1, 1.0 / n)) <= spec_tol(n, dbl)
+    assert not np.any(got[3 * n:])  # nothing written past the requested batch
+    assert lib.syclfft_b200_execute_batch(h, xi.data_ptr(), out.data_ptr(), 9, None, err, 1024) != 0
+    api.destroy(h)
+
+
+def test_device_bluestein_tables_accuracy(torch):
+    """Chirp spectra made on the device (FP64 FFT) keep Bluestein at FP64 accuracy."""
+    import syclfft_b200 as sf
+    for n in (257, 4099, 30011, 65537):
+        x = uniform_complex(2 * n, n, np.complex128)
+        p = sf.plan_many_dft("double", [n], 2, sf.direction.forward)
+        xt = torch.from_numpy(x).cuda()
+        out = torch.empty_like(xt)
+        p.execute(xt, out).synchronize()
+        assert rel_l2(out.cpu().numpy(), fp64_fft(x, [n], 2, -1)) <= spec_tol(n, True)
+
+
+def test_serving_alone_vs_mix(torch):
+    """Each request's result is the same served alone (plain, one at a time) and in the mix
+    (continuous batching, grouped launches, several streams)."""
+    from syclfft_b200 import serving
+    reqs = serving.make_request_stream(count=160, rate=20000.0, seed=11, max_batch=16)
+    reqs = [r for r in reqs if r.lengths[0] <= 1 << 16]
+    srv = serving.Server(budget_bytes=2e9, streams=3)
+    try:
+        mixed = srv.run(reqs, mode="served", keep_results=True)
+        results = {r.rid: r.result for r in reqs}
+        alone = srv.run(reqs, mode="plain", keep_results=True)
+        for r in reqs:
+            a, b = results[r.rid].numpy(), r.result.numpy()
+            assert rel_l2(a, b) <= spec_tol(r.lengths[0], r.double), r
+        # and against FP64 for a few
+        for r in reqs[:12]:
+            g = torch.Generator(device="cuda").manual_seed(r.seed)
+            fdt = torch.float64 if r.double else torch.float32
+            xi = torch.rand(2 * r.elements, device="cuda", dtype=fdt, generator=g) * 2 - 1
+            x = torch.view_as_complex(xi.view(-1, 2)).cpu().numpy()
+            n = r.lengths[0]
+            ref = fp64_fft(x, [n], r.batch, r.direction, norm_scale(r.normalization, r.direction, n))
+            assert rel_l2(results[r.rid].numpy(), ref) <= spec_tol(n, r.double)
+        for st in (mixed, alone):
+            assert st["requests"] == len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
+        assert mixed["groups"] >= 1
+    finally:
+        srv.close()

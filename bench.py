@@ -417,6 +417,34 @@ def run_ours(args):
     return 0
 
 
+def run_serve(args):
+    """Serving configuration: the mixed request stream through the continuous-batching loop
+    and through per-request plain executes; one JSON line with both."""
+    import torch
+    from syclfft_b200 import serving
+    torch.cuda.set_device(0)
+    reqs = serving.make_request_stream(count=args.requests, rate=args.rate, seed=5)
+    out = {"metric": "FFT serving stream: throughput (GFLOP/s, 5N log2N) and p50/p99 latency (arrival to completion)",
+           "unit": "GFLOP/s", "higher_is_better": True, "n_gpus": 1, "data": "synthetic (seeded uniform[-1,1))",
+           "config": {"workload": "serving_stream", "requests": len(reqs), "arrival_rate_per_s": args.rate,
+                      "lengths": "1/3 pow2 2^6..2^20, 1/3 7-smooth, 1/3 primes 257..65537",
+                      "batch": "log-uniform 1..512", "precision": "80% c64 / 20% c128",
+                      "hbm_budget_gb": args.budget_gb}}
+    for mode in ("served", "plain"):
+        srv = serving.Server(budget_bytes=args.budget_gb * 1e9, streams=4)
+        try:
+            st = srv.run([serving.Request(**{k: getattr(r, k) for k in ("rid", "lengths", "batch", "double",
+                                                                         "direction", "normalization", "seed",
+                                                                         "arrival")}) for r in reqs], mode=mode)
+        finally:
+            srv.close()
+        out[mode] = {k: (round(v, 4) if isinstance(v, float) else v) for k, v in st.items()}
+    out["value"] = out["served"]["throughput_gflops"]
+    out["speedup_vs_plain"] = round(out["served"]["throughput_gflops"] / out["plain"]["throughput_gflops"], 3)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -429,11 +457,17 @@ def main():
     ap.add_argument("--only", default="", help="run one plan of the workload (profiling)")
     ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
     ap.add_argument("--plan", default="", help="replace the workload: N[xM[xK]]:batch:c64|c128[,...]")
+    ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
+    ap.add_argument("--requests", type=int, default=20000)
+    ap.add_argument("--rate", type=float, default=50000.0)
+    ap.add_argument("--budget-gb", type=float, default=120.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve:
+        return run_serve(args)
     return run_ours(args)
 
 

@@ -94,11 +94,27 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void *plan, char *buf, 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
 /* Library version string. */
 SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
+/* create with options (serving): SYCLFFT_B200_CREATE_STREAM_SCRATCH -- the plan owns no
+ * scratch; each execute borrows a scratch arena of the executing stream (stream-ordered,
+ * grown on demand), so many resident plans cost only their tables.
+ * SYCLFFT_B200_CREATE_SYNC -- return only when the tables are on the device (create()
+ * does this); without it, executes wait for the tables on the device and the host does not. */
+#define SYCLFFT_B200_CREATE_STREAM_SCRATCH 1u
+#define SYCLFFT_B200_CREATE_SYNC 2u
+SYCLFFT_B200_EXPORT void *syclfft_b200_create_ex(const syclfft_b200_plan_config_v1 *config, uint32_t flags, char *err,
+                                                 size_t cap);
 /* Like execute, for the first `batch` transforms only (1 <= batch <= the plan's
  * batch_count): a plan made for up to B transforms serves any smaller batch with the same
  * resident tables and scratch. */
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_batch(void *plan, const void *in, void *out, uint64_t batch,
                                                    void *stream, char *err, size_t cap);
+/* Like execute_batch (batch 0 = the plan's batch count), in another direction and/or
+ * normalization than the plan was made for: direction 0 = the plan's, -1 / +1;
+ * normalization -1 = the plan's, else SYCLFFT_B200_NORM_*. The inverse is formed as
+ * conj(F(conj x)), so one resident plan (tables, chirps, scratch) serves both directions. */
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void *plan, const void *in, void *out, uint64_t batch,
+                                                int32_t direction, int32_t normalization, void *stream, char *err,
+                                                size_t cap);
 /* Device status word of the plan: 0 = healthy; 1 = a kernel's bounded wait on an
  * asynchronous copy gave up (the execution's output is incomplete). Synchronous. -1 on error. */
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void *plan);

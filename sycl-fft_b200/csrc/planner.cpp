@@ -8,6 +8,8 @@
 #include <cmath>
 #include <limits>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
 
@@ -80,6 +82,25 @@ int maxt_for(int threads) {
     return 1024;
 }
 
+// Process-wide cache of generated tables: stage twiddles and four-step twiddles depend only
+// on their radix sequence / length, so plans of the same lengths reuse them.
+std::mutex g_table_mu;
+std::map<std::vector<int64_t>, std::shared_ptr<const std::vector<std::complex<double>>>> g_tables;
+
+template <class Make>
+std::shared_ptr<const std::vector<std::complex<double>>> cached_table(std::vector<int64_t> key, Make make) {
+    {
+        std::lock_guard<std::mutex> lock(g_table_mu);
+        auto it = g_tables.find(key);
+        if (it != g_tables.end()) return it->second;
+    }
+    auto t = std::make_shared<const std::vector<std::complex<double>>>(make());
+    std::lock_guard<std::mutex> lock(g_table_mu);
+    if (g_tables.size() > 4096) g_tables.clear();  // bound the cache
+    g_tables[key] = t;
+    return t;
+}
+
 struct Builder {
     PlanSpec& plan;
     const PlanRequest& req;
@@ -88,7 +109,15 @@ struct Builder {
     std::map<std::vector<int>, int> seq_tables;  // radix sequence -> twiddle table id
 
     int add_table(std::vector<std::complex<double>> t) {
+        plan.table_sizes.push_back(t.size());
         plan.tables.push_back(std::move(t));
+        return static_cast<int>(plan.tables.size()) - 1;
+    }
+
+    // A table of n entries the device fills (no host data).
+    int add_device_table(size_t n) {
+        plan.table_sizes.push_back(n);
+        plan.tables.emplace_back();
         return static_cast<int>(plan.tables.size()) - 1;
     }
 
@@ -113,19 +142,23 @@ struct Builder {
             *table_id = it->second;
             return s;
         }
-        std::vector<std::complex<double>> tw(std::max(off, 1));
-        ns = 1;
-        for (int i = 0; i < s.nstages; ++i) {
-            const int R = radices[i];
-            for (int jm = 0; jm < ns; ++jm) {
-                for (int r = 1; r < R; ++r) {
-                    tw[s.tw_off[i] + jm * (R - 1) + (r - 1)] =
-                        cis_neg(static_cast<int64_t>(r) * jm, static_cast<int64_t>(ns) * R);
-                }
+        std::vector<int64_t> ckey(radices.begin(), radices.end());
+        ckey.push_back(-100);
+        const StageSeq sc = s;
+        auto tw = cached_table(ckey, [&] {
+            std::vector<std::complex<double>> t(std::max(off, 1));
+            int ns2 = 1;
+            for (int i = 0; i < sc.nstages; ++i) {
+                const int R = radices[i];
+                for (int jm = 0; jm < ns2; ++jm)
+                    for (int r = 1; r < R; ++r)
+                        t[sc.tw_off[i] + jm * (R - 1) + (r - 1)] =
+                            cis_neg(static_cast<int64_t>(r) * jm, static_cast<int64_t>(ns2) * R);
+                ns2 *= R;
             }
-            ns *= R;
-        }
-        *table_id = add_table(std::move(tw));
+            return t;
+        });
+        *table_id = add_table(*tw);
         seq_tables[key] = *table_id;
         return s;
     }
@@ -136,14 +169,19 @@ struct Builder {
         key.push_back(-1);  // distinct from the full-table key
         auto it = seq_tables.find(key);
         if (it != seq_tables.end()) return it->second;
-        std::vector<std::complex<double>> tw;
-        int64_t ns = 1;
-        for (int R : radices) {
-            for (int64_t jm = 0; jm < ns; ++jm) tw.push_back(cis_neg(jm, ns * R));
-            ns *= R;
-        }
-        if (tw.empty()) tw.push_back(1.0);
-        const int id = add_table(std::move(tw));
+        std::vector<int64_t> ckey(radices.begin(), radices.end());
+        ckey.push_back(-200);
+        auto tw = cached_table(ckey, [&] {
+            std::vector<std::complex<double>> t;
+            int64_t ns = 1;
+            for (int R : radices) {
+                for (int64_t jm = 0; jm < ns; ++jm) t.push_back(cis_neg(jm, ns * R));
+                ns *= R;
+            }
+            if (t.empty()) t.push_back(1.0);
+            return t;
+        });
+        const int id = add_table(*tw);
         seq_tables[key] = id;
         return id;
     }
@@ -159,11 +197,18 @@ struct Builder {
         while ((int64_t(1) << (2 * shift)) < ntot) ++shift;  // 2^shift >= sqrt(ntot)
         const int64_t B = int64_t(1) << shift;
         const int64_t nhi = (ntot + B - 1) / B + 1;
-        std::vector<std::complex<double>> hi(nhi), lo(B);
-        for (int64_t q = 0; q < nhi; ++q) hi[q] = cis_neg(q * B, ntot);
-        for (int64_t r = 0; r < B; ++r) lo[r] = cis_neg(r, ntot);
-        ps.tables.tw4_hi = add_table(std::move(hi));
-        ps.tables.tw4_lo = add_table(std::move(lo));
+        auto hi = cached_table({ntot, B, -300}, [&] {
+            std::vector<std::complex<double>> t(nhi);
+            for (int64_t q = 0; q < nhi; ++q) t[q] = cis_neg(q * B, ntot);
+            return t;
+        });
+        auto lo = cached_table({ntot, B, -400}, [&] {
+            std::vector<std::complex<double>> t(B);
+            for (int64_t r = 0; r < B; ++r) t[r] = cis_neg(r, ntot);
+            return t;
+        });
+        ps.tables.tw4_hi = add_table(*hi);
+        ps.tables.tw4_lo = add_table(*lo);
         ps.p.tw4_shift = shift;
         ps.p.tw4_sign = sign;
     }
@@ -424,8 +469,10 @@ struct Builder {
         // h_n = conj(c_n) (exact n^2 mod 2L reduction), convolution of length M via FFT.
         const int64_t M = static_cast<int64_t>(bluestein_length(static_cast<uint64_t>(L)));
         const int sgn = req.direction;  // -1 forward, +1 backward
-        std::vector<std::complex<double>> chirp(L), kern(M, 0.0);
+        std::vector<std::complex<double>> chirp, kern;
         if (!req.device_spectrum) {
+            chirp.assign(L, 0.0);
+            kern.assign(M, 0.0);
             for (int64_t n = 0; n < L; ++n) {
                 const uint64_t r = (static_cast<unsigned __int128>(n) * n) % static_cast<uint64_t>(2 * L);
                 // h_n = exp(-i*sgn*pi*r/L) = exp(-2 pi i * (sgn*r) / (2L))
@@ -437,7 +484,7 @@ struct Builder {
             host_fft_fp64(kern, -1);
             for (auto& v : kern) v /= static_cast<double>(M);
         }
-        const int chirp_id = add_table(std::move(chirp));
+        const int chirp_id = req.device_spectrum ? add_device_table(L) : add_table(std::move(chirp));
         const int mode = s == 1 ? kModeK : kModeC;
         if (fits(M, mode)) {
             PassSpec ps;
@@ -457,7 +504,7 @@ struct Builder {
             p.in_len = p.out_len = L;
             ps.tables.premul = chirp_id;
             ps.tables.postmul = chirp_id;
-            ps.tables.pointwise = add_table(std::move(kern));
+            ps.tables.pointwise = req.device_spectrum ? add_device_table(M) : add_table(std::move(kern));
             if (req.device_spectrum) {
                 BluesteinJob job;
                 job.L = L;
@@ -483,12 +530,15 @@ struct Builder {
         int64_t n1, n2;
         if (!split(M, n1, n2)) throw std::runtime_error("Bluestein length too large for this provider");
         // K'[k1*N2 + k2] = K[k1 + N1*k2]
-        std::vector<std::complex<double>> kp(M);
+        int kp_id;
         if (!req.device_spectrum) {
+            std::vector<std::complex<double>> kp(M);
             for (int64_t k1 = 0; k1 < n1; ++k1)
                 for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = kern[k1 + n1 * k2];
+            kp_id = add_table(std::move(kp));
+        } else {
+            kp_id = add_device_table(M);
         }
-        const int kp_id = add_table(std::move(kp));
         if (req.device_spectrum) {
             BluesteinJob job;
             job.L = L;

@@ -119,6 +119,9 @@ struct PlanSpec {
     uint64_t elements = 0, transform_size = 0;
     double scale = 1.0;
     std::vector<std::vector<std::complex<double>>> tables;
+    // Entries of each table; a table whose data is empty but whose size is not is generated on
+    // the device (Bluestein chirp and spectrum with PlanRequest::device_spectrum).
+    std::vector<size_t> table_sizes;
     std::vector<PassSpec> passes;
     uint64_t scratch_elements = 0;
 };

@@ -65,7 +65,8 @@ private:
 
 struct BoundPass {
     PassParams p;
-    PassSpec spec;
+    const PassSpec* spec_ptr = nullptr;  // the plan's PassSpec (stable: plan->spec.passes)
+    const PassSpec& spec_ref() const { return *spec_ptr; }
     FixedParams fp;    // used when spec.fixed_id >= 0
     ClusterParams cp;  // used when spec.cluster_id >= 0
     PipedParams pp;    // used when spec.piped_id >= 0 and the buffers are 16-byte aligned
@@ -123,6 +124,25 @@ FixedParams to_fixed(const PassParams& p) {
     return f;
 }
 
+// Per-device stream for plan memory: allocations and frees are stream-ordered
+// (cudaMallocAsync / cudaFreeAsync), so releasing a plan never synchronizes the device.
+cudaStream_t memory_stream(int device) {
+    static std::mutex mu;
+    static std::map<int, cudaStream_t> streams;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = streams.find(device);
+    if (it != streams.end()) return it->second;
+    cudaStream_t s = nullptr;
+    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = uint64_t(4) << 30;  // keep up to 4 GiB of freed plan memory for the next plans
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    streams[device] = s;
+    return s;
+}
+
 struct DevicePlan {
     PlanSpec spec;
     int device = 0;
@@ -132,20 +152,55 @@ struct DevicePlan {
     int sms = 148;
     std::vector<BoundPass> passes;
     cudaEvent_t done = nullptr;
+    cudaEvent_t ready = nullptr;  // tables complete (recorded on the memory stream at creation)
+    bool stream_scratch = false;  // scratch comes from the executing stream's arena
     std::mutex mu;
 
     ~DevicePlan() {
         int prev = 0;
         if (cudaGetDevice(&prev) == cudaSuccess && prev != device) cudaSetDevice(device);
-        if (done) {
-            cudaEventSynchronize(done);
-            cudaEventDestroy(done);
+        cudaStream_t ms = nullptr;
+        try {
+            ms = memory_stream(device);
+        } catch (...) {
         }
-        if (scratch) cudaFree(scratch);
-        if (table_mem) cudaFree(table_mem);
+        if (ms) {
+            // free after the plan's last execution, without blocking host or device
+            if (done) cudaStreamWaitEvent(ms, done, 0);
+            if (scratch) cudaFreeAsync(scratch, ms);
+            if (table_mem) cudaFreeAsync(table_mem, ms);
+        } else {
+            if (done) cudaEventSynchronize(done);
+            if (scratch) cudaFree(scratch);
+            if (table_mem) cudaFree(table_mem);
+        }
+        if (done) cudaEventDestroy(done);
+        if (ready) cudaEventDestroy(ready);
         if (prev != device) cudaSetDevice(prev);
     }
 };
+
+// Scratch arenas, one per (device, stream): stream-ordered (cudaMallocAsync on the stream
+// itself), grown on demand, shared by every stream-scratch plan executed on that stream.
+void* stream_arena(int device, cudaStream_t stream, size_t bytes) {
+    struct Arena {
+        void* ptr = nullptr;
+        size_t size = 0;
+    };
+    static std::mutex mu;
+    static std::map<std::pair<int, cudaStream_t>, Arena> arenas;
+    std::lock_guard<std::mutex> lock(mu);
+    Arena& a = arenas[{device, stream}];
+    if (a.size < bytes) {
+        if (a.ptr) check(cudaFreeAsync(a.ptr, stream), "cudaFreeAsync(arena)");
+        a.ptr = nullptr;
+        a.size = 0;
+        size_t grow = bytes + bytes / 4;
+        check(cudaMallocAsync(&a.ptr, grow, stream), "cudaMallocAsync(arena)");
+        a.size = grow;
+    }
+    return a.ptr;
+}
 
 template <class T>
 void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned char>& blob, size_t off) {
@@ -156,8 +211,9 @@ void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned
     }
 }
 
-DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg);
-void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch);
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags = 0);
+void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch = 0,
+                  int direction = 0, int normalization = -1);
 
 // FP64 forward in-place FFT plans of length M used to make chirp spectra; kept for the process.
 DevicePlan* spectrum_plan(int device, int64_t M) {
@@ -180,7 +236,7 @@ DevicePlan* spectrum_plan(int device, int64_t M) {
     return p;
 }
 
-DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) {
     if (cfg.abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION) throw std::runtime_error("B200 provider ABI mismatch");
     if (cfg.scalar != SYCLFFT_B200_SCALAR_FLOAT && cfg.scalar != SYCLFFT_B200_SCALAR_DOUBLE)
         throw std::invalid_argument("unsupported scalar type");
@@ -221,7 +277,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
     size_t total = 0;
     for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
         offsets[i] = total;
-        total += (plan->spec.tables[i].size() * cs + 255) / 256 * 256;
+        total += (plan->spec.table_sizes[i] * cs + 255) / 256 * 256;
     }
     const size_t status_off = total;
     total += 256;  // status word(s), zero-initialised with the tables
@@ -230,12 +286,14 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         if (req.dbl) pack_table<double>(plan->spec.tables[i], blob, offsets[i]);
         else pack_table<float>(plan->spec.tables[i], blob, offsets[i]);
     }
-    check(cudaMalloc(&plan->table_mem, blob.size()), "cudaMalloc(tables)");
-    check(cudaMemcpy(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(tables)");
+    cudaStream_t ms = memory_stream(device);
+    check(cudaMallocAsync(&plan->table_mem, blob.size(), ms), "cudaMallocAsync(tables)");
+    check(cudaMemcpyAsync(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(tables)");
     plan->status = reinterpret_cast<int*>(static_cast<unsigned char*>(plan->table_mem) + status_off);
     check(cudaDeviceGetAttribute(&plan->sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    if (plan->spec.scratch_elements) {
-        check(cudaMalloc(&plan->scratch, plan->spec.scratch_elements * cs), "cudaMalloc(scratch)");
+    plan->stream_scratch = (flags & SYCLFFT_B200_CREATE_STREAM_SCRATCH) != 0;
+    if (plan->spec.scratch_elements && !plan->stream_scratch) {
+        check(cudaMallocAsync(&plan->scratch, plan->spec.scratch_elements * cs, ms), "cudaMallocAsync(scratch)");
     }
     check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
     if (!plan->spec.bluestein_jobs.empty()) {
@@ -243,22 +301,26 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         int64_t maxM = 0;
         for (const auto& j : plan->spec.bluestein_jobs) maxM = std::max(maxM, j.M);
         void* kern = nullptr;
-        check(cudaMalloc(&kern, static_cast<size_t>(maxM) * 16), "cudaMalloc(chirp kernel)");
+        check(cudaMallocAsync(&kern, static_cast<size_t>(maxM) * 16, ms), "cudaMallocAsync(chirp kernel)");
         try {
             for (const auto& j : plan->spec.bluestein_jobs) {
                 void* chirp = static_cast<unsigned char*>(plan->table_mem) + offsets[j.chirp_table];
                 void* spec = static_cast<unsigned char*>(plan->table_mem) + offsets[j.spectrum_table];
-                check(bluestein_chirp(req.dbl, chirp, kern, j.L, j.M, j.sgn, nullptr), "chirp kernel");
-                execute_plan(spectrum_plan(device, j.M), kern, kern, nullptr, 0);
-                check(bluestein_spectrum(req.dbl, spec, kern, j.M, j.n1, j.n2, j.large, nullptr), "spectrum kernel");
+                check(bluestein_chirp(req.dbl, chirp, kern, j.L, j.M, j.sgn, ms), "chirp kernel");
+                execute_plan(spectrum_plan(device, j.M), kern, kern, ms, 0);
+                check(bluestein_spectrum(req.dbl, spec, kern, j.M, j.n1, j.n2, j.large, ms), "spectrum kernel");
             }
-            check(cudaStreamSynchronize(nullptr), "chirp spectrum");
         } catch (...) {
-            cudaFree(kern);
+            cudaFreeAsync(kern, ms);
+            cudaStreamSynchronize(ms);
             throw;
         }
-        cudaFree(kern);
+        cudaFreeAsync(kern, ms);
     }
+    // executes wait for the tables (and chirp spectra) on the device; the host does not
+    check(cudaEventCreateWithFlags(&plan->ready, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventRecord(plan->ready, ms), "cudaEventRecord");
+    if (flags & SYCLFFT_B200_CREATE_SYNC) check(cudaStreamSynchronize(ms), "plan tables");
 
     auto tab = [&](int id) -> const void* {
         return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
@@ -267,7 +329,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
         if (ps.fixed_id < 0 && ps.cluster_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
             throw std::runtime_error("no kernel variant for pass");
         BoundPass bp;
-        bp.spec = ps;
+        bp.spec_ptr = &ps;  // plan->spec.passes is not modified after this point
         bp.p = ps.p;
         bp.p.fft1.tw = tab(ps.tables.tw1);
         bp.p.fft2.tw = tab(ps.tables.tw2);
@@ -287,11 +349,11 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg) {
 // Line counts of a pass for the first `batch` transforms of a plan made for `planned`.
 BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
     if (batch == planned) return bp;
-    if (bp.spec.batch_dim < 0) throw std::invalid_argument("plan cannot run a smaller batch");
+    if (bp.spec_ref().batch_dim < 0) throw std::invalid_argument("plan cannot run a smaller batch");
     BoundPass r = bp;
     PassParams& p = r.p;
     const int64_t b = static_cast<int64_t>(batch), B = static_cast<int64_t>(planned);
-    if (bp.spec.batch_dim == 0) p.n_outer = p.n_outer / B * b;
+    if (bp.spec_ref().batch_dim == 0) p.n_outer = p.n_outer / B * b;
     else p.n_cols = p.n_cols / B * b;
     p.col_tiles = (p.n_cols + p.w - 1) / p.w;
     p.tiles = p.n_outer * p.col_tiles;
@@ -299,11 +361,35 @@ BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
     r.fp.col_tiles = p.col_tiles;
     r.cp.lines = p.n_cols;
     r.pp.lines = p.n_cols;
-    if (bp.spec.cluster_id >= 0) p.tiles = p.n_cols * bp.spec.cl_p;
+    if (bp.spec_ref().cluster_id >= 0) p.tiles = p.n_cols * bp.spec_ref().cl_p;
     return r;
 }
 
-void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch = 0) {
+// Direction / normalization override: conj(F(conj x)) turns a plan's transform into the
+// other direction (conjugation on the first load and the last store; intermediate passes
+// keep their own conjugation pairs), and the last store carries the requested scale.
+void apply_override(BoundPass& bp, bool first, bool last, bool flip, double scale, bool set_scale) {
+    if (flip) {
+        if (first) {
+            bp.p.conj_in ^= 1;
+            bp.fp.conj_in ^= 1;
+            bp.cp.conj_in ^= 1;
+            bp.pp.conj_in ^= 1;
+        }
+        if (last) {
+            bp.p.conj_out ^= 1;
+            bp.fp.conj_out ^= 1;
+            bp.cp.conj_out ^= 1;
+            bp.pp.conj_out ^= 1;
+        }
+    }
+    if (last && set_scale) {
+        bp.p.scale = bp.fp.scale = bp.cp.scale = bp.pp.scale = scale;
+    }
+}
+
+void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch,
+                  int direction, int normalization) {
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
     const uint64_t planned = plan->spec.req.batch;
     if (batch == 0) batch = planned;
@@ -313,31 +399,44 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     if (!in_place && in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
     std::lock_guard<std::mutex> lock(plan->mu);
     DeviceGuard guard(plan->device);
-    for (const BoundPass& planned_pass : plan->passes) {
-        const BoundPass bp = rescale(planned_pass, batch, planned);
+    if (plan->ready) check(cudaStreamWaitEvent(stream, plan->ready, 0), "cudaStreamWaitEvent");
+    void* scratch = plan->scratch;
+    if (plan->stream_scratch && plan->spec.scratch_elements) {
+        const size_t need = plan->spec.scratch_elements / planned * batch * (plan->spec.req.dbl ? 16 : 8) + 256;
+        scratch = stream_arena(plan->device, stream, std::max<size_t>(need, plan->spec.scratch_elements / planned * batch *
+                                                                               (plan->spec.req.dbl ? 16 : 8)));
+    }
+    const int dir = direction == 0 ? plan->spec.req.direction : direction;
+    const int norm = normalization < 0 ? plan->spec.req.normalization : normalization;
+    const bool flip = dir != plan->spec.req.direction;
+    const bool set_scale = flip || norm != plan->spec.req.normalization;
+    const double scale = normalization_scale(norm, dir, plan->spec.transform_size);
+    for (size_t i = 0; i < plan->passes.size(); ++i) {
+        BoundPass bp = rescale(plan->passes[i], batch, planned);
+        if (flip || set_scale) apply_override(bp, i == 0, i + 1 == plan->passes.size(), flip, scale, set_scale);
         auto buf = [&](Buf b) -> void* {
             if (b == Buf::Input) return const_cast<void*>(in);
             if (b == Buf::Output) return out;
-            return plan->scratch;
+            return scratch;
         };
-        const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec.src)) % 16 == 0) &&
-                             (reinterpret_cast<uintptr_t>(buf(bp.spec.dst)) % 16 == 0);
-        if (bp.spec.piped_id >= 0 && aligned) {
+        const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().src)) % 16 == 0) &&
+                             (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().dst)) % 16 == 0);
+        if (bp.spec_ref().piped_id >= 0 && aligned) {
             const int64_t lines = bp.pp.lines;
             const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
-            check(launch_piped(bp.spec.piped_id, bp.pp, grid, buf(bp.spec.src), buf(bp.spec.dst), stream),
+            check(launch_piped(bp.spec_ref().piped_id, bp.pp, grid, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
                   "FFT pipelined pass launch");
-        } else if (bp.spec.cluster_id >= 0) {
-            check(launch_cluster(bp.spec.cluster_id, bp.cp, buf(bp.spec.src), buf(bp.spec.dst), stream),
+        } else if (bp.spec_ref().cluster_id >= 0) {
+            check(launch_cluster(bp.spec_ref().cluster_id, bp.cp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
                   "FFT cluster pass launch");
-        } else if (bp.spec.fixed_id >= 0) {
-            check(launch_fixed(bp.spec.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, bp.spec.threads,
-                               static_cast<size_t>(bp.spec.smem_bytes), bp.p.tiles, buf(bp.spec.src),
-                               buf(bp.spec.dst), stream),
+        } else if (bp.spec_ref().fixed_id >= 0) {
+            check(launch_fixed(bp.spec_ref().fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, bp.spec_ref().threads,
+                               static_cast<size_t>(bp.spec_ref().smem_bytes), bp.p.tiles, buf(bp.spec_ref().src),
+                               buf(bp.spec_ref().dst), stream),
                   "FFT pass launch");
         } else {
-            check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec.kc.maxv, bp.spec.kc.maxt, bp.spec.threads,
-                              static_cast<size_t>(bp.spec.smem_bytes), buf(bp.spec.src), buf(bp.spec.dst), stream),
+            check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec_ref().kc.maxv, bp.spec_ref().kc.maxt, bp.spec_ref().threads,
+                              static_cast<size_t>(bp.spec_ref().smem_bytes), buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
                   "FFT pass launch");
         }
     }
@@ -364,7 +463,7 @@ int p_supports(int32_t device, char* err, size_t cap) {
 void* p_create(const syclfft_b200_plan_config_v1* cfg, char* err, size_t cap) {
     try {
         if (!cfg) throw std::invalid_argument("null plan configuration");
-        return create_plan(*cfg);
+        return create_plan(*cfg, SYCLFFT_B200_CREATE_SYNC);
     } catch (const std::exception& e) {
         set_error(err, cap, e.what());
         return nullptr;
@@ -413,11 +512,37 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
 
 SYCLFFT_B200_EXPORT const char* syclfft_b200_version(void) { return "syclfft-b200 0.1"; }
 
+SYCLFFT_B200_EXPORT void* syclfft_b200_create_ex(const syclfft_b200_plan_config_v1* cfg, uint32_t flags, char* err,
+                                                 size_t cap) {
+    try {
+        if (!cfg) throw std::invalid_argument("null plan configuration");
+        return sfb::create_plan(*cfg, flags);
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return nullptr;
+    }
+}
+
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_batch(void* plan, const void* in, void* out, uint64_t batch, void* stream,
                                                    char* err, size_t cap) {
     try {
         if (batch == 0) throw std::invalid_argument("batch must be non-zero");
         sfb::execute_plan(static_cast<sfb::DevicePlan*>(plan), in, out, static_cast<cudaStream_t>(stream), batch);
+        return 0;
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return 1;
+    }
+}
+
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void* plan, const void* in, void* out, uint64_t batch,
+                                                int32_t direction, int32_t normalization, void* stream, char* err,
+                                                size_t cap) {
+    try {
+        if (direction != 0 && direction != -1 && direction != 1) throw std::invalid_argument("Invalid FFT direction");
+        if (normalization > 3) throw std::invalid_argument("Invalid normalization");
+        sfb::execute_plan(static_cast<sfb::DevicePlan*>(plan), in, out, static_cast<cudaStream_t>(stream), batch,
+                          direction, normalization);
         return 0;
     } catch (const std::exception& e) {
         sfb::set_error(err, cap, e.what());

@@ -16,6 +16,8 @@ PROVIDER_DIR = os.path.join(LIB_DIR, "syclfft", "providers")
 PROVIDER_PATH = os.path.join(PROVIDER_DIR, "syclfft_provider_b200.so")
 
 ABI_VERSION = 1
+CREATE_STREAM_SCRATCH = 1
+CREATE_SYNC = 2
 SCALAR_FLOAT = 1
 SCALAR_DOUBLE = 2
 ERR_CAP = 1024
@@ -73,7 +75,9 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_plan_launches",
     "syclfft_b200_version",
     "syclfft_b200_plan_status",
+    "syclfft_b200_create_ex",
     "syclfft_b200_execute_batch",
+    "syclfft_b200_execute_ex",
     "syclfft_b200_group_supports",
     "syclfft_b200_group_create",
     "syclfft_b200_group_execute",
@@ -104,6 +108,13 @@ def load(path: str | None = None):
     lib.syclfft_b200_execute_batch.restype = ctypes.c_int
     lib.syclfft_b200_execute_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_create_ex.restype = ctypes.c_void_p
+    lib.syclfft_b200_create_ex.argtypes = [ctypes.POINTER(PlanConfigV1), ctypes.c_uint32, ctypes.c_char_p,
+                                           ctypes.c_size_t]
+    lib.syclfft_b200_execute_ex.restype = ctypes.c_int
+    lib.syclfft_b200_execute_ex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_char_p,
+                                            ctypes.c_size_t]
     lib.syclfft_b200_plan_status.restype = ctypes.c_int
     lib.syclfft_b200_plan_status.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_group_supports.restype = ctypes.c_int

@@ -6,7 +6,8 @@ requests while their buffers (and any new plan's scratch) fit an HBM budget, and
 everything admitted so far without waiting for earlier work: requests whose length has a
 size-specialised single-pass kernel are packed into one grouped launch per length family
 (syclfft_b200_group_execute), the others run on resident plans made for up to a
-power-of-two batch (syclfft_b200_execute_batch). Families are spread over several CUDA
+any batch up to 512 (syclfft_b200_execute_ex), created ahead of admission by a worker
+thread while the request waits. Families are spread over several CUDA
 streams so independent work overlaps on the device. Latency is measured from a request's
 arrival to the CUDA event that completes it; the per-request plain mode executes one
 request at a time with one plan execute each and waits for it, for comparison.
@@ -100,35 +101,81 @@ def _pow2_ceil(v):
 
 
 class Server:
-    def __init__(self, device=None, budget_bytes=120e9, streams=4, torch_module=None):
+    """`budget_bytes` bounds the request buffers in flight; `plan_budget_bytes` bounds the
+    resident plans (least recently used plans are released once their last launch is done)."""
+
+    def __init__(self, device=None, budget_bytes=120e9, streams=4, plan_budget_bytes=16e9):
         import torch
+        from collections import OrderedDict
         self.torch = torch
         self.dev = torch.cuda.current_device() if device is None else device
         self.lib = _provider.load()
         self.api = _provider.provider(self.lib)
         self.budget = float(budget_bytes)
+        self.plan_budget = float(plan_budget_bytes)
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(streams)]
-        self.plans = {}   # (lengths, double, direction, norm, cap) -> (handle, scratch bytes)
-        self.groups = {}  # (n, double) -> handle
+        # (lengths, double, batch class) -> [handle, bytes, last launch event]; both directions
+        # and every normalization run on one plan (syclfft_b200_execute_ex)
+        self.plans = OrderedDict()
+        self.retired = []   # (handle, event): released when the event has completed
+        self.groups = {}    # (n, double) -> handle
         self.err = ctypes.create_string_buffer(ERR)
         self.plan_bytes = 0
+        self.plans_created = 0
+        self.pending = {}   # plan key -> future of a plan being created ahead of use
+        self.pool = None
 
     # ---------------------------------------------------------------- resident state
+    MAX_BATCH = 512
+
+    def _create(self, lengths, double):
+        """Create a resident plan (tables only; any batch up to MAX_BATCH). Thread-safe: called
+        from the plan-prefetch worker too (ctypes releases the GIL during creation)."""
+        err = ctypes.create_string_buffer(ERR)
+        cfg = _provider.make_config(list(lengths), self.MAX_BATCH, -1, double, False, 0, False, self.dev)
+        # scratch comes from the executing stream's arena; creation does not block on the device
+        handle = self.lib.syclfft_b200_create_ex(ctypes.byref(cfg), _provider.CREATE_STREAM_SCRATCH, err, ERR)
+        if not handle:
+            raise RuntimeError(err.value.decode())
+        return handle
+
+    def _prefetch(self, r: Request):
+        key = (r.lengths, r.double)
+        if key in self.plans or key in self.pending or self.pool is None or self.groupable(r):
+            return
+        self.pending[key] = self.pool.submit(self._create, r.lengths, r.double)
+
     def _plan(self, r: Request):
-        cap = _pow2_ceil(r.batch)
-        key = (r.lengths, r.double, r.direction, r.normalization, cap)
+        key = (r.lengths, r.double)
         h = self.plans.get(key)
-        if h is None:
-            cfg = _provider.make_config(list(r.lengths), cap, r.direction, r.double, False, r.normalization,
-                                        False, self.dev)
-            handle = self.api.create(ctypes.byref(cfg), self.err, ERR)
-            if not handle:
-                raise RuntimeError(self.err.value.decode())
-            scratch = int(self.api.scratch_bytes(handle))
-            self.plan_bytes += scratch
-            h = (handle, scratch)
-            self.plans[key] = h
-        return h[0]
+        if h is not None:
+            self.plans.move_to_end(key)
+            return h
+        fut = self.pending.pop(key, None)
+        handle = fut.result() if fut is not None else self._create(r.lengths, r.double)
+        n = math.prod(r.lengths)
+        nbytes = 16 * n * (16 if r.double else 8)  # bound on the tables
+        h = [handle, nbytes, None]
+        self.plans[key] = h
+        self.plan_bytes += nbytes
+        self.plans_created += 1
+        while self.plan_bytes > self.plan_budget and len(self.plans) > 1:
+            _, (oh, ob, oev) = self.plans.popitem(last=False)
+            self.plan_bytes -= ob
+            self.retired.append((oh, oev))
+        self._reap()
+        return h
+
+    def _reap(self, wait=False):
+        keep = []
+        for handle, ev in self.retired:
+            if ev is None or wait or ev.query():
+                if ev is not None and wait:
+                    ev.synchronize()
+                self.api.destroy(handle)
+            else:
+                keep.append((handle, ev))
+        self.retired = keep
 
     def _group(self, n, double):
         key = (n, double)
@@ -144,31 +191,45 @@ class Server:
         return len(r.lengths) == 1 and bool(self.lib.syclfft_b200_group_supports(2 if r.double else 1, r.lengths[0]))
 
     def close(self):
+        for fut in self.pending.values():
+            self.api.destroy(fut.result())
+        self.pending.clear()
         self.torch.cuda.synchronize(self.dev)
-        for handle, _ in self.plans.values():
+        self._reap(wait=True)
+        for handle, _, _ in self.plans.values():
             self.api.destroy(handle)
         for g in self.groups.values():
             self.lib.syclfft_b200_group_destroy(g)
         self.plans.clear()
         self.groups.clear()
+        # hand the request buffers cached by torch back to the device for other pools
+        self.torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- data
     def _fill(self, r: Request, stream):
+        """Input buffer filled with uniform[-1, 1) from the request's seed, and an output buffer.
+        Both come from the allocator's pool of the host thread's current stream (warmed at the
+        start of a run) and are marked as used on `stream`."""
         torch = self.torch
         fdt = torch.float64 if r.double else torch.float32
+        ri = torch.empty(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt)
+        r.inp = torch.view_as_complex(ri.view(-1, 2))
+        r.out = torch.empty_like(r.inp)
+        ri.record_stream(stream)
+        r.out.record_stream(stream)
         with torch.cuda.stream(stream):
             g = torch.Generator(device=f"cuda:{self.dev}")
             g.manual_seed(r.seed)
-            ri = torch.rand(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt, generator=g) * 2 - 1
-            r.inp = torch.view_as_complex(ri.view(-1, 2))
-            r.out = torch.empty_like(r.inp)
+            torch.rand(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt, generator=g, out=ri)
+            ri.mul_(2).sub_(1)
 
     def _execute_one(self, r: Request, stream):
         h = self._plan(r)
-        rc = self.lib.syclfft_b200_execute_batch(h, r.inp.data_ptr(), r.out.data_ptr(), r.batch, stream.cuda_stream,
-                                                 self.err, ERR)
+        rc = self.lib.syclfft_b200_execute_ex(h[0], r.inp.data_ptr(), r.out.data_ptr(), r.batch, r.direction,
+                                              r.normalization, stream.cuda_stream, self.err, ERR)
         if rc:
             raise RuntimeError(self.err.value.decode())
+        return h
 
     def _execute_group(self, key, reqs, stream):
         n, double = key
@@ -193,6 +254,15 @@ class Server:
             r.nbytes = 2 * r.elements * (16 if r.double else 8)
         start = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(self.dev)
+        torch.cuda.empty_cache()
+        # one cached segment the size of the admission budget: request buffers are carved from it
+        # without cudaMalloc during the run
+        free, _ = torch.cuda.mem_get_info(self.dev)
+        # leave room for resident plans and the streams' scratch arenas (CUDA memory pool)
+        warm = int(min(self.budget, free - self.plan_budget - 8e9))
+        if warm > (1 << 20):
+            torch.empty(warm, dtype=torch.uint8, device=f"cuda:{self.dev}")
+        torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
         start.record(self.streams[0])
         done_events = []
@@ -203,9 +273,10 @@ class Server:
                     pass
                 self._fill(r, s)
                 with torch.cuda.stream(s):
-                    self._execute_one(r, s)
+                    h = self._execute_one(r, s)
                     ev = torch.cuda.Event(enable_timing=True)
                     ev.record(s)
+                h[2] = ev
                 ev.synchronize()
                 r.t_done = start.elapsed_time(ev) / 1e3
                 if keep_results:
@@ -224,28 +295,39 @@ class Server:
             "throughput_gflops": total_flops / makespan / 1e9, "throughput_gbs": total_bytes / makespan / 1e9,
             "requests_per_s": len(reqs) / makespan,
             "p50_ms": 1e3 * lat_sorted[len(lat) // 2], "p99_ms": 1e3 * lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))],
-            "mean_ms": 1e3 * statistics.mean(lat), "plans": len(self.plans), "groups": len(self.groups),
-            "plan_scratch_bytes": self.plan_bytes,
+            "mean_ms": 1e3 * statistics.mean(lat), "plans_resident": len(self.plans),
+            "plans_created": self.plans_created, "groups": len(self.groups),
+            "plan_bytes": self.plan_bytes,
         }
 
     def _serve(self, reqs, t0, start, keep_results):
+        from concurrent.futures import ThreadPoolExecutor
+        self.pool = ThreadPoolExecutor(max_workers=2)
+        try:
+            self._serve_loop(reqs, t0, start, keep_results)
+        finally:
+            self.pool.shutdown(wait=True)
+            self.pool = None
+
+    def _serve_loop(self, reqs, t0, start, keep_results):
         torch = self.torch
         nxt = 0
         waiting = deque()
-        in_flight = deque()  # (event, [requests])
-        used = 0.0
         S = len(self.streams)
+        in_flight = [deque() for _ in range(S)]  # per stream, in launch order: (event, [requests])
+        used = 0.0
         completed = 0
         while completed < len(reqs):
             now = time.perf_counter() - t0
             while nxt < len(reqs) and reqs[nxt].arrival <= now:
                 waiting.append(reqs[nxt])
+                self._prefetch(reqs[nxt])  # start its plan while it waits for admission
                 nxt += 1
             # admission by HBM budget (FIFO; a request larger than the budget runs alone)
             bins = {}
             while waiting:
                 r = waiting[0]
-                if used + r.nbytes > self.budget and (used > 0 or in_flight):
+                if used + r.nbytes > self.budget and used > 0:
                     break
                 waiting.popleft()
                 used += r.nbytes
@@ -253,35 +335,44 @@ class Server:
                 bins.setdefault(key, []).append(r)
             # launch everything admitted: one grouped launch per length family
             for key, rs in bins.items():
-                s = self.streams[hash(key) % S]
+                si = hash(key) % S
+                s = self.streams[si]
                 for r in rs:
                     self._fill(r, s)
+                used_plans = []
                 with torch.cuda.stream(s):
                     if key[0] == "g":
                         self._execute_group((key[1], key[2]), rs, s)
                     else:
                         for r in rs:
-                            self._execute_one(r, s)
+                            used_plans.append(self._execute_one(r, s))
                     ev = torch.cuda.Event(enable_timing=True)
                     ev.record(s)
-                in_flight.append((ev, rs))
-            # completions
+                for h in used_plans:
+                    h[2] = ev
+                in_flight[si].append((ev, rs))
+            # completions: work on one stream completes in launch order, so only each
+            # stream's oldest launch needs polling
             progressed = False
-            while in_flight and in_flight[0][0].query():
-                ev, rs = in_flight.popleft()
-                t = start.elapsed_time(ev) / 1e3
-                for r in rs:
-                    r.t_done = t
-                    if keep_results:
-                        r.result = r.out.cpu()
-                    r.inp = r.out = None
-                    used -= r.nbytes
-                completed += len(rs)
-                progressed = True
+            for q in in_flight:
+                while q and q[0][0].query():
+                    ev, rs = q.popleft()
+                    t = start.elapsed_time(ev) / 1e3
+                    for r in rs:
+                        r.t_done = t
+                        if keep_results:
+                            r.result = r.out.cpu()
+                        r.inp = r.out = None
+                        used -= r.nbytes
+                    completed += len(rs)
+                    progressed = True
+            if progressed and self.retired:
+                self._reap()
             if not progressed and not bins:
-                if in_flight and (waiting or nxt >= len(reqs)):
-                    # blocked on memory or draining: wait for the oldest launch
-                    in_flight[0][0].synchronize()
+                busy = [q for q in in_flight if q]
+                if busy and (waiting or nxt >= len(reqs)):
+                    # blocked on memory or draining: wait for the oldest launch of a busy stream
+                    busy[0][0][0].synchronize()
                 elif nxt < len(reqs):
                     # idle until the next arrival (short sleeps keep arrival times honest)
                     gap = reqs[nxt].arrival - (time.perf_counter() - t0)

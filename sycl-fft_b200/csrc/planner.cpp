@@ -257,7 +257,7 @@ struct Builder {
             if (e->radices[i] != p.fft1.radix[i]) return;
         if (p.mode == kModeK) {
             if (p.in.ks != 1 || p.out.ks != 1 || p.n_outer != 1) return;
-            int w = std::max(1, 256 / e->tpl);
+            int w = req.force_w > 0 ? req.force_w : std::max(1, 256 / e->tpl);
             w = static_cast<int>(std::min<int64_t>(w, p.n_cols));
             while (w > 1 && (w * e->tpl > e->maxt || static_cast<int64_t>(w) * p.pitch * cs > smem_limit)) --w;
             p.w = w;
@@ -933,6 +933,7 @@ PlanSpec make_plan(const PlanRequest& req) {
 std::string describe_plan(const PlanSpec& plan) {
     std::ostringstream os;
     os << "{\"elements\":" << plan.elements << ",\"scratch_elements\":" << plan.scratch_elements
+       << ",\"tuning\":" << (plan.tuning.empty() ? std::string("null") : plan.tuning)
        << ",\"scale\":" << plan.scale << ",\"passes\":[";
     for (size_t i = 0; i < plan.passes.size(); ++i) {
         const PassSpec& ps = plan.passes[i];

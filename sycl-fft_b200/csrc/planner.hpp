@@ -116,6 +116,7 @@ struct BluesteinJob {
 struct PlanSpec {
     PlanRequest req;
     std::vector<BluesteinJob> bluestein_jobs;
+    std::string tuning;  // autotuner report (JSON object), empty when not tuned
     uint64_t elements = 0, transform_size = 0;
     double scale = 1.0;
     std::vector<std::vector<std::complex<double>>> tables;

@@ -10,7 +10,9 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <fstream>
 #include <map>
+#include <sstream>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -182,7 +184,7 @@ struct DevicePlan {
 
 // Scratch arenas, one per (device, stream): stream-ordered (cudaMallocAsync on the stream
 // itself), grown on demand, shared by every stream-scratch plan executed on that stream.
-void* stream_arena(int device, cudaStream_t stream, size_t bytes) {
+void* stream_arena(int device, cudaStream_t stream, size_t bytes, bool capturing) {
     struct Arena {
         void* ptr = nullptr;
         size_t size = 0;
@@ -192,6 +194,10 @@ void* stream_arena(int device, cudaStream_t stream, size_t bytes) {
     std::lock_guard<std::mutex> lock(mu);
     Arena& a = arenas[{device, stream}];
     if (a.size < bytes) {
+        // memory allocated inside a CUDA-graph capture would belong to the graph
+        if (capturing)
+            throw std::runtime_error("stream scratch arena too small under CUDA-graph capture: execute this plan once "
+                                     "on the stream before capturing");
         if (a.ptr) check(cudaFreeAsync(a.ptr, stream), "cudaFreeAsync(arena)");
         a.ptr = nullptr;
         a.size = 0;
@@ -236,6 +242,9 @@ DevicePlan* spectrum_plan(int device, int64_t M) {
     return p;
 }
 
+DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::string& tuning);
+PlanRequest tune(const PlanRequest& req, int device, std::string* report);
+
 DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) {
     if (cfg.abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION) throw std::runtime_error("B200 provider ABI mismatch");
     if (cfg.scalar != SYCLFFT_B200_SCALAR_FLOAT && cfg.scalar != SYCLFFT_B200_SCALAR_DOUBLE)
@@ -262,6 +271,16 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     int device = cfg.device;
     if (device < 0) check(cudaGetDevice(&device), "cudaGetDevice");
     DeviceGuard guard(device);
+    std::string tuning;
+    if (cfg.measure) {
+        // planning_mode::measure: time the candidate decompositions and kernels
+        (void)make_plan(req);  // argument validation before any device work
+        req = tune(req, device, &tuning);
+    }
+    return build_plan(req, device, flags, tuning);
+}
+
+DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::string& tuning) {
     int smem_optin = 0;
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "cudaDeviceGetAttribute");
     req.smem_limit = smem_optin;
@@ -270,6 +289,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     auto plan = std::make_unique<DevicePlan>();
     plan->device = device;
     plan->spec = make_plan(req);
+    plan->spec.tuning = tuning;
     const size_t cs = req.dbl ? 16 : 8;
 
     // All tables in one allocation, each 256-byte aligned.
@@ -399,12 +419,27 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     if (!in_place && in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
     std::lock_guard<std::mutex> lock(plan->mu);
     DeviceGuard guard(plan->device);
-    if (plan->ready) check(cudaStreamWaitEvent(stream, plan->ready, 0), "cudaStreamWaitEvent");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
+    if (plan->ready) {
+        if (!capturing) {
+            check(cudaStreamWaitEvent(stream, plan->ready, 0), "cudaStreamWaitEvent");
+        } else {
+            // A graph cannot depend on work outside its capture: finish the plan's tables on
+            // the host now (relaxed mode lets this thread synchronize while a capture is open),
+            // so every replay finds them complete.
+            cudaStreamCaptureMode mode = cudaStreamCaptureModeRelaxed;
+            check(cudaThreadExchangeStreamCaptureMode(&mode), "cudaThreadExchangeStreamCaptureMode");
+            const cudaError_t e = cudaEventSynchronize(plan->ready);
+            cudaThreadExchangeStreamCaptureMode(&mode);
+            check(e, "cudaEventSynchronize(tables)");
+        }
+    }
     void* scratch = plan->scratch;
     if (plan->stream_scratch && plan->spec.scratch_elements) {
         const size_t need = plan->spec.scratch_elements / planned * batch * (plan->spec.req.dbl ? 16 : 8) + 256;
-        scratch = stream_arena(plan->device, stream, std::max<size_t>(need, plan->spec.scratch_elements / planned * batch *
-                                                                               (plan->spec.req.dbl ? 16 : 8)));
+        scratch = stream_arena(plan->device, stream, need, capturing);
     }
     const int dir = direction == 0 ? plan->spec.req.direction : direction;
     const int norm = normalization < 0 ? plan->spec.req.normalization : normalization;
@@ -440,7 +475,157 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
                   "FFT pass launch");
         }
     }
-    check(cudaEventRecord(plan->done, stream), "cudaEventRecord");
+    // Under capture the record becomes a node of the graph, so destroying the plan still
+    // waits for the last replay that used its tables and scratch.
+    check(capturing ? cudaEventRecordWithFlags(plan->done, stream, cudaEventRecordExternal)
+                    : cudaEventRecord(plan->done, stream),
+          "cudaEventRecord");
+}
+
+// ---------------------------------------------------------------- autotuner
+struct Knobs {
+    const char* name;
+    bool no_fixed, no_piped, no_cluster;
+    int cluster_p, force_w, force_maxv;
+};
+
+std::string tune_key(const PlanRequest& r, int device) {
+    cudaDeviceProp prop{};
+    cudaGetDeviceProperties(&prop, device);
+    std::ostringstream k;
+    k << prop.name << "|" << (r.dbl ? "z" : "c") << "|" << (r.in_place ? "ip" : "oop") << "|b" << r.batch;
+    for (auto v : r.shape) k << "|" << v;
+    return k.str();
+}
+
+// Decisions survive the process when SYCLFFT_B200_TUNE_CACHE names a file (one line per key).
+std::map<std::string, std::string>& tune_cache() {
+    static std::map<std::string, std::string> cache;
+    static bool loaded = false;
+    if (!loaded) {
+        loaded = true;
+        if (const char* path = std::getenv("SYCLFFT_B200_TUNE_CACHE")) {
+            std::ifstream in(path);
+            std::string key, value;
+            while (std::getline(in, key, '\t') && std::getline(in, value)) cache[key] = value;
+        }
+    }
+    return cache;
+}
+
+float time_candidate(DevicePlan* plan, int64_t batch, void* a, void* b) {
+    cudaStream_t s = nullptr;
+    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    void* out = plan->spec.req.in_place ? a : b;
+    float best = 1e30f;
+    try {
+        for (int i = 0; i < 2; ++i) execute_plan(plan, a, out, s, static_cast<uint64_t>(batch));
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, s);
+            for (int i = 0; i < 3; ++i) execute_plan(plan, a, out, s, static_cast<uint64_t>(batch));
+            cudaEventRecord(e1, s);
+            check(cudaEventSynchronize(e1), "autotune timing");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best = std::min(best, ms / 3);
+        }
+    } catch (...) {
+        best = 1e30f;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    return best;
+}
+
+PlanRequest apply(PlanRequest r, const Knobs& k) {
+    r.no_fixed = k.no_fixed;
+    r.no_piped = k.no_piped;
+    r.no_cluster = k.no_cluster;
+    r.cluster_p = k.cluster_p;
+    r.force_w = k.force_w;
+    r.force_maxv = k.force_maxv;
+    return r;
+}
+
+PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
+    static const Knobs kCandidates[] = {
+        {"default", false, false, false, 0, 0, 0},    {"generic", true, false, false, 0, 0, 0},
+        {"no_pipeline", false, true, false, 0, 0, 0}, {"cluster8", false, false, false, 8, 0, 0},
+        {"cluster16", false, false, false, 16, 0, 0}, {"w1", false, false, false, 0, 1, 0},
+        {"w2", false, false, false, 0, 2, 0},         {"w4", false, false, false, 0, 4, 0},
+        {"maxv16", true, false, false, 0, 0, 16},
+    };
+    const std::string key = tune_key(req, device);
+    auto& cache = tune_cache();
+    auto hit = cache.find(key);
+    if (hit != cache.end()) {
+        for (const auto& k : kCandidates)
+            if (hit->second == k.name) {
+                *report = std::string("{\"choice\":\"") + k.name + "\",\"cached\":true}";
+                return apply(req, k);
+            }
+    }
+    const size_t cs = req.dbl ? 16 : 8;
+    const uint64_t elements = checked_element_count(req.shape, req.batch);
+    const uint64_t per = elements / req.batch;
+    // time on at most ~256 MB per buffer: a sub-batch has the same per-line kernel behaviour
+    const int64_t batch = static_cast<int64_t>(std::max<uint64_t>(1, std::min<uint64_t>(req.batch, (uint64_t(256) << 20) / (per * cs))));
+    void *a = nullptr, *b = nullptr;
+    check(cudaMalloc(&a, batch * per * cs), "cudaMalloc(autotune)");
+    if (cudaMalloc(&b, batch * per * cs) != cudaSuccess) {
+        cudaFree(a);
+        throw std::runtime_error("cudaMalloc(autotune)");
+    }
+    cudaMemset(a, 0, batch * per * cs);
+    std::ostringstream rep;
+    rep << "{\"timed_batch\":" << batch << ",\"candidates\":{";
+    std::string best_name = "default";
+    float best = 1e30f;
+    std::vector<std::string> seen;
+    bool first = true;
+    for (const auto& k : kCandidates) {
+        PlanRequest r = apply(req, k);
+        std::string desc;
+        try {
+            PlanRequest rd = r;
+            rd.device_spectrum = true;  // the description does not need the chirp spectra
+            desc = describe_plan(make_plan(rd));
+        } catch (...) {
+            continue;
+        }
+        if (std::find(seen.begin(), seen.end(), desc) != seen.end()) continue;  // same kernels as an earlier one
+        seen.push_back(desc);
+        std::unique_ptr<DevicePlan> p;
+        try {
+            p.reset(build_plan(r, device, SYCLFFT_B200_CREATE_SYNC, ""));
+        } catch (...) {
+            continue;
+        }
+        const float ms = time_candidate(p.get(), batch, a, b);
+        rep << (first ? "" : ",") << "\"" << k.name << "\":" << ms;
+        first = false;
+        if (ms < best) {
+            best = ms;
+            best_name = k.name;
+        }
+    }
+    cudaDeviceSynchronize();
+    cudaFree(a);
+    cudaFree(b);
+    rep << "},\"choice\":\"" << best_name << "\"}";
+    *report = rep.str();
+    cache[key] = best_name;
+    if (const char* path = std::getenv("SYCLFFT_B200_TUNE_CACHE")) {
+        std::ofstream out(path, std::ios::app);
+        out << key << '\t' << best_name << '\n';
+    }
+    for (const auto& k : kCandidates)
+        if (best_name == k.name) return apply(req, k);
+    return req;
 }
 
 int p_supports(int32_t device, char* err, size_t cap) {

@@ -215,9 +215,13 @@ class Plan:
         torch = _torch()
         s = stream or torch.cuda.current_stream(self._device)
         with self._lock:
+            with torch.cuda.stream(s):
+                capturing = torch.cuda.is_current_stream_capturing()
             for dep in dependencies or ():
                 s.wait_event(dep)
-            if self._last_event is not None:
+            if self._last_event is not None and not capturing:
+                # A graph cannot depend on work outside its capture; captured launches run
+                # only at replay, which the caller orders against earlier executes.
                 s.wait_event(self._last_event)
             err = ctypes.create_string_buffer(_provider.ERR_CAP)
             rc = self._api.execute(self._handle, inp, out, s.cuda_stream, err, _provider.ERR_CAP)
@@ -225,7 +229,9 @@ class Plan:
                 raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
             ev = torch.cuda.Event()
             ev.record(s)
-            self._last_event = ev
+            # an event recorded inside a capture belongs to the graph: ordering of replays
+            # against later executes is the caller's, as for any captured work
+            self._last_event = None if capturing else ev
             return ev
 
     def close(self):

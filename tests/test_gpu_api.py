@@ -99,3 +99,26 @@ def test_raw_c_abi(sf, torch):
     assert not api.create(ctypes.byref(bad), err, 1024) and b"ABI" in err.value
     bad = _provider.make_config([16], 1, 0)
     assert not api.create(ctypes.byref(bad), err, 1024) and b"direction" in err.value
+
+
+@pytest.mark.parametrize("shape,batch,dbl", [([4096], 512, False), ([13440], 64, False), ([65536], 8, True),
+                                             ([1009], 32, False), ([64, 64], 4, True)], ids=str)
+def test_autotuned_plans(sf, torch, shape, batch, dbl, tmp_path, monkeypatch):
+    """planning_mode::measure times candidate kernels, reports them, keeps the fastest, and
+    reuses the decision from the on-disk cache."""
+    from conftest import fp64_fft, rel_l2, uniform_complex
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("SYCLFFT_B200_TUNE_CACHE", str(cache))
+    opts = sf.plan_options(planning=sf.planning_mode.measure)
+    kind = "double" if dbl else "float"
+    p = sf.plan_many_dft(kind, shape, batch, sf.direction.forward, opts)
+    tuning = p.describe()["tuning"]
+    assert tuning["choice"] and (tuning.get("cached") or len(tuning["candidates"]) >= 1), tuning
+    n = int(np.prod(shape))
+    x = uniform_complex(n * batch, n, np.complex128 if dbl else np.complex64)
+    xt = torch.from_numpy(x).cuda()
+    out = torch.empty_like(xt)
+    p.execute(xt, out).synchronize()
+    tol = (1e-12 if dbl else 1e-5) * max(1.0, np.log2(n))
+    assert rel_l2(out.cpu().numpy(), fp64_fft(x, shape, batch, -1)) <= tol
+    assert cache.exists()

@@ -125,3 +125,54 @@ def test_serving_alone_vs_mix(torch):
         assert mixed["groups"] >= 1
     finally:
         srv.close()
+
+
+def test_cuda_graph_capture_and_replay(torch):
+    """Plan executes and grouped launches are capturable in a CUDA graph; replays with new
+    input data give the same results as direct execution."""
+    import syclfft_b200 as sf
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal)
+    plans = [sf.plan_many_dft("float", [4096], 64, sf.direction.forward, opts),
+             sf.plan_many_dft("double", [65536], 4, sf.direction.backward, opts),
+             sf.plan_many_dft("float", [1009], 16, sf.direction.forward, opts)]
+    bufs = [torch.randn(4096 * 64, dtype=torch.complex64, device="cuda"),
+            torch.randn(65536 * 4, dtype=torch.complex128, device="cuda"),
+            torch.randn(1009 * 16, dtype=torch.complex64, device="cuda")]
+    g = lib.syclfft_b200_group_create(1, 256, -1, err, 1024)
+    ga = torch.randn(256 * 8, dtype=torch.complex64, device="cuda")
+    gb = torch.randn(256 * 3, dtype=torch.complex64, device="cuda")
+    items = (_provider.GroupItemV1 * 2)()
+    items[0].in_, items[0].out, items[0].batch, items[0].direction, items[0].normalization = ga.data_ptr(), ga.data_ptr(), 8, -1, 0
+    items[1].in_, items[1].out, items[1].batch, items[1].direction, items[1].normalization = gb.data_ptr(), gb.data_ptr(), 3, 1, 2
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+
+    def step():
+        for p, b in zip(plans, bufs):
+            p.execute(b, stream=s)
+        assert lib.syclfft_b200_group_execute(g, items, 2, s.cuda_stream, err, 1024) == 0, err.value
+
+    with torch.cuda.stream(s):
+        step()  # warm-up outside capture (kernel attributes, tables)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s):
+        step()
+    for trial in range(2):
+        inputs = [b.clone().normal_() for b in bufs] + [ga.clone().normal_(), gb.clone().normal_()]
+        for dst, src in zip(bufs + [ga, gb], inputs):
+            dst.copy_(src)
+        graph.replay()
+        torch.cuda.synchronize()
+        for (p, b, x) in zip(plans, bufs, inputs):
+            n = int(np.prod(p.shape()))
+            d = int(p.direction())
+            ref = fp64_fft(x.cpu().numpy(), p.shape(), p.batch_count(), d, 1 / math.sqrt(n))
+            assert rel_l2(b.cpu().numpy(), ref) <= spec_tol(n, b.dtype == torch.complex128)
+        assert rel_l2(ga.cpu().numpy(), fp64_fft(inputs[3].cpu().numpy(), [256], 8, -1)) <= spec_tol(256, False)
+        assert rel_l2(gb.cpu().numpy(), fp64_fft(inputs[4].cpu().numpy(), [256], 3, 1, 1 / 256)) <= spec_tol(256, False)
+    del graph
+    lib.syclfft_b200_group_destroy(g)

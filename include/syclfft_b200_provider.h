@@ -98,9 +98,16 @@ SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
  * scratch; each execute borrows a scratch arena of the executing stream (stream-ordered,
  * grown on demand), so many resident plans cost only their tables.
  * SYCLFFT_B200_CREATE_SYNC -- return only when the tables are on the device (create()
- * does this); without it, executes wait for the tables on the device and the host does not. */
+ * does this); without it, executes wait for the tables on the device and the host does not.
+ * SYCLFFT_B200_CREATE_SPLIT_BF16 -- complex<float> plans only (ignored for double): axes whose
+ * length has a tensor-core kernel (256 and 4096 points, contiguous lines; 256 on strided
+ * axes) run their radix-16 butterflies as BF16 hi/lo matrix products with FP32 accumulation
+ * on the tensor cores; all other passes, the twiddles and the exchanges stay FP32. Results
+ * are within about 1e-5 relative L2 of the exact transform (see the error reports of the
+ * tests); the reference has no counterpart (an extension of this provider). */
 #define SYCLFFT_B200_CREATE_STREAM_SCRATCH 1u
 #define SYCLFFT_B200_CREATE_SYNC 2u
+#define SYCLFFT_B200_CREATE_SPLIT_BF16 4u
 SYCLFFT_B200_EXPORT void *syclfft_b200_create_ex(const syclfft_b200_plan_config_v1 *config, uint32_t flags, char *err,
                                                  size_t cap);
 /* Like execute, for the first `batch` transforms only (1 <= batch <= the plan's

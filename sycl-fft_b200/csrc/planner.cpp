@@ -3,6 +3,8 @@
 #include "cluster_catalog.h"
 #include "fixed_catalog.h"
 #include "piped_catalog.h"
+#include "tc_catalog.h"
+#include "tc_shape.h"
 
 #include <algorithm>
 #include <cmath>
@@ -184,6 +186,36 @@ struct Builder {
         const int id = add_table(*tw);
         seq_tables[key] = id;
         return id;
+    }
+
+    // Split-precision tensor-core kernel for a plain single-pass axis of a float plan: the
+    // line length must be a catalog length (radix-16 powers) and the pass must carry no
+    // fused extras (those are the Bluestein and four-step passes, which stay FP32).
+    void try_tc(PassSpec& ps) {
+        PassParams& p = ps.p;
+        if (req.dbl || ps.kind != "single" || p.fft2.nstages != 0 || p.in_len != p.n || p.out_len != p.n ||
+            ps.tables.premul >= 0 || ps.tables.pointwise >= 0 || ps.tables.postmul >= 0 || p.tw4_sign != 0 ||
+            p.store_via_smem || p.ts_rows)
+            return;
+        const bool cols = p.mode == kModeC;
+        const TcEntry* e = find_tc(p.n, cols);
+        if (!e || e->smem > smem_limit) return;
+        if (cols ? (p.in.cs != 1 || p.out.cs != 1) : (p.in.ks != 1 || p.out.ks != 1)) return;
+        const int64_t n = p.n;
+        auto tw = cached_table({n, -400}, [&] {
+            // two levels: W_n^(64a) for a < ceil(n/64), then W_n^b for b < 64
+            std::vector<std::complex<double>> t;
+            for (int64_t a = 0; a < (n + 63) / 64; ++a) t.push_back(cis_neg(64 * a, n));
+            for (int64_t b = 0; b < 64; ++b) t.push_back(cis_neg(b, n));
+            return t;
+        });
+        ps.tables.tc_tw = add_table(*tw);
+        ps.tc_id = e->id;
+        ps.threads = e->threads;
+        ps.smem_bytes = e->smem;
+        p.w = e->l;
+        p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+        p.tiles = p.n_outer * p.col_tiles;
     }
 
     void use_base_table(PassSpec& ps) {
@@ -382,6 +414,7 @@ struct Builder {
                 set_fft(ps, p.fft1, &ps.tables.tw1, p.n, cfg);
                 geometry(ps, cfg, req.force_w);
                 try_fixed(ps, cfg);
+                if (req.split_bf16) try_tc(ps);
                 ps.src = cur;
                 ps.dst = Buf::Output;
                 ps.bytes_moved = 2 * E * cs;
@@ -890,6 +923,17 @@ const PipedEntry* find_piped(bool dbl, int n) {
     return nullptr;
 }
 
+#define SFB_TENTRY(ID, R, S, L, COLS, G) \
+    TcEntry{ID, R, S, L, COLS, TcShape<R, S, L, G>::N, TcShape<R, S, L, G>::THREADS, int64_t(TcShape<R, S, L, G>::SMEM)},
+const TcEntry kTc[] = {SFB_TC_CATALOG(SFB_TENTRY)};
+#undef SFB_TENTRY
+
+const TcEntry* find_tc(int n, bool cols) {
+    for (const TcEntry& e : kTc)
+        if (e.n == n && (e.cols != 0) == cols) return &e;
+    return nullptr;
+}
+
 const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
     for (const FixedEntry& e : kFixed)
         if (e.dbl == (dbl ? 1 : 0) && e.modec == (mode == kModeC ? 1 : 0) && e.n == n && e.feat == feat) return &e;
@@ -947,7 +991,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
-           << ",\"piped_id\":" << ps.piped_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
            << ps.cl_p << "]}";
     }
     os << "]}";

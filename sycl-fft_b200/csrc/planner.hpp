@@ -30,6 +30,7 @@ enum class Buf : int { Input = 0, Output = 1, Scratch = 2 };
 
 struct TableIds {
     int tw1 = -1, tw2 = -1, premul = -1, pointwise = -1, postmul = -1, tw4_hi = -1, tw4_lo = -1;
+    int tc_tw = -1;  // two-level W_N^k table of the tensor-core kernel
 };
 
 struct KernelChoice {
@@ -57,6 +58,7 @@ struct PassSpec {
     int piped_id = -1;       // copy-engine-pipelined kernel (piped_catalog.h), used when the
                              // buffers are 16-byte aligned; otherwise fixed_id runs
     int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
+    int tc_id = -1;          // split-precision tensor-core kernel (tc_catalog.h), float plans only
 };
 
 // One entry of cluster_catalog.h as seen by the host.
@@ -85,6 +87,15 @@ struct PipedEntry {
 };
 const PipedEntry* find_piped(bool dbl, int n);
 
+// One entry of tc_catalog.h (split-precision tensor-core kernels, complex<float> only).
+struct TcEntry {
+    int id, r, s, l, cols;
+    int n, threads;
+    int64_t smem;
+};
+// Entry for a line length and layout (cols: the lines are adjacent columns), or nullptr.
+const TcEntry* find_tc(int n, bool cols);
+
 struct PlanRequest {
     bool dbl = false;
     int direction = -1;      // -1 forward, +1 backward
@@ -101,6 +112,9 @@ struct PlanRequest {
     bool no_piped = false;   // never use the copy-engine-pipelined kernels
     int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size
     bool device_spectrum = false;  // leave Bluestein chirp/spectrum tables to the device (zeroed here)
+    // complex<float> only: run the radix-16 butterflies of eligible single-pass axes as BF16
+    // hi/lo matrix products on the tensor cores (FP32 accumulation); other passes stay FP32
+    bool split_bf16 = false;
 };
 
 // A Bluestein axis whose chirp and chirp spectrum the provider generates on the device

@@ -26,6 +26,7 @@
 #include "fixed_launch.hpp"
 #include "launch.hpp"
 #include "piped_launch.hpp"
+#include "tc_launch.hpp"
 #include "planner.hpp"
 
 namespace sfb {
@@ -72,7 +73,24 @@ struct BoundPass {
     FixedParams fp;    // used when spec.fixed_id >= 0
     ClusterParams cp;  // used when spec.cluster_id >= 0
     PipedParams pp;    // used when spec.piped_id >= 0 and the buffers are 16-byte aligned
+    TcParams tp;       // used when spec.tc_id >= 0
 };
+
+TcParams to_tc(const PassParams& p, const void* tw, int* status) {
+    TcParams q;
+    q.n_outer = p.n_outer;
+    q.n_cols = p.n_cols;
+    q.col_tiles = p.col_tiles;
+    q.tiles = p.tiles;
+    q.in = p.in;
+    q.out = p.out;
+    q.scale = static_cast<float>(p.scale);
+    q.conj_in = p.conj_in;
+    q.conj_out = p.conj_out;
+    q.tw = tw;
+    q.status = status;
+    return q;
+}
 
 PipedParams to_piped(const PassParams& p, int* status) {
     PipedParams q;
@@ -257,6 +275,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     req.in_place = cfg.in_place != 0;
     req.shape.assign(cfg.lengths, cfg.lengths + cfg.rank);
     req.batch = cfg.batch_count;
+    req.split_bf16 = !req.dbl && (flags & SYCLFFT_B200_CREATE_SPLIT_BF16) != 0;
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
@@ -285,6 +304,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
     check(cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "cudaDeviceGetAttribute");
     req.smem_limit = smem_optin;
     req.device_spectrum = true;
+    if (flags & SYCLFFT_B200_CREATE_SPLIT_BF16) req.split_bf16 = !req.dbl;
 
     auto plan = std::make_unique<DevicePlan>();
     plan->device = device;
@@ -346,7 +366,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
     };
     for (const PassSpec& ps : plan->spec.passes) {
-        if (ps.fixed_id < 0 && ps.cluster_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
+        if (ps.fixed_id < 0 && ps.cluster_id < 0 && ps.tc_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
             throw std::runtime_error("no kernel variant for pass");
         BoundPass bp;
         bp.spec_ptr = &ps;  // plan->spec.passes is not modified after this point
@@ -361,6 +381,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         bp.fp = to_fixed(bp.p);
         bp.cp = to_cluster(bp.p);
         bp.pp = to_piped(bp.p, plan->status);
+        bp.tp = to_tc(bp.p, tab(ps.tables.tc_tw), plan->status);
         plan->passes.push_back(bp);
     }
     return plan.release();
@@ -381,6 +402,10 @@ BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
     r.fp.col_tiles = p.col_tiles;
     r.cp.lines = p.n_cols;
     r.pp.lines = p.n_cols;
+    r.tp.n_outer = p.n_outer;
+    r.tp.n_cols = p.n_cols;
+    r.tp.col_tiles = p.col_tiles;
+    r.tp.tiles = p.tiles;
     if (bp.spec_ref().cluster_id >= 0) p.tiles = p.n_cols * bp.spec_ref().cl_p;
     return r;
 }
@@ -395,16 +420,19 @@ void apply_override(BoundPass& bp, bool first, bool last, bool flip, double scal
             bp.fp.conj_in ^= 1;
             bp.cp.conj_in ^= 1;
             bp.pp.conj_in ^= 1;
+            bp.tp.conj_in ^= 1;
         }
         if (last) {
             bp.p.conj_out ^= 1;
             bp.fp.conj_out ^= 1;
             bp.cp.conj_out ^= 1;
             bp.pp.conj_out ^= 1;
+            bp.tp.conj_out ^= 1;
         }
     }
     if (last && set_scale) {
         bp.p.scale = bp.fp.scale = bp.cp.scale = bp.pp.scale = scale;
+        bp.tp.scale = static_cast<float>(scale);
     }
 }
 
@@ -456,7 +484,10 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
         };
         const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().src)) % 16 == 0) &&
                              (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().dst)) % 16 == 0);
-        if (bp.spec_ref().piped_id >= 0 && aligned) {
+        if (bp.spec_ref().tc_id >= 0) {
+            check(launch_tc(bp.spec_ref().tc_id, bp.tp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
+                  "FFT tensor-core pass launch");
+        } else if (bp.spec_ref().piped_id >= 0 && aligned) {
             const int64_t lines = bp.pp.lines;
             const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
             check(launch_piped(bp.spec_ref().piped_id, bp.pp, grid, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
@@ -493,7 +524,8 @@ std::string tune_key(const PlanRequest& r, int device) {
     cudaDeviceProp prop{};
     cudaGetDeviceProperties(&prop, device);
     std::ostringstream k;
-    k << prop.name << "|" << (r.dbl ? "z" : "c") << "|" << (r.in_place ? "ip" : "oop") << "|b" << r.batch;
+    k << prop.name << "|" << (r.dbl ? "z" : (r.split_bf16 ? "c-tc" : "c")) << "|" << (r.in_place ? "ip" : "oop")
+      << "|b" << r.batch;
     for (auto v : r.shape) k << "|" << v;
     return k.str();
 }

@@ -18,6 +18,7 @@ PROVIDER_PATH = os.path.join(PROVIDER_DIR, "syclfft_provider_b200.so")
 ABI_VERSION = 1
 CREATE_STREAM_SCRATCH = 1
 CREATE_SYNC = 2
+CREATE_SPLIT_BF16 = 4
 SCALAR_FLOAT = 1
 SCALAR_DOUBLE = 2
 ERR_CAP = 1024

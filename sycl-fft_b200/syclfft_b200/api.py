@@ -78,6 +78,10 @@ class plan_options:
     normalization: normalization = normalization.none
     planning: planning_mode = planning_mode.estimate
     preferred_provider: provider = provider.automatic
+    # B200 extension (no counterpart in syclfft::plan_options): complex<float> plans run the
+    # radix-16 butterflies of eligible axes (256 / 4096 points) as BF16 hi/lo matrix products
+    # with FP32 accumulation on the tensor cores; ignored for complex<double>.
+    split_precision: bool = False
 
 
 def _torch():
@@ -138,7 +142,11 @@ class Plan:
                                     options.placement == placement.in_place, int(options.normalization),
                                     options.planning == planning_mode.measure, self._device)
         self._cfg = cfg
-        h = self._api.create(ctypes.byref(cfg), err, _provider.ERR_CAP)
+        if options.split_precision and not self._double:
+            h = self._lib.syclfft_b200_create_ex(ctypes.byref(cfg), _provider.CREATE_SYNC | _provider.CREATE_SPLIT_BF16,
+                                                 err, _provider.ERR_CAP)
+        else:
+            h = self._api.create(ctypes.byref(cfg), err, _provider.ERR_CAP)
         if not h:
             raise SyclfftError(error_code.planning_failed, err.value.decode() or "B200 plan creation failed")
         self._handle = h

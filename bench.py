@@ -417,6 +417,135 @@ def run_ours(args):
     return 0
 
 
+def _plane_wave_input(shape, seed, dtype):
+    """uniform[-1,1) complex plus a sum of 8 random plane waves (integer wave vectors)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    n = math.prod(shape)
+    x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).reshape(shape)
+    idx = np.indices(shape, dtype=np.float64)
+    for _ in range(8):
+        k = [int(rng.integers(-s // 2, s // 2)) for s in shape]
+        amp, ph = rng.uniform(0.5, 2.0), rng.uniform(0, 2 * np.pi)
+        arg = sum(2 * np.pi * k[a] * idx[a] / shape[a] for a in range(len(shape)))
+        x = x + amp * np.exp(1j * (arg + ph))
+    return x.reshape(-1).astype(dtype)
+
+
+def _errors(got, ref):
+    import numpy as np
+    d = got.astype(np.complex128) - ref
+    return {"rel_l2": float(np.linalg.norm(d) / np.linalg.norm(ref)),
+            "max_rel": float(np.abs(d).max() / np.abs(ref).max())}
+
+
+def run_config(args):
+    """Secondary configurations, one JSON line each (device-resident, CUDA-event timed):
+    3: Bluestein primes N in {1009, 4099, 65537}, c64 and c128, batch 256, out of place,
+       forward normalization, complex Gaussian inputs; errors against an FP64 direct DFT
+       (N=1009) or an FP64 FFT (others), on the first 8 lines.
+    4: 3D c64 256^3 in place forward+backward with backward normalization (split-precision
+       tensor-core path and pure FP32) and 2D c128 2048^2 out of place forward+backward;
+       inputs uniform plus 8 plane waves; errors of the forward result against FP64."""
+    import numpy as np
+    import torch
+    import syclfft_b200 as sf
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    peak, peak_kind = measured_peaks()
+
+    def timed(fn, reps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    cases = []
+    reps = max(5, min(args.steps, 200))
+    if args.config == 3:
+        for n in (1009, 4099, 65537):
+            for dbl in (False, True):
+                batch = 256
+                rng = np.random.default_rng(n + dbl)
+                dt = np.complex128 if dbl else np.complex64
+                x = (rng.standard_normal(n * batch) + 1j * rng.standard_normal(n * batch)).astype(dt)
+                opts = sf.plan_options(placement=sf.placement.out_of_place, normalization=sf.normalization.forward)
+                p = sf.plan_many_dft("double" if dbl else "float", [n], batch, sf.direction.forward, opts)
+                xi = torch.from_numpy(x).to(dev)
+                out = torch.empty_like(xi)
+                ms = timed(lambda: p.execute(xi, out), reps)
+                got = out[: 8 * n].cpu().numpy().reshape(8, n)
+                xs = x[: 8 * n].reshape(8, n).astype(np.complex128)
+                if n == 1009:
+                    k = np.arange(n)
+                    ref = xs @ np.exp(-2j * np.pi * np.outer(k, k) / n) / n
+                else:
+                    ref = np.fft.fft(xs, axis=1) / n
+                nbytes = 2 * n * batch * (16 if dbl else 8)
+                cases.append({"case": f"{'c128' if dbl else 'c64'}_N{n}x{batch}", "ms": round(ms, 4),
+                              "gflops": round(flops([n], batch) / ms / 1e6, 1),
+                              "gbs_alg": round(nbytes / ms / 1e6, 1),
+                              "frac_of_peak": round(nbytes / ms / 1e6 / peak, 4),
+                              "launches": p.launches(),
+                              "passes": [ps["kind"] for ps in p.describe()["passes"]],
+                              "oracle": "fp64 direct DFT" if n == 1009 else "fp64 FFT",
+                              **_errors(got.reshape(-1), ref.reshape(-1))})
+    else:
+        shape = [256, 256, 256]
+        x = _plane_wave_input(shape, 404, np.complex64)
+        ref = np.fft.fftn(x.reshape(shape).astype(np.complex128)).reshape(-1)
+        for split in (True, False):
+            opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.backward,
+                                   split_precision=split)
+            f = sf.plan_many_dft("float", shape, 1, sf.direction.forward, opts)
+            b = sf.plan_many_dft("float", shape, 1, sf.direction.backward, opts)
+            buf = torch.from_numpy(x).to(dev)
+            f.execute(buf)
+            fwd = buf.cpu().numpy()
+            b.execute(buf)
+            back = buf.cpu().numpy()
+            ms = timed(lambda: (f.execute(buf), b.execute(buf)), reps)
+            nbytes = 2 * 2 * x.size * 8
+            tc = sum(1 for ps in f.describe()["passes"] if ps.get("tc_id", -1) >= 0)
+            cases.append({"case": f"c64_256^3_{'split_bf16' if split else 'fp32'}", "ms_fwd_bwd": round(ms, 4),
+                          "gflops": round(2 * flops(shape, 1) / ms / 1e6, 1), "gbs_alg": round(nbytes / ms / 1e6, 1),
+                          "launches": f.launches() + b.launches(), "tensor_core_passes": tc,
+                          "forward": _errors(fwd, ref), "round_trip": _errors(back, x.astype(np.complex128))})
+        shape = [2048, 2048]
+        x = _plane_wave_input(shape, 2048, np.complex128)
+        ref = np.fft.fftn(x.reshape(shape)).reshape(-1)
+        opts = sf.plan_options(placement=sf.placement.out_of_place)
+        f = sf.plan_many_dft("double", shape, 1, sf.direction.forward, opts)
+        b = sf.plan_many_dft("double", shape, 1, sf.direction.backward, opts)
+        xi = torch.from_numpy(x).to(dev)
+        y = torch.empty_like(xi)
+        z = torch.empty_like(xi)
+        f.execute(xi, y)
+        fwd = y.cpu().numpy()
+        ms = timed(lambda: (f.execute(xi, y), b.execute(y, z)), reps)
+        nbytes = 2 * 2 * x.size * 16
+        cases.append({"case": "c128_2048^2_out_of_place", "ms_fwd_bwd": round(ms, 4),
+                      "gflops": round(2 * flops(shape, 1) / ms / 1e6, 1), "gbs_alg": round(nbytes / ms / 1e6, 1),
+                      "launches": f.launches() + b.launches(), "forward": _errors(fwd, ref)})
+    total_flops = sum(c["gflops"] * c.get("ms", c.get("ms_fwd_bwd")) for c in cases)
+    total_ms = sum(c.get("ms", c.get("ms_fwd_bwd")) for c in cases)
+    line = {"metric": f"config {args.config}: GFLOP/s (5N log2N) and accuracy vs FP64", "unit": UNIT,
+            "value": round(total_flops / total_ms, 1), "higher_is_better": True, "n_gpus": 1,
+            "data": "synthetic (seeded)", "peak_gbs": peak, "peak_source": peak_kind,
+            "config": {"workload": "config3_bluestein" if args.config == 3 else "config4_multidim",
+                       "l2": "inputs larger than L2 except where a case's buffer is smaller"},
+            "cases": cases}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_serve(args):
     """Serving configuration: the mixed request stream through the continuous-batching loop
     and through per-request plain executes; one JSON line with both."""
@@ -458,6 +587,8 @@ def main():
     ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
     ap.add_argument("--plan", default="", help="replace the workload: N[xM[xK]]:batch:c64|c128[,...]")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
+    ap.add_argument("--config", type=int, choices=[3, 4], default=0,
+                    help="run a secondary configuration instead (3: Bluestein primes, 4: 3D/2D)")
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rate", type=float, default=50000.0)
     ap.add_argument("--budget-gb", type=float, default=120.0)
@@ -468,6 +599,8 @@ def main():
         return run_reference(args)
     if args.serve:
         return run_serve(args)
+    if args.config:
+        return run_config(args)
     return run_ours(args)
 
 

@@ -163,6 +163,30 @@ void set_err(char* err, size_t cap, const std::string& m) {
 
 }  // namespace
 
+// Plan description only (no execution): the planner's choice for a request.
+extern "C" int emu_describe(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
+                            uint64_t batch, int force_maxv, int smem_limit, int split_bf16, char* desc,
+                            size_t desc_cap, char* err, size_t cap) {
+    try {
+        PlanRequest req;
+        req.dbl = dbl != 0;
+        req.direction = dir;
+        req.normalization = norm;
+        req.in_place = in_place != 0;
+        req.shape.assign(shape, shape + rank);
+        req.batch = batch;
+        req.force_maxv = force_maxv;
+        req.smem_limit = smem_limit;
+        req.split_bf16 = split_bf16 != 0;
+        req.device_spectrum = true;
+        set_err(desc, desc_cap, describe_plan(make_plan(req)));
+        return 0;
+    } catch (const std::exception& e) {
+        set_err(err, cap, e.what());
+        return 1;
+    }
+}
+
 extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
                        uint64_t batch, int force_maxv, int smem_limit, const double* in, double* out,
                        char* desc, size_t desc_cap, char* err, size_t cap) {

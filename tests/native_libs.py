@@ -44,3 +44,19 @@ def emulate(x, shape, batch, direction, norm=0, double=False, in_place=False, fo
     if rc:
         raise RuntimeError(err.value.decode())
     return out, json.loads(desc.value.decode())
+
+
+def describe(shape, batch, direction=-1, norm=0, double=False, in_place=False, smem_limit=232448, split_bf16=False):
+    """The planner's plan for a request (no execution), as the provider describes it."""
+    L = _load("libplan_emulator.so")
+    L.emu_describe.argtypes = [ctypes.c_int] * 4 + [ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                                    ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t,
+                                                    ctypes.c_char_p, ctypes.c_size_t]
+    sh = (ctypes.c_uint64 * 3)(*(list(shape) + [0] * (3 - len(shape))))
+    desc = ctypes.create_string_buffer(1 << 18)
+    err = ctypes.create_string_buffer(1024)
+    rc = L.emu_describe(int(double), direction, norm, int(in_place), len(shape), sh, batch, 0, smem_limit,
+                        int(split_bf16), desc, len(desc), err, len(err))
+    if rc != 0:
+        raise ValueError(err.value.decode())
+    return json.loads(desc.value.decode())

@@ -66,3 +66,21 @@ def test_small_smem_limit_forces_fourstep():
     y, d = emulate(x, [4096], 1, -1, smem_limit=16 * 1024)
     assert d["passes"][0]["kind"] == "fourstep_cols"
     assert rel_l2(y, fp64_fft(x, [4096], 1, -1)) < 1e-13
+
+
+def test_split_precision_pass_selection():
+    """The tensor-core kernels replace plain single passes of float plans whose axis length
+    has one (256, 4096 contiguous; 256 strided); everything else keeps its FP32/FP64 pass."""
+    from native_libs import describe
+
+    def tc(shape, batch, double=False, split=True):
+        return [p["tc_id"] for p in describe(shape, batch, double=double, split_bf16=split)["passes"]]
+
+    assert tc([256], 64) == [0]
+    assert tc([4096], 8) == [2]
+    assert tc([256, 256, 256], 1) == [0, 1, 1]        # last axis contiguous, then strided columns
+    assert tc([4096, 4096], 1)[0] == 2 and all(t < 0 for t in tc([4096, 4096], 1)[1:])
+    assert all(t < 0 for t in tc([256], 64, double=True))    # double plans stay FP64
+    assert all(t < 0 for t in tc([256], 64, split=False))    # opt-in only
+    assert all(t < 0 for t in tc([1009], 8))                 # Bluestein passes stay FP32
+    assert all(t < 0 for t in tc([13440], 8))                # no tensor-core kernel for this length

@@ -57,6 +57,7 @@ __device__ __forceinline__ cplx<T> load_elem(const PassParams& P, const TileCtx<
         const int64_t g = (int64_t)k * P.g_k + X.sel;
         if (X.line_ok && g < P.in_len) {
             a = X.in[X.in_base + (int64_t)k * P.in.ks];
+            if (P.flip_in) a.y = -a.y;
             if (P.premul) a = cmul(a, ldg_c(static_cast<const C*>(P.premul) + g));
             if (P.conj_in) a.y = -a.y;
         }
@@ -94,6 +95,7 @@ __device__ __forceinline__ void store_elem(const PassParams& P, const TileCtx<T>
     if (P.postmul) v = cmul(v, ldg_c(static_cast<const C*>(P.postmul) + g));
     v.x *= X.scale;
     v.y *= X.scale;
+    if (P.flip_out) v.y = -v.y;
     X.out[base + (int64_t)k * P.out.ks] = v;
 }
 

@@ -74,6 +74,11 @@ struct PassParams {
     const void* postmul = nullptr;    // indexed by g on store
     double scale = 1.0;
     int store_via_smem = 0;           // transpose through shared memory before storing
+    // Direction override of a whole plan (conj(F(conj x))): conjugate the raw input before
+    // the pre-multiply and the final value after the post-multiply and scale. Used instead of
+    // conj_in / conj_out by passes that carry premul / postmul tables (Bluestein), where the
+    // plan's own conjugations sit between the FFTs and the chirp products.
+    int flip_in = 0, flip_out = 0;
     // Size-specialised four-step row pass: row l (= o*ts_rows + k1) stored at
     // (l / ts_rows) * ts_line + l % ts_rows + k * ts_rows.
     int64_t ts_rows = 0, ts_line = 0;

@@ -413,7 +413,17 @@ BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
 // Direction / normalization override: conj(F(conj x)) turns a plan's transform into the
 // other direction (conjugation on the first load and the last store; intermediate passes
 // keep their own conjugation pairs), and the last store carries the requested scale.
-void apply_override(BoundPass& bp, bool first, bool last, bool flip, double scale, bool set_scale) {
+void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double scale, bool set_scale) {
+    bool last = last_pass;
+    const PassSpec& ps = bp.spec_ref();
+    if (flip && first && ps.tables.premul >= 0) {
+        bp.p.flip_in ^= 1;  // conjugate before the chirp pre-multiply
+        first = false;
+    }
+    if (flip && last && ps.tables.postmul >= 0) {
+        bp.p.flip_out ^= 1;  // conjugate after the chirp post-multiply
+        last = false;
+    }
     if (flip) {
         if (first) {
             bp.p.conj_in ^= 1;
@@ -430,7 +440,7 @@ void apply_override(BoundPass& bp, bool first, bool last, bool flip, double scal
             bp.tp.conj_out ^= 1;
         }
     }
-    if (last && set_scale) {
+    if (last_pass && set_scale) {
         bp.p.scale = bp.fp.scale = bp.cp.scale = bp.pp.scale = scale;
         bp.tp.scale = static_cast<float>(scale);
     }

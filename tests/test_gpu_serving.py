@@ -176,3 +176,33 @@ def test_cuda_graph_capture_and_replay(torch):
         assert rel_l2(gb.cpu().numpy(), fp64_fft(inputs[4].cpu().numpy(), [256], 3, 1, 1 / 256)) <= spec_tol(256, False)
     del graph
     lib.syclfft_b200_group_destroy(g)
+
+
+@pytest.mark.parametrize("shape,dbl", [([4096], False), ([13440], False), ([65536], True), ([1009], False),
+                                       ([1009], True), ([4099], True), ([65537], False), ([30011], True),
+                                       ([24, 1009], False), ([60, 40], True)], ids=str)
+def test_execute_ex_direction_override(torch, shape, dbl):
+    """A forward plan run as a backward transform (and the reverse) through execute_ex, with
+    every normalization: Bluestein plans conjugate outside their chirp products."""
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    api = _provider.provider(lib)
+    err = ctypes.create_string_buffer(1024)
+    n = int(np.prod(shape))
+    batch = 3
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 5 + n, dt)
+    xi = torch.from_numpy(x).cuda()
+    s = torch.cuda.current_stream().cuda_stream
+    for plan_dir in (-1, 1):
+        cfg = _provider.make_config(shape, batch, plan_dir, double=dbl, normalization=0)
+        h = api.create(ctypes.byref(cfg), err, 1024)
+        assert h, err.value
+        for d, nm in ((-plan_dir, 0), (-plan_dir, 3), (plan_dir, 1)):
+            out = torch.empty_like(xi)
+            assert lib.syclfft_b200_execute_ex(h, xi.data_ptr(), out.data_ptr(), batch, d, nm, s, err, 1024) == 0, \
+                err.value
+            torch.cuda.synchronize()
+            ref = fp64_fft(x, shape, batch, d, norm_scale(nm, d, n))
+            assert rel_l2(out.cpu().numpy(), ref) <= spec_tol(n, dbl), (plan_dir, d, nm)
+        api.destroy(h)

@@ -4,9 +4,11 @@
 // offsets and shared-memory offsets then fold into immediates, so a thread's work is
 // loads, butterflies and stores with almost no index arithmetic.
 //
-// Only plain passes use them: a whole line per CTA row (no zero padding, tables or
-// four-step twiddle), conjugation for inverse transforms and the normalization scale
-// fused into the store.
+// Plain passes use them (a whole line per CTA row, conjugation for inverse transforms and
+// the normalization scale fused into the store), the four-step column and row passes
+// (twiddle fused into the store, transposed store), and the Bluestein passes: a zero-padded
+// chirp pre-multiply on the first load, a spectrum multiply between two FFTs held in
+// shared memory, and a chirp post-multiply with truncation on the last store.
 //   kModeK: lines are contiguous (line pitch `in_pitch`), threads walk elements;
 //   kModeC: lines are strided columns (element stride `in_ks`, columns contiguous),
 //           threads walk W adjacent columns so every access is a W-wide segment.
@@ -36,9 +38,36 @@ struct FixedParams {
     // kFeatTStore (kModeK row pass of a four-step): row l = o*rows + k1 of length N is
     // stored transposed at o * line + k1 + k2 * rows (coalesced over consecutive rows).
     int64_t rows = 1, line = 0;
+    // Bluestein features. Element index g = k * g_k + sel (sel: the column in kModeC, 0 in
+    // kModeK); kFeatPremul loads x[g] * premul[g] for g < in_len and 0 beyond; kFeatConv
+    // multiplies the first FFT's output k by pointwise[k + sel * pw_stride] (sel: the row
+    // index modulo `rows` in kModeK), conjugates it when conj_mid, and runs the FFT again;
+    // kFeatPostmul stores v * postmul[g] for g < out_len only. flip_in / flip_out conjugate
+    // the raw input and the final value (a direction override of the whole plan).
+    const void* premul = nullptr;
+    const void* postmul = nullptr;
+    const void* pointwise = nullptr;
+    int g_k = 1;
+    int in_len = 0, out_len = 0;
+    int pw_stride = 0;
+    int conj_mid = 0;
+    int flip_in = 0, flip_out = 0;
 };
 
-enum : int { kFeatPlain = 0, kFeatTw4 = 1, kFeatTStore = 2 };
+// Features (bits): kFeatTw4 four-step twiddle on the last store, kFeatTStore transposed
+// row store, kFeatPremul / kFeatConv / kFeatPostmul the Bluestein hooks above,
+// kFeatTw4Conj the conjugate twiddle (inverse four-step), kFeatMid (internal) the first
+// FFT of a kFeatConv pass storing its spectrum product to shared memory.
+enum : int {
+    kFeatPlain = 0,
+    kFeatTw4 = 1,
+    kFeatTStore = 2,
+    kFeatPremul = 4,
+    kFeatMid = 8,
+    kFeatPostmul = 16,
+    kFeatTw4Conj = 32,
+    kFeatConv = 64,
+};
 
 template <class T>
 struct FixedCtx {
@@ -53,9 +82,12 @@ struct FixedCtx {
     int64_t in_ks, out_ks;
     T scale;
     bool conj_in, conj_out;
-    int sel;              // column index (kFeatTw4)
+    int sel;              // column index (kFeatTw4, Bluestein element index)
     const C *tw4_hi, *tw4_lo;
     int tw4_shift;
+    const C *premul, *postmul, *pw;  // pw: pointwise table of this line (kFeatConv)
+    int g_k, in_len, out_len;
+    bool conj_mid, flip_in, flip_out;
 };
 
 template <class T> __host__ __device__ constexpr int pad_shift_c() { return sizeof(T) == 4 ? 4 : 3; }
@@ -82,7 +114,21 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * TPL;
         if (X.active && (EXACT || j < NR)) {
-            if constexpr (FIRST) {
+            if constexpr (FIRST && (FEAT & kFeatPremul)) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int k = j + r * NR;
+                    const int g = k * X.g_k + X.sel;
+                    C a = cmake<C>(T(0), T(0));
+                    if (X.line_ok && g < X.in_len) {
+                        a = MODEC ? X.gin[(int64_t)k * X.in_ks] : X.gin[k];
+                        if (X.flip_in) a.y = -a.y;
+                        a = cmul(a, __ldg(X.premul + g));
+                        if (X.conj_in) a.y = -a.y;
+                    }
+                    v[i * R + r] = a;
+                }
+            } else if constexpr (FIRST) {
                 if (X.line_ok) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
@@ -119,8 +165,16 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 twiddle_powers<R>(u, __ldg(X.twb + TWOFF + jm));
             }
             dft<R, T>(u);
-            if constexpr (LAST && FEAT == kFeatTStore) {
-                // natural order into shared memory; the transposed store follows the stages
+            if constexpr (LAST && (FEAT & (kFeatTStore | kFeatMid))) {
+                // natural order into shared memory: the transposed store, or the second FFT
+                // of a Bluestein convolution (after the spectrum multiply), follows
+                if constexpr (FEAT & kFeatMid) {
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        u[r] = cmul(u[r], __ldg(X.pw + j + r * NR));
+                        if (X.conj_mid) u[r].y = -u[r].y;
+                    }
+                }
                 if constexpr (NR % PAD == 0) {
                     C* p = X.sm + pidx<T>(j);
 #pragma unroll
@@ -134,17 +188,28 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 if (X.line_ok) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
+                        const int k = j + r * NR;
                         C a = u[r];
                         if (X.conj_out) a.y = -a.y;
-                        if constexpr (FEAT == kFeatTw4) {
-                            const int m = (j + r * NR) * X.sel;
-                            a = cmul(a, cmul(__ldg(X.tw4_hi + (m >> X.tw4_shift)),
-                                             __ldg(X.tw4_lo + (m & ((1 << X.tw4_shift) - 1)))));
+                        if constexpr (FEAT & kFeatTw4) {
+                            const int m = k * X.sel;
+                            C w = cmul(__ldg(X.tw4_hi + (m >> X.tw4_shift)),
+                                       __ldg(X.tw4_lo + (m & ((1 << X.tw4_shift) - 1))));
+                            if constexpr (FEAT & kFeatTw4Conj) w.y = -w.y;
+                            a = cmul(a, w);
+                        }
+                        if constexpr (FEAT & kFeatPostmul) {
+                            const int g = k * X.g_k + X.sel;
+                            if (g >= X.out_len) continue;
+                            a = cmul(a, __ldg(X.postmul + g));
                         }
                         a.x *= X.scale;
                         a.y *= X.scale;
-                        if constexpr (MODEC) X.gout[(int64_t)(j + r * NR) * X.out_ks] = a;
-                        else X.gout[j + r * NR] = a;
+                        if constexpr (FEAT & kFeatPostmul) {
+                            if (X.flip_out) a.y = -a.y;
+                        }
+                        if constexpr (MODEC) X.gout[(int64_t)k * X.out_ks] = a;
+                        else X.gout[k] = a;
                     }
                 }
             } else {
@@ -163,7 +228,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             }
         }
     }
-    if constexpr (!LAST || FEAT == kFeatTStore) __syncthreads();
+    if constexpr (!LAST || (FEAT & (kFeatTStore | kFeatMid))) __syncthreads();
 }
 
 template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int NS, int TWOFF, bool FIRST, int R, int... Rest>
@@ -193,6 +258,14 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
     X.scale = static_cast<T>(P.scale);
     X.conj_in = P.conj_in != 0;
     X.conj_out = P.conj_out != 0;
+    X.premul = static_cast<const C*>(P.premul);
+    X.postmul = static_cast<const C*>(P.postmul);
+    X.g_k = P.g_k;
+    X.in_len = P.in_len;
+    X.out_len = P.out_len;
+    X.conj_mid = P.conj_mid != 0;
+    X.flip_in = P.flip_in != 0;
+    X.flip_out = P.flip_out != 0;
     const int tid = threadIdx.x;
     if constexpr (MODEC) {
         const int w = tid % W;
@@ -222,9 +295,22 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         X.gout = out + c * P.out_pitch;
         X.in_ks = 1;
         X.out_ks = 1;
+        // row index within its line (four-step row passes: the k1 of the twiddle and of
+        // the spectrum table); 0 for whole lines
+        X.sel = (FEAT & (kFeatTw4 | kFeatConv)) && P.rows > 1 ? static_cast<int>(c % P.rows) : 0;
+        X.tw4_hi = static_cast<const C*>(P.tw4_hi);
+        X.tw4_lo = static_cast<const C*>(P.tw4_lo);
+        X.tw4_shift = P.tw4_shift;
+    }
+    if constexpr (FEAT & kFeatConv) {
+        // Bluestein convolution: FFT, spectrum multiply (to shared memory), FFT again
+        X.pw = static_cast<const C*>(P.pointwise) + (int64_t)X.sel * P.pw_stride;
+        fixed_stages<T, N, TPL, MODEC, W, (FEAT & kFeatPremul) | kFeatMid, 1, 0, true, Rs...>(X);
+        fixed_stages<T, N, TPL, MODEC, W, FEAT & ~(kFeatPremul | kFeatConv), 1, 0, false, Rs...>(X);
+        return;
     }
     fixed_stages<T, N, TPL, MODEC, W, FEAT, 1, 0, true, Rs...>(X);
-    if constexpr (FEAT == kFeatTStore && !MODEC) {
+    if constexpr ((FEAT & kFeatTStore) && !MODEC) {
         // Rows blockIdx.x*w .. +w-1 are consecutive k1 of one line when rows % w == 0:
         // walk (row fastest, element) so every store is a w-wide segment.
         const int64_t row0 = (int64_t)blockIdx.x * P.w;

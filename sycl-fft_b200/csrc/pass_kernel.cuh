@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(MAXT, 65536 / (MAXT * reg_target<T, MAXV>()))
     X.line_ok = X.active && c < P.n_cols;
     X.in_base = line_base(P.in, o, c);
     X.out_base = line_base(P.out, o, c);
-    X.sel = P.sel_mode == kSelCol ? c : (P.sel_mode == kSelOuterLo ? o % P.sel_d : 0);
+    X.sel = P.sel_mode == kSelCol ? c
+            : P.sel_mode == kSelOuterLo ? o % P.sel_d
+            : P.sel_mode == kSelColMod  ? c % P.sel_d
+                                        : 0;
     if constexpr (!FULL) {
         run_seq<T, MAXV, false>(P, P.fft1, X, true, kDstGlobal);
         return;
@@ -249,7 +252,10 @@ __global__ void __launch_bounds__(MAXT, 65536 / (MAXT * reg_target<T, MAXV>()))
             }
             const int64_t cc = c0 + w;
             if (cc >= P.n_cols) continue;
-            const int64_t sel = P.sel_mode == kSelCol ? cc : (P.sel_mode == kSelOuterLo ? o % P.sel_d : 0);
+            const int64_t sel = P.sel_mode == kSelCol ? cc
+                                : P.sel_mode == kSelOuterLo ? o % P.sel_d
+                                : P.sel_mode == kSelColMod  ? cc % P.sel_d
+                                                            : 0;
             store_elem<T, FULL>(P, X, line_base(P.out, o, cc), sel, k, X.sm[smem_index(P, w, k)]);
         }
     }

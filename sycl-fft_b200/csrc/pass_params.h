@@ -16,7 +16,7 @@
 //   store: conjugation, the four-step twiddle W_N^(sign*k*sel), post-multiply by a
 //          table indexed by g, the normalization scale, truncation (g >= out_len is
 //          not written).
-// The element index is g = k * g_k + sel with sel = 0, c, or (o % sel_d).
+// The element index is g = k * g_k + sel with sel = 0, c, (o % sel_d) or (c % sel_d).
 //
 // This header is plain C++ so host planning code and device code share it.
 #pragma once
@@ -28,7 +28,7 @@ namespace sfb {
 constexpr int kMaxStages = 16;
 
 enum : int { kModeK = 0, kModeC = 1 };         // thread mapping / coalesced dimension
-enum : int { kSelNone = 0, kSelCol = 1, kSelOuterLo = 2 };
+enum : int { kSelNone = 0, kSelCol = 1, kSelOuterLo = 2, kSelColMod = 3 };
 
 struct LineLayout {
     int64_t hi = 0, lo = 0, d = 1, cs = 0, ks = 1;

@@ -4,6 +4,7 @@
 #include "fixed_catalog.h"
 #include "piped_catalog.h"
 #include "tc_catalog.h"
+#include "bluestein_catalog.h"
 #include "tc_shape.h"
 
 #include <algorithm>
@@ -388,6 +389,256 @@ struct Builder {
         return true;
     }
 
+    // Chirp c_n = conj(h_n) and the convolution kernel's spectrum FFT_M(h)/M, with
+    // h_n = exp(-i*sgn*pi*(n^2 mod 2L)/L) (exact reduction), h mirrored to M - n.
+    void chirp_tables(int64_t L, int64_t M, int sgn, std::vector<std::complex<double>>& chirp,
+                      std::vector<std::complex<double>>& kern) {
+        chirp.assign(L, 0.0);
+        kern.assign(M, 0.0);
+        for (int64_t n = 0; n < L; ++n) {
+            const uint64_t r = (static_cast<unsigned __int128>(n) * n) % static_cast<uint64_t>(2 * L);
+            const std::complex<double> h = cis_neg(sgn * static_cast<int64_t>(r), 2 * L);
+            kern[n] = h;
+            if (n) kern[M - n] = h;
+            chirp[n] = std::conj(h);
+        }
+        host_fft_fp64(kern, -1);
+        for (auto& v : kern) v /= static_cast<double>(M);
+    }
+
+    // Stage sequence of a catalog entry (twiddles: the base table of its radices).
+    StageSeq entry_seq(const BlueEntry& e) {
+        StageSeq q;
+        q.nstages = e.nstages;
+        int ns = 1;
+        for (int i = 0; i < e.nstages; ++i) {
+            q.radix[i] = e.radices[i];
+            q.ns[i] = ns;
+            ns *= e.radices[i];
+        }
+        return q;
+    }
+
+    // Lines per CTA of a kModeK catalog kernel: about 256 threads, within MAXT and shared memory.
+    int lines_per_cta(int tpl, int maxt, int64_t pitch, int64_t n_cols) {
+        int w = std::max(1, 256 / tpl);
+        w = static_cast<int>(std::min<int64_t>(w, n_cols));
+        while (w > 1 && (w * tpl > maxt || static_cast<int64_t>(w) * pitch * cs > smem_limit)) --w;
+        return w;
+    }
+
+    // Bluestein on the size-specialised kernels (contiguous axes): the smallest catalog
+    // convolution length M >= 2L - 1, as one fused pass where a fused kernel of length M fits
+    // a CTA, else as M = n1 * n2 over a column kernel (n1) and a row kernel (n2) in three
+    // passes. Returns false (generic kernels) when the catalog has no such length.
+    bool bluestein_fixed(int ax, int64_t L, int64_t O, Buf& cur) {
+        if (req.no_fixed) return false;
+        int count = 0;
+        const BlueEntry* cat = blue_entries(&count);
+        const int64_t need = 2 * L - 1;
+        const int ps_shift = pad_shift_for(req.dbl);
+        const BlueEntry* fused = nullptr;
+        for (int i = 0; i < count; ++i) {
+            const BlueEntry& e = cat[i];
+            if (e.dbl != (req.dbl ? 1 : 0) || e.kind != kBlueFused || e.n < need) continue;
+            if (int64_t(kmode_pitch(e.n, ps_shift)) * cs > smem_limit) continue;
+            if (!fused || e.n < fused->n) fused = &e;
+        }
+        const BlueEntry *cf = nullptr, *rc = nullptr;
+        int64_t best = 0;
+        for (int i = 0; i < count && !fused; ++i) {
+            const BlueEntry& a = cat[i];
+            if (a.dbl != (req.dbl ? 1 : 0) || a.kind != kBlueColsFwd) continue;
+            if (int64_t(a.n) * a.w * cs > smem_limit) continue;
+            for (int k = 0; k < count; ++k) {
+                const BlueEntry& b = cat[k];
+                if (b.dbl != (req.dbl ? 1 : 0) || b.kind != kBlueRowsConv) continue;
+                const int64_t M = int64_t(a.n) * b.n;
+                if (M < need || int64_t(kmode_pitch(b.n, ps_shift)) * cs > smem_limit) continue;
+                const bool better = !cf || M < best ||
+                                    (M == best && std::abs(std::log(double(b.n) / a.n)) <
+                                                      std::abs(std::log(double(rc->n) / cf->n)));
+                if (better) {
+                    best = M;
+                    cf = &a;
+                    rc = &b;
+                }
+            }
+        }
+        const BlueEntry* ci = nullptr;
+        if (cf)
+            for (int i = 0; i < count; ++i)
+                if (cat[i].dbl == cf->dbl && cat[i].kind == kBlueColsInv && cat[i].n == cf->n) ci = &cat[i];
+        if (!fused && !(cf && rc && ci)) return false;
+
+        const bool bwd = req.direction == 1;
+        (void)bwd;
+        const int sgn = req.direction;
+        const int64_t E = static_cast<int64_t>(plan.elements);
+        const int64_t M = fused ? fused->n : best;
+        std::vector<std::complex<double>> chirp, kern;
+        if (!req.device_spectrum) chirp_tables(L, M, sgn, chirp, kern);
+        const int chirp_id = req.device_spectrum ? add_device_table(L) : add_table(std::move(chirp));
+        BluesteinJob job;
+        job.L = L;
+        job.M = M;
+        job.sgn = sgn;
+        job.chirp_table = chirp_id;
+        if (fused) {
+            PassSpec ps;
+            ps.kind = "bluestein_fused";
+            ps.axis = ax;
+            PassParams& p = ps.p;
+            p.n = static_cast<int>(M);
+            p.mode = kModeK;
+            p.n_outer = 1;
+            p.n_cols = O;
+            p.in.cs = L;
+            p.in.ks = 1;
+            p.out = p.in;
+            p.in_len = p.out_len = L;
+            ps.tables.premul = chirp_id;
+            ps.tables.postmul = chirp_id;
+            ps.tables.pointwise = req.device_spectrum ? add_device_table(M) : add_table(std::move(kern));
+            job.spectrum_table = ps.tables.pointwise;
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            p.fft1 = entry_seq(*fused);
+            p.fft2 = p.fft1;
+            use_base_table(ps);
+            ps.tables.tw2 = ps.tables.tw1;
+            p.pad_shift = ps_shift;
+            p.pitch = kmode_pitch(p.n, ps_shift);
+            p.tpl = fused->tpl;
+            p.w = lines_per_cta(fused->tpl, fused->maxt, p.pitch, O);
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.col_tiles;
+            ps.threads = round_up(p.w * p.tpl, 32);
+            ps.smem_bytes = static_cast<int64_t>(p.w) * p.pitch * cs;
+            ps.kc.maxt = fused->maxt;
+            ps.blue_id = fused->id;
+            ps.blue_kind = kBlueFused;
+            ps.src = cur;
+            ps.dst = Buf::Output;
+            ps.bytes_moved = 2 * E * cs;
+            plan.passes.push_back(ps);
+            if (req.device_spectrum) plan.bluestein_jobs.push_back(job);
+            cur = Buf::Output;
+            return true;
+        }
+        const int64_t n1 = cf->n, n2 = rc->n;
+        int kp_id;
+        if (!req.device_spectrum) {
+            std::vector<std::complex<double>> kp(M);  // K'[k1*n2 + k2] = K[k1 + n1*k2]
+            for (int64_t k1 = 0; k1 < n1; ++k1)
+                for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = kern[k1 + n1 * k2];
+            kp_id = add_table(std::move(kp));
+        } else {
+            kp_id = add_device_table(M);
+            job.n1 = n1;
+            job.n2 = n2;
+            job.large = true;
+            job.spectrum_table = kp_id;
+            plan.bluestein_jobs.push_back(job);
+        }
+        plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(O * M));
+        auto cols = [&](PassSpec& a, const BlueEntry& e) {
+            PassParams& p = a.p;
+            p.n = static_cast<int>(n1);
+            p.mode = kModeC;
+            p.g_k = n2;
+            p.n_outer = O;
+            p.n_cols = n2;
+            p.sel_mode = kSelCol;
+            p.fft1 = entry_seq(e);
+            use_base_table(a);
+            p.tpl = e.tpl;
+            p.w = e.w;
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.n_outer * p.col_tiles;
+            a.threads = round_up(e.w * e.tpl, 32);
+            a.smem_bytes = static_cast<int64_t>(e.w) * n1 * cs;
+            a.kc.maxt = e.maxt;
+            a.blue_id = e.id;
+            a.blue_kind = e.kind;
+        };
+        // pass 1: columns of the zero-padded, chirp-multiplied line; W_M^(k1*c) on the store
+        PassSpec a;
+        a.kind = "bluestein_cols_fwd";
+        a.axis = ax;
+        cols(a, *cf);
+        a.p.in.hi = L; a.p.in.cs = 1; a.p.in.ks = n2;
+        a.p.out.hi = M; a.p.out.cs = 1; a.p.out.ks = n2;
+        a.p.in_len = L;
+        a.p.out_len = kNoLimit;
+        a.tables.premul = chirp_id;
+        add_tw4(a, M, -1);
+        a.src = cur;
+        a.dst = Buf::Scratch;
+        a.bytes_moved = (E + O * M) * cs;
+        plan.passes.push_back(a);
+        // pass 2: rows (all lines' rows in one flat range): FFT, spectrum multiply, inverse
+        // FFT, inverse twiddle, in place
+        PassSpec b;
+        b.kind = "bluestein_rows_conv";
+        b.axis = ax;
+        {
+            PassParams& p = b.p;
+            p.n = static_cast<int>(n2);
+            p.mode = kModeK;
+            p.n_outer = 1;
+            p.n_cols = O * n1;
+            p.in.cs = n2;
+            p.in.ks = 1;
+            p.out = p.in;
+            p.sel_mode = kSelColMod;
+            p.sel_d = n1;
+            p.in_len = p.out_len = kNoLimit;
+            b.tables.pointwise = kp_id;
+            p.pw_stride = n2;
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            p.fft1 = entry_seq(*rc);
+            p.fft2 = p.fft1;
+            use_base_table(b);
+            b.tables.tw2 = b.tables.tw1;
+            add_tw4(b, M, +1);
+            p.pad_shift = ps_shift;
+            p.pitch = kmode_pitch(p.n, ps_shift);
+            p.tpl = rc->tpl;
+            p.w = lines_per_cta(rc->tpl, rc->maxt, p.pitch, p.n_cols);
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.col_tiles;
+            b.threads = round_up(p.w * p.tpl, 32);
+            b.smem_bytes = static_cast<int64_t>(p.w) * p.pitch * cs;
+            b.kc.maxt = rc->maxt;
+            b.blue_id = rc->id;
+            b.blue_kind = kBlueRowsConv;
+            b.src = Buf::Scratch;
+            b.dst = Buf::Scratch;
+            b.bytes_moved = 2 * O * M * cs;
+        }
+        plan.passes.push_back(b);
+        // pass 3: columns: inverse FFT, chirp post-multiply, truncation to L
+        PassSpec c;
+        c.kind = "bluestein_cols_inv";
+        c.axis = ax;
+        cols(c, *ci);
+        c.p.in.hi = M; c.p.in.cs = 1; c.p.in.ks = n2;
+        c.p.out.hi = L; c.p.out.cs = 1; c.p.out.ks = n2;
+        c.p.in_len = kNoLimit;
+        c.p.out_len = L;
+        c.p.conj_in = 1;
+        c.p.conj_out = 1;
+        c.tables.postmul = chirp_id;
+        c.src = Buf::Scratch;
+        c.dst = Buf::Output;
+        c.bytes_moved = (O * M + E) * cs;
+        plan.passes.push_back(c);
+        cur = Buf::Output;
+        return true;
+    }
+
     void axis(int ax, int64_t L, int64_t s, int64_t O, Buf& cur) {
         const bool bwd = req.direction == 1;
         const int64_t E = static_cast<int64_t>(plan.elements);
@@ -498,6 +749,7 @@ struct Builder {
             return;
         }
 
+        if (s == 1 && bluestein_fixed(ax, L, O, cur)) return;
         // Bluestein: y_k = c_k * sum_n (x_n c_n) h_{k-n}, c_n = exp(-i*sgn*pi*n^2/L) conj-chirp,
         // h_n = conj(c_n) (exact n^2 mod 2L reduction), convolution of length M via FFT.
         const int64_t M = static_cast<int64_t>(bluestein_length(static_cast<uint64_t>(L)));
@@ -928,6 +1180,16 @@ const PipedEntry* find_piped(bool dbl, int n) {
 const TcEntry kTc[] = {SFB_TC_CATALOG(SFB_TENTRY)};
 #undef SFB_TENTRY
 
+#define SFB_BENTRY(ID, DBL, KIND, N, TPL, W, MAXT, ...) \
+    BlueEntry{ID, DBL, KIND, N, TPL, W, MAXT, {__VA_ARGS__}, count_args(__VA_ARGS__)},
+const BlueEntry kBlue[] = {SFB_BLUESTEIN_CATALOG(SFB_BENTRY)};
+#undef SFB_BENTRY
+
+const BlueEntry* blue_entries(int* count) {
+    *count = static_cast<int>(sizeof(kBlue) / sizeof(kBlue[0]));
+    return kBlue;
+}
+
 const TcEntry* find_tc(int n, bool cols) {
     for (const TcEntry& e : kTc)
         if (e.n == n && (e.cols != 0) == cols) return &e;
@@ -991,7 +1253,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
-           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
            << ps.cl_p << "]}";
     }
     os << "]}";

@@ -59,6 +59,8 @@ struct PassSpec {
                              // buffers are 16-byte aligned; otherwise fixed_id runs
     int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
     int tc_id = -1;          // split-precision tensor-core kernel (tc_catalog.h), float plans only
+    int blue_id = -1;        // size-specialised Bluestein kernel (bluestein_catalog.h)
+    int blue_kind = -1;      // its kind: kBlueFused / kBlueColsFwd / kBlueRowsConv / kBlueColsInv
 };
 
 // One entry of cluster_catalog.h as seen by the host.
@@ -86,6 +88,15 @@ struct PipedEntry {
     int nstages;
 };
 const PipedEntry* find_piped(bool dbl, int n);
+
+// One entry of bluestein_catalog.h as seen by the host.
+enum : int { kBlueFused = 0, kBlueColsFwd = 1, kBlueRowsConv = 2, kBlueColsInv = 3 };
+struct BlueEntry {
+    int id, dbl, kind, n, tpl, w, maxt;
+    int radices[kMaxStages];
+    int nstages;
+};
+const BlueEntry* blue_entries(int* count);
 
 // One entry of tc_catalog.h (split-precision tensor-core kernels, complex<float> only).
 struct TcEntry {

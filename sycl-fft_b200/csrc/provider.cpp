@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdlib>
 #include <fstream>
 #include <map>
@@ -27,6 +28,7 @@
 #include "launch.hpp"
 #include "piped_launch.hpp"
 #include "tc_launch.hpp"
+#include "bluestein_launch.hpp"
 #include "planner.hpp"
 
 namespace sfb {
@@ -139,8 +141,19 @@ FixedParams to_fixed(const PassParams& p) {
     f.tw4_hi = p.tw4_hi;
     f.tw4_lo = p.tw4_lo;
     f.tw4_shift = p.tw4_shift;
-    f.rows = p.ts_rows;
+    f.rows = p.ts_rows ? p.ts_rows : (p.sel_mode == kSelColMod ? p.sel_d : 1);
     f.line = p.ts_line;
+    auto clamp = [](int64_t v) { return static_cast<int>(std::min<int64_t>(v, INT32_MAX)); };
+    f.premul = p.premul;
+    f.postmul = p.postmul;
+    f.pointwise = p.pointwise;
+    f.g_k = clamp(p.g_k);
+    f.in_len = clamp(p.in_len);
+    f.out_len = clamp(p.out_len);
+    f.pw_stride = clamp(p.pw_stride);
+    f.conj_mid = p.conj_mid;
+    f.flip_in = p.flip_in;
+    f.flip_out = p.flip_out;
     return f;
 }
 
@@ -366,7 +379,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + offsets[id];
     };
     for (const PassSpec& ps : plan->spec.passes) {
-        if (ps.fixed_id < 0 && ps.cluster_id < 0 && ps.tc_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
+        if (ps.fixed_id < 0 && ps.cluster_id < 0 && ps.tc_id < 0 && ps.blue_id < 0 && !has_variant(req.dbl, ps.kc.maxv, ps.kc.maxt))
             throw std::runtime_error("no kernel variant for pass");
         BoundPass bp;
         bp.spec_ptr = &ps;  // plan->spec.passes is not modified after this point
@@ -418,10 +431,12 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
     const PassSpec& ps = bp.spec_ref();
     if (flip && first && ps.tables.premul >= 0) {
         bp.p.flip_in ^= 1;  // conjugate before the chirp pre-multiply
+        bp.fp.flip_in ^= 1;
         first = false;
     }
     if (flip && last && ps.tables.postmul >= 0) {
         bp.p.flip_out ^= 1;  // conjugate after the chirp post-multiply
+        bp.fp.flip_out ^= 1;
         last = false;
     }
     if (flip) {
@@ -494,7 +509,12 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
         };
         const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().src)) % 16 == 0) &&
                              (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().dst)) % 16 == 0);
-        if (bp.spec_ref().tc_id >= 0) {
+        if (bp.spec_ref().blue_id >= 0) {
+            check(launch_blue(bp.spec_ref().blue_id, plan->spec.req.dbl, bp.spec_ref().blue_kind, bp.fp,
+                              bp.spec_ref().threads, static_cast<size_t>(bp.spec_ref().smem_bytes), bp.p.tiles,
+                              buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
+                  "FFT Bluestein pass launch");
+        } else if (bp.spec_ref().tc_id >= 0) {
             check(launch_tc(bp.spec_ref().tc_id, bp.tp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
                   "FFT tensor-core pass launch");
         } else if (bp.spec_ref().piped_id >= 0 && aligned) {

@@ -103,7 +103,8 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
     for (int64_t o = 0; o < p.n_outer; ++o) {
         for (int64_t c = 0; c < p.n_cols; ++c) {
             Line L{o, c, std::vector<cd>(p.n)};
-            const int64_t sel = p.sel_mode == kSelCol ? c : (p.sel_mode == kSelOuterLo ? o % p.sel_d : 0);
+            const int64_t sel = p.sel_mode == kSelCol ? c : p.sel_mode == kSelOuterLo ? o % p.sel_d
+                                : p.sel_mode == kSelColMod ? c % p.sel_d : 0;
             const int64_t ib = line_base(p.in, o, c);
             for (int k = 0; k < p.n; ++k) {
                 const int64_t g = int64_t(k) * p.g_k + sel;
@@ -119,14 +120,15 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
         }
     }
     for (auto& L : lines) {
-        const int64_t sel = p.sel_mode == kSelCol ? L.c : (p.sel_mode == kSelOuterLo ? L.o % p.sel_d : 0);
+        const int64_t sel = p.sel_mode == kSelCol ? L.c : p.sel_mode == kSelOuterLo ? L.o % p.sel_d
+                            : p.sel_mode == kSelColMod ? L.c % p.sel_d : 0;
         stockham(L.v, p.fft1, plan.tables[ps.tables.tw1], p.n, ps.tw_base);
         if (p.fft2.nstages > 0) {
             for (int k = 0; k < p.n; ++k) {
                 if (pointwise) L.v[k] *= (*pointwise)[k + sel * p.pw_stride];
                 if (p.conj_mid) L.v[k] = std::conj(L.v[k]);
             }
-            stockham(L.v, p.fft2, plan.tables[ps.tables.tw2], p.n);
+            stockham(L.v, p.fft2, plan.tables[ps.tables.tw2], p.n, ps.tw_base);
         }
         const int64_t ob = line_base(p.out, L.o, L.c);
         const bool tstore = ps.fixed_id >= 0 && ps.fixed_feat == kFixedTStore;

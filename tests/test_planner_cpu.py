@@ -84,3 +84,29 @@ def test_split_precision_pass_selection():
     assert all(t < 0 for t in tc([256], 64, split=False))    # opt-in only
     assert all(t < 0 for t in tc([1009], 8))                 # Bluestein passes stay FP32
     assert all(t < 0 for t in tc([13440], 8))                # no tensor-core kernel for this length
+
+
+def test_bluestein_on_catalog_kernels():
+    """Contiguous Bluestein axes take the smallest catalog convolution length >= 2L - 1: one
+    fused pass where it fits a CTA, else three passes over M = n1 * n2; strided axes and
+    the generic-kernel switch keep the runtime-parameterised passes."""
+    from native_libs import describe, emulate
+
+    def kinds(shape, dbl=False, batch=2):
+        d = describe(shape, batch, double=dbl)
+        return [(p["kind"], p["n"], p["blue_id"] >= 0) for p in d["passes"]]
+
+    assert kinds([1009]) == [("bluestein_fused", 2048, True)]
+    assert kinds([4099]) == [("bluestein_fused", 10240, True)]
+    k = kinds([65537])
+    assert [x[0] for x in k] == ["bluestein_cols_fwd", "bluestein_rows_conv", "bluestein_cols_inv"]
+    assert all(x[2] for x in k) and k[0][1] * k[1][1] >= 2 * 65537 - 1
+    assert all(x[2] for x in kinds([4099], dbl=True))
+    assert not any(x[2] for x in kinds([1009, 6]))           # strided prime axis: generic passes
+    rng = np.random.default_rng(9)
+    for shape, dbl in (([1009], False), ([4099], True), ([12289], False)):
+        n = int(np.prod(shape))
+        x = rng.standard_normal(2 * n) + 1j * rng.standard_normal(2 * n)
+        out, _ = emulate(x, shape, 2, -1, norm=1, double=dbl)
+        ref = np.fft.fft(x.reshape(2, n), axis=1).reshape(-1) / n
+        assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13

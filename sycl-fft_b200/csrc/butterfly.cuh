@@ -182,6 +182,27 @@ template <class T, class C> SFB_HD void bfly16(C* v) {
     t = v[11]; v[11] = v[14]; v[14] = t;
 }
 
+// Radix 15 as a prime-factor (Good-Thomas) DFT, 15 = 3 * 5 with coprime factors: no
+// internal twiddles. Input n = (5*n1 + 3*n2) mod 15 feeds five-point DFTs over n2, then
+// three-point DFTs over n1; output (k1, k2) is X[(10*k1 + 6*k2) mod 15], since
+// W15^(n k) = W3^(n1 k1) * W5^(n2 k2) for those index maps.
+template <class T, class C> SFB_HD void bfly15(C* v) {
+    C a[3][5];
+#pragma unroll
+    for (int n1 = 0; n1 < 3; ++n1) {
+#pragma unroll
+        for (int n2 = 0; n2 < 5; ++n2) a[n1][n2] = v[(5 * n1 + 3 * n2) % 15];
+        bfly5<T>(a[n1]);
+    }
+#pragma unroll
+    for (int k2 = 0; k2 < 5; ++k2) {
+        C b[3] = {a[0][k2], a[1][k2], a[2][k2]};
+        bfly3<T>(b);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) v[(10 * k1 + 6 * k2) % 15] = b[k1];
+    }
+}
+
 // u[r] *= w^r for r = 1..R-1, the powers formed by a balanced product tree
 // (w^r = w^h * w^(r-h), h the largest power of two <= r): at most log2(R)+1 roundings deep.
 template <int R, class C> SFB_HD void twiddle_powers(C* u, C w) {
@@ -212,6 +233,8 @@ template <int R, class T, class C> SFB_HD void dft(C* v) {
         bfly7<T>(v);
     } else if constexpr (R == 8) {
         bfly8<T>(v);
+    } else if constexpr (R == 15) {
+        bfly15<T>(v);
     } else if constexpr (R == 16) {
         bfly16<T>(v);
     }

@@ -311,21 +311,21 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
     }
     fixed_stages<T, N, TPL, MODEC, W, FEAT, 1, 0, true, Rs...>(X);
     if constexpr ((FEAT & kFeatTStore) && !MODEC) {
-        // Rows blockIdx.x*w .. +w-1 are consecutive k1 of one line when rows % w == 0:
-        // walk (row fastest, element) so every store is a w-wide segment.
-        const int64_t row0 = (int64_t)blockIdx.x * P.w;
+        // Rows blockIdx.x*W .. +W-1 are consecutive k1 of one line (the planner keeps
+        // rows % W == 0): walk (row fastest, element) so every store is a W-wide segment.
+        const int64_t row0 = (int64_t)blockIdx.x * W;
+        const int64_t o = row0 / P.rows;
+        C* dst = out + o * P.line + (row0 - o * P.rows);
+        const int valid = static_cast<int>(P.n_cols - row0 < W ? P.n_cols - row0 : W);
         const T sc = X.scale;
-        for (int idx = tid; idx < P.w * N; idx += blockDim.x) {
-            const int k = idx / P.w;
-            const int w = idx - k * P.w;
-            const int64_t l = row0 + w;
-            if (l >= P.n_cols) continue;
-            C a = sm[w * kpitch<T, N>() + pidx<T>(k)];
-            if (X.conj_out) a.y = -a.y;
-            a.x *= sc;
-            a.y *= sc;
-            const int64_t o = l / P.rows;
-            out[o * P.line + (l - o * P.rows) + (int64_t)k * P.rows] = a;
+        const T sy = X.conj_out ? -sc : sc;
+#pragma unroll 4
+        for (int idx = tid; idx < W * N; idx += blockDim.x) {
+            const int k = idx / W;
+            const int w = idx - k * W;
+            if (w >= valid) continue;
+            const C a = sm[w * kpitch<T, N>() + pidx<T>(k)];
+            dst[w + (int64_t)k * P.rows] = cmake<C>(a.x * sc, a.y * sy);
         }
     }
 }

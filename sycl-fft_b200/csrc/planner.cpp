@@ -285,9 +285,19 @@ struct Builder {
         PassParams& p = ps.p;
         const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n, kFixedPlain);
         if (!e) return;
-        if (e->nstages != p.fft1.nstages) return;
-        for (int i = 0; i < e->nstages; ++i)
-            if (e->radices[i] != p.fft1.radix[i]) return;
+        // The entry's own radix sequence (it may use butterflies the runtime-parameterised
+        // kernel does not have, such as the prime-factor radix 15).
+        if (e->nstages != p.fft1.nstages || !std::equal(e->radices, e->radices + e->nstages, p.fft1.radix)) {
+            StageSeq q;
+            q.nstages = e->nstages;
+            int ns = 1;
+            for (int i = 0; i < e->nstages; ++i) {
+                q.radix[i] = e->radices[i];
+                q.ns[i] = ns;
+                ns *= e->radices[i];
+            }
+            p.fft1 = q;
+        }
         if (p.mode == kModeK) {
             if (p.in.ks != 1 || p.out.ks != 1 || p.n_outer != 1) return;
             int w = req.force_w > 0 ? req.force_w : std::max(1, 256 / e->tpl);

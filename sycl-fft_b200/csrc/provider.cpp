@@ -461,6 +461,33 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
     }
 }
 
+// Launches one bound pass of a plan on its kernel family.
+void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cudaStream_t stream) {
+    const bool aligned = (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0);
+    const PassSpec& ps = bp.spec_ref();
+    if (ps.blue_id >= 0) {
+        check(launch_blue(ps.blue_id, plan->spec.req.dbl, ps.blue_kind, bp.fp, ps.threads,
+                          static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
+              "FFT Bluestein pass launch");
+    } else if (ps.tc_id >= 0) {
+        check(launch_tc(ps.tc_id, bp.tp, src, dst, stream), "FFT tensor-core pass launch");
+    } else if (ps.piped_id >= 0 && aligned) {
+        const int64_t lines = bp.pp.lines;
+        const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
+        check(launch_piped(ps.piped_id, bp.pp, grid, src, dst, stream), "FFT pipelined pass launch");
+    } else if (ps.cluster_id >= 0) {
+        check(launch_cluster(ps.cluster_id, bp.cp, src, dst, stream), "FFT cluster pass launch");
+    } else if (ps.fixed_id >= 0) {
+        check(launch_fixed(ps.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, ps.threads,
+                           static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
+              "FFT pass launch");
+    } else {
+        check(launch_pass(bp.p, plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt, ps.threads, static_cast<size_t>(ps.smem_bytes),
+                          src, dst, stream),
+              "FFT pass launch");
+    }
+}
+
 void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch,
                   int direction, int normalization) {
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
@@ -499,42 +526,15 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     const bool flip = dir != plan->spec.req.direction;
     const bool set_scale = flip || norm != plan->spec.req.normalization;
     const double scale = normalization_scale(norm, dir, plan->spec.transform_size);
+    auto buf = [&](Buf b) -> void* {
+        if (b == Buf::Input) return const_cast<void*>(in);
+        if (b == Buf::Output) return out;
+        return scratch;
+    };
     for (size_t i = 0; i < plan->passes.size(); ++i) {
         BoundPass bp = rescale(plan->passes[i], batch, planned);
         if (flip || set_scale) apply_override(bp, i == 0, i + 1 == plan->passes.size(), flip, scale, set_scale);
-        auto buf = [&](Buf b) -> void* {
-            if (b == Buf::Input) return const_cast<void*>(in);
-            if (b == Buf::Output) return out;
-            return scratch;
-        };
-        const bool aligned = (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().src)) % 16 == 0) &&
-                             (reinterpret_cast<uintptr_t>(buf(bp.spec_ref().dst)) % 16 == 0);
-        if (bp.spec_ref().blue_id >= 0) {
-            check(launch_blue(bp.spec_ref().blue_id, plan->spec.req.dbl, bp.spec_ref().blue_kind, bp.fp,
-                              bp.spec_ref().threads, static_cast<size_t>(bp.spec_ref().smem_bytes), bp.p.tiles,
-                              buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
-                  "FFT Bluestein pass launch");
-        } else if (bp.spec_ref().tc_id >= 0) {
-            check(launch_tc(bp.spec_ref().tc_id, bp.tp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
-                  "FFT tensor-core pass launch");
-        } else if (bp.spec_ref().piped_id >= 0 && aligned) {
-            const int64_t lines = bp.pp.lines;
-            const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
-            check(launch_piped(bp.spec_ref().piped_id, bp.pp, grid, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
-                  "FFT pipelined pass launch");
-        } else if (bp.spec_ref().cluster_id >= 0) {
-            check(launch_cluster(bp.spec_ref().cluster_id, bp.cp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
-                  "FFT cluster pass launch");
-        } else if (bp.spec_ref().fixed_id >= 0) {
-            check(launch_fixed(bp.spec_ref().fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, bp.spec_ref().threads,
-                               static_cast<size_t>(bp.spec_ref().smem_bytes), bp.p.tiles, buf(bp.spec_ref().src),
-                               buf(bp.spec_ref().dst), stream),
-                  "FFT pass launch");
-        } else {
-            check(launch_pass(bp.p, plan->spec.req.dbl, bp.spec_ref().kc.maxv, bp.spec_ref().kc.maxt, bp.spec_ref().threads,
-                              static_cast<size_t>(bp.spec_ref().smem_bytes), buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream),
-                  "FFT pass launch");
-        }
+        launch_bound_pass(plan, bp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream);
     }
     // Under capture the record becomes a node of the graph, so destroying the plan still
     // waits for the last replay that used its tables and scratch.

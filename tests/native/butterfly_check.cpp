@@ -21,6 +21,7 @@ static int dispatch(int radix, const T* in, T* out) {
         case 5: run<5, T>(in, out); return 0;
         case 7: run<7, T>(in, out); return 0;
         case 8: run<8, T>(in, out); return 0;
+        case 15: run<15, T>(in, out); return 0;
         case 16: run<16, T>(in, out); return 0;
         default: return 1;
     }

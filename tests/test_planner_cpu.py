@@ -9,13 +9,13 @@ from conftest import fp64_fft, gaussian_complex, norm_scale, rel_l2
 from native_libs import butterfly, emulate
 
 
-@pytest.mark.parametrize("radix", [1, 2, 3, 4, 5, 7, 8, 16])
+@pytest.mark.parametrize("radix", [1, 2, 3, 4, 5, 7, 8, 15, 16])
 def test_butterflies_fp64(radix):
     x = gaussian_complex(radix, radix, np.complex128)
     assert np.max(np.abs(butterfly(radix, x) - np.fft.fft(x))) < 1e-14 * max(1, radix)
 
 
-@pytest.mark.parametrize("radix", [2, 3, 4, 5, 7, 8, 16])
+@pytest.mark.parametrize("radix", [2, 3, 4, 5, 7, 8, 15, 16])
 def test_butterflies_fp32(radix):
     x = gaussian_complex(radix, radix + 100, np.complex128)
     assert np.max(np.abs(butterfly(radix, x, double=False) - np.fft.fft(x))) < 2e-6 * radix

@@ -9,11 +9,14 @@ size-specialised single-pass kernel are packed into one grouped launch per lengt
 any batch up to 512 (syclfft_b200_execute_ex), created ahead of admission by a worker
 thread while the request waits. Families are spread over several CUDA
 streams so independent work overlaps on the device. Latency is measured from a request's
-arrival to the CUDA event that completes it; the per-request plain mode executes one
-request at a time with one plan execute each and waits for it, for comparison.
+arrival to the CUDA event that completes it. For comparison, the plain mode executes one
+request at a time on the resident plans and waits for it, and the plan-per-request mode
+does what a user of the plan API does for each request: create a plan for it, execute,
+wait, destroy.
 """
 from __future__ import annotations
 
+import bisect
 import ctypes
 import math
 import statistics
@@ -96,6 +99,62 @@ def make_request_stream(count=20000, rate=50000.0, seed=5, max_batch=512, float_
     return reqs
 
 
+class Arena:
+    """First-fit sub-allocator over one device buffer for the request buffers in flight: a
+    request is admitted when its buffers fit, so admission tracks the real free space and no
+    allocation or release during a run touches the CUDA allocator (whose retries after a
+    failed allocation synchronize the device)."""
+
+    ALIGN = 256
+
+    def __init__(self, tensor):
+        self.t = tensor
+        self.size = tensor.numel()
+        self.free = [(0, self.size)]  # (offset, bytes), sorted by offset, coalesced
+        self.used = 0
+
+    def alloc(self, nbytes):
+        n = (nbytes + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        for i, (off, sz) in enumerate(self.free):
+            if sz >= n:
+                if sz == n:
+                    del self.free[i]
+                else:
+                    self.free[i] = (off + n, sz - n)
+                self.used += n
+                return off
+        return None
+
+    def release(self, off, nbytes):
+        n = (nbytes + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        self.used -= n
+        i = bisect.bisect_left(self.free, (off, 0))
+        self.free.insert(i, (off, n))
+        # coalesce with the neighbours
+        if i + 1 < len(self.free) and self.free[i][0] + self.free[i][1] == self.free[i + 1][0]:
+            self.free[i] = (off, self.free[i][1] + self.free[i + 1][1])
+            del self.free[i + 1]
+        if i > 0 and self.free[i - 1][0] + self.free[i - 1][1] == self.free[i][0]:
+            self.free[i - 1] = (self.free[i - 1][0], self.free[i - 1][1] + self.free[i][1])
+            del self.free[i]
+
+    def view(self, off, nbytes, dtype):
+        return self.t[off: off + nbytes].view(dtype)
+
+
+def synthetic_input(r: Request, out=None, generator=None):
+    """The request's input: 2 * elements reals uniform in [-1, 1) from its seed, viewed as
+    complex (written into `out` when given, on the current stream)."""
+    import torch
+    fdt = torch.float64 if r.double else torch.float32
+    if out is None:
+        out = torch.empty(2 * r.elements, device="cuda", dtype=fdt)
+    g = generator if generator is not None else torch.Generator(device=out.device)
+    g.manual_seed(r.seed)
+    out.uniform_(-1.0, 1.0, generator=g)
+    return torch.view_as_complex(out.view(-1, 2))
+
+
 def _pow2_ceil(v):
     return 1 << max(0, (int(v) - 1).bit_length())
 
@@ -124,6 +183,8 @@ class Server:
         self.plans_created = 0
         self.pending = {}   # plan key -> future of a plan being created ahead of use
         self.pool = None
+        self._gen = None
+        self.arena = None   # request buffers of a run (Arena)
 
     # ---------------------------------------------------------------- resident state
     MAX_BATCH = 512
@@ -202,26 +263,32 @@ class Server:
             self.lib.syclfft_b200_group_destroy(g)
         self.plans.clear()
         self.groups.clear()
+        self.arena = None
         # hand the request buffers cached by torch back to the device for other pools
         self.torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- data
     def _fill(self, r: Request, stream):
-        """Input buffer filled with uniform[-1, 1) from the request's seed, and an output buffer.
-        Both come from the allocator's pool of the host thread's current stream (warmed at the
-        start of a run) and are marked as used on `stream`."""
+        """Input and output buffers of a request from the arena (r.buf_off, reserved at
+        admission), the input filled with uniform[-1, 1) from the request's seed on `stream`."""
         torch = self.torch
         fdt = torch.float64 if r.double else torch.float32
-        ri = torch.empty(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt)
-        r.inp = torch.view_as_complex(ri.view(-1, 2))
-        r.out = torch.empty_like(r.inp)
-        ri.record_stream(stream)
-        r.out.record_stream(stream)
+        buf = self.arena.view(r.buf_off, r.nbytes, fdt)
+        if self._gen is None:
+            self._gen = torch.Generator(device=f"cuda:{self.dev}")
         with torch.cuda.stream(stream):
-            g = torch.Generator(device=f"cuda:{self.dev}")
-            g.manual_seed(r.seed)
-            torch.rand(2 * r.elements, device=f"cuda:{self.dev}", dtype=fdt, generator=g, out=ri)
-            ri.mul_(2).sub_(1)
+            r.inp = synthetic_input(r, buf[: 2 * r.elements], self._gen)
+        r.out = torch.view_as_complex(buf[2 * r.elements:].view(-1, 2))
+
+    def _reserve(self, r: Request):
+        off = self.arena.alloc(r.nbytes)
+        if off is not None:
+            r.buf_off = off
+        return off is not None
+
+    def _release(self, r: Request):
+        self.arena.release(r.buf_off, r.nbytes)
+        r.inp = r.out = None
 
     def _execute_one(self, r: Request, stream):
         h = self._plan(r)
@@ -247,7 +314,9 @@ class Server:
 
     # ---------------------------------------------------------------- loops
     def run(self, requests, mode="served", keep_results=False):
-        """Serve `requests` (sorted by arrival); returns statistics. mode 'served' or 'plain'."""
+        """Serve `requests` (sorted by arrival); returns statistics. mode 'served' (continuous
+        batching), 'plain' (one request at a time on resident plans) or 'plan_per_request'
+        (one request at a time, each with its own plan created and destroyed around it)."""
         torch = self.torch
         reqs = sorted(requests, key=lambda r: r.arrival)
         for r in reqs:
@@ -255,22 +324,50 @@ class Server:
         start = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize(self.dev)
         torch.cuda.empty_cache()
-        # one cached segment the size of the admission budget: request buffers are carved from it
-        # without cudaMalloc during the run
+        # the admission budget as one arena for the request buffers, leaving room for resident
+        # plans and the streams' scratch arenas (CUDA memory pool)
         free, _ = torch.cuda.mem_get_info(self.dev)
-        # leave room for resident plans and the streams' scratch arenas (CUDA memory pool)
-        warm = int(min(self.budget, free - self.plan_budget - 8e9))
-        if warm > (1 << 20):
-            torch.empty(warm, dtype=torch.uint8, device=f"cuda:{self.dev}")
+        size = int(min(self.budget, free - self.plan_budget - 8e9))
+        if size < max(r.nbytes for r in reqs):
+            raise RuntimeError("admission budget smaller than the largest request")
+        self.arena = Arena(torch.empty(size, dtype=torch.uint8, device=f"cuda:{self.dev}"))
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
         start.record(self.streams[0])
         done_events = []
-        if mode == "plain":
+        if mode == "plan_per_request":
+            # The reference's usage: a plan for each request's exact shape, batch, direction
+            # and normalization, one execute, wait, destroy.
             s = self.streams[0]
             for r in reqs:
                 while time.perf_counter() - t0 < r.arrival:
                     pass
+                self._reserve(r)
+                self._fill(r, s)
+                cfg = _provider.make_config(list(r.lengths), r.batch, r.direction, r.double, False, r.normalization,
+                                            False, self.dev)
+                h = self.api.create(ctypes.byref(cfg), self.err, ERR)
+                if not h:
+                    raise RuntimeError(self.err.value.decode())
+                self.plans_created += 1
+                rc = self.api.execute(h, r.inp.data_ptr(), r.out.data_ptr(), s.cuda_stream, self.err, ERR)
+                if rc:
+                    raise RuntimeError(self.err.value.decode())
+                with torch.cuda.stream(s):
+                    ev = torch.cuda.Event(enable_timing=True)
+                    ev.record(s)
+                ev.synchronize()
+                self.api.destroy(h)
+                r.t_done = start.elapsed_time(ev) / 1e3
+                if keep_results:
+                    r.result = r.out.cpu()
+                self._release(r)
+        elif mode == "plain":
+            s = self.streams[0]
+            for r in reqs:
+                while time.perf_counter() - t0 < r.arrival:
+                    pass
+                self._reserve(r)
                 self._fill(r, s)
                 with torch.cuda.stream(s):
                     h = self._execute_one(r, s)
@@ -281,7 +378,7 @@ class Server:
                 r.t_done = start.elapsed_time(ev) / 1e3
                 if keep_results:
                     r.result = r.out.cpu()
-                r.inp = r.out = None
+                self._release(r)
         else:
             self._serve(reqs, t0, start, keep_results)
         torch.cuda.synchronize(self.dev)
@@ -315,7 +412,6 @@ class Server:
         waiting = deque()
         S = len(self.streams)
         in_flight = [deque() for _ in range(S)]  # per stream, in launch order: (event, [requests])
-        used = 0.0
         completed = 0
         while completed < len(reqs):
             now = time.perf_counter() - t0
@@ -323,14 +419,13 @@ class Server:
                 waiting.append(reqs[nxt])
                 self._prefetch(reqs[nxt])  # start its plan while it waits for admission
                 nxt += 1
-            # admission by HBM budget (FIFO; a request larger than the budget runs alone)
+            # admission by HBM budget: FIFO, while the request's buffers fit in the arena
             bins = {}
             while waiting:
                 r = waiting[0]
-                if used + r.nbytes > self.budget and used > 0:
+                if not self._reserve(r):
                     break
                 waiting.popleft()
-                used += r.nbytes
                 key = ("g", r.lengths[0], r.double) if self.groupable(r) else ("p", r.lengths, r.double)
                 bins.setdefault(key, []).append(r)
             # launch everything admitted: one grouped launch per length family
@@ -362,8 +457,7 @@ class Server:
                         r.t_done = t
                         if keep_results:
                             r.result = r.out.cpu()
-                        r.inp = r.out = None
-                        used -= r.nbytes
+                        self._release(r)
                     completed += len(rs)
                     progressed = True
             if progressed and self.retired:

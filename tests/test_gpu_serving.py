@@ -113,10 +113,7 @@ def test_serving_alone_vs_mix(torch):
             assert rel_l2(a, b) <= spec_tol(r.lengths[0], r.double), r
         # and against FP64 for a few
         for r in reqs[:12]:
-            g = torch.Generator(device="cuda").manual_seed(r.seed)
-            fdt = torch.float64 if r.double else torch.float32
-            xi = torch.rand(2 * r.elements, device="cuda", dtype=fdt, generator=g) * 2 - 1
-            x = torch.view_as_complex(xi.view(-1, 2)).cpu().numpy()
+            x = serving.synthetic_input(r).cpu().numpy()
             n = r.lengths[0]
             ref = fp64_fft(x, [n], r.batch, r.direction, norm_scale(r.normalization, r.direction, n))
             assert rel_l2(results[r.rid].numpy(), ref) <= spec_tol(n, r.double)

@@ -250,7 +250,8 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
-    opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal)
+    opts = sf.plan_options(placement=sf.placement.in_place, normalization=sf.normalization.orthogonal,
+                           split_precision=args.split)
     plans, bufs, hosts = [], [], []
     workload = [w for w in WORKLOAD if not args.only or w[0] == args.only]
     if args.plan:
@@ -401,7 +402,8 @@ def run_ours(args):
                        else "subset", "plans": [f"{w[0]} (batch {w[2]})" for w in workload],
                        "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
                        "parallelism": f"replicas x{world} (independent batches per GPU)",
-                       "l2": "inputs larger than L2 (no flush)"},
+                       "l2": "inputs larger than L2 (no flush)",
+                       "split_precision": args.split},
             "gbs_alg": round(alg_bytes_step * world * args.steps / (elapsed_ms / 1e3) / 1e9, 1),
             "per_plan": per_plan,
             "roofline": roofline,
@@ -594,6 +596,8 @@ def main():
     ap.add_argument("--only", default="", help="run one plan of the workload (profiling)")
     ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
     ap.add_argument("--plan", default="", help="replace the workload: N[xM[xK]]:batch:c64|c128[,...]")
+    ap.add_argument("--split", action="store_true",
+                    help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
     ap.add_argument("--config", type=int, choices=[3, 4], default=0,
                     help="run a secondary configuration instead (3: Bluestein primes, 4: 3D/2D)")

@@ -137,6 +137,17 @@ def dist_env():
     return world, rank, local
 
 
+def max_over_ranks(values, world, device):
+    """Element-wise maximum of per-rank floats: every multi-GPU time is the slowest rank's
+    (the caller's process group: NCCL on GPUs, gloo in the CPU tests)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
 def cpu_baseline(sample_div: int = 2, repeats: int = 10):
     """Oracle (CPU restatement of the portable provider) on 1/sample_div of each batch."""
     import numpy as np
@@ -307,11 +318,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = clocks.stop()
     barrier()
-    elapsed_ms = start.elapsed_time(end)
-    t = torch.tensor([elapsed_ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks([start.elapsed_time(end)], world, dev)[0]
     total_flops = step_flops(workload) * args.steps * world
     value = total_flops / (elapsed_ms / 1e3) / 1e9
 
@@ -378,10 +385,7 @@ def run_ours(args):
             e2e_step()
         e2.record(stream)
         torch.cuda.synchronize()
-        t2 = torch.tensor([s2.elapsed_time(e2)], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t2.item())
+        e2e_ms = max_over_ranks([s2.elapsed_time(e2)], world, dev)[0]
         e2e = {"value": step_flops(workload) * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": args.e2e_steps,
                "ms_per_step": e2e_ms / args.e2e_steps}

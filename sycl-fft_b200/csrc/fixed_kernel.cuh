@@ -67,6 +67,7 @@ enum : int {
     kFeatPostmul = 16,
     kFeatTw4Conj = 32,
     kFeatConv = 64,
+    kFeatSmemIn = 128,  // the first stage reads the tile from shared memory (TMA-staged passes)
 };
 
 template <class T>
@@ -114,7 +115,14 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * TPL;
         if (X.active && (EXACT || j < NR)) {
-            if constexpr (FIRST && (FEAT & kFeatPremul)) {
+            if constexpr (FIRST && (FEAT & kFeatSmemIn)) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    C a = MODEC ? X.sm[(j + r * NR) * W] : X.sm[pidx<T>(j + r * NR)];
+                    if (X.conj_in) a.y = -a.y;
+                    v[i * R + r] = a;
+                }
+            } else if constexpr (FIRST && (FEAT & kFeatPremul)) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
                     const int k = j + r * NR;
@@ -153,7 +161,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             }
         }
     }
-    if constexpr (!FIRST) __syncthreads();
+    if constexpr (!FIRST || (FEAT & kFeatSmemIn)) __syncthreads();
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * TPL;

@@ -345,6 +345,8 @@ struct Builder {
             if (smem > smem_limit || p.in.d != 1 || p.out.d != 1 || p.in.cs != 1 || p.out.cs != 1) return;
             p.w = e->w;
             ps.smem_bytes = smem;
+            // contiguous lines, columns of at most one tensor-map box: the TMA-staged variant
+            ps.tma = req.use_tma && p.n <= 256 && p.in.ks * p.n == p.in.hi && p.n_outer >= 1;
         } else {
             if (rows % e->w != 0) return;
             const int64_t smem = static_cast<int64_t>(e->w) * p.pitch * cs;
@@ -1263,7 +1265,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
-           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"tma\":" << (ps.tma ? 1 : 0) << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
            << ps.cl_p << "]}";
     }
     os << "]}";

@@ -59,6 +59,7 @@ struct PassSpec {
                              // buffers are 16-byte aligned; otherwise fixed_id runs
     int cl_n1 = 0, cl_n2 = 0, cl_p = 0;
     int tc_id = -1;          // split-precision tensor-core kernel (tc_catalog.h), float plans only
+    bool tma = false;        // four-step column pass with a TMA-staged variant of fixed_id (tma_cols_kernel.cuh)
     int blue_id = -1;        // size-specialised Bluestein kernel (bluestein_catalog.h)
     int blue_kind = -1;      // its kind: kBlueFused / kBlueColsFwd / kBlueRowsConv / kBlueColsInv
 };
@@ -121,6 +122,8 @@ struct PlanRequest {
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
     bool no_cluster = false; // force the two-pass four-step for long lines
     bool no_piped = false;   // never use the copy-engine-pipelined kernels
+    bool use_tma = false;    // four-step column passes on the TMA-staged kernels (opt-in: measured
+                             // level with the plain size-specialised kernel on B200)
     int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size
     bool device_spectrum = false;  // leave Bluestein chirp/spectrum tables to the device (zeroed here)
     // complex<float> only: run the radix-16 butterflies of eligible single-pass axes as BF16

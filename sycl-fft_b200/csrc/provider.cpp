@@ -28,6 +28,7 @@
 #include "launch.hpp"
 #include "piped_launch.hpp"
 #include "tc_launch.hpp"
+#include "tma_launch.hpp"
 #include "bluestein_launch.hpp"
 #include "planner.hpp"
 
@@ -292,6 +293,8 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
+    // SYCLFFT_B200_TMA=1: four-step column passes on the TMA-staged kernels.
+    if (const char* k = std::getenv("SYCLFFT_B200_TMA")) req.use_tma = std::strcmp(k, "1") == 0;
     // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
     if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
     // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
@@ -461,6 +464,31 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
     }
 }
 
+// TMA-staged four-step column pass; false when the tensor map cannot describe the buffer
+// (the caller then runs the plain size-specialised kernel).
+bool launch_tma(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cudaStream_t stream) {
+    const PassParams& p = bp.p;
+    const FixedParams& f = bp.fp;
+    TmaColParams q;
+    q.col_tiles = static_cast<int>((p.n_cols + f.w - 1) / f.w);
+    q.n2 = static_cast<int>(p.n_cols);
+    q.tiles = p.n_outer * q.col_tiles;
+    q.out_hi = p.out.hi;
+    q.out_ks = p.out.ks;
+    q.tw = f.tw;
+    q.tw4_hi = f.tw4_hi;
+    q.tw4_lo = f.tw4_lo;
+    q.tw4_shift = f.tw4_shift;
+    q.conj_in = f.conj_in;
+    q.conj_out = f.conj_out;
+    q.scale = f.scale;
+    q.status = plan->status;
+    const cudaError_t e = launch_tma_cols(bp.spec_ref().fixed_id, src, dst, p.n_outer, q, stream);
+    if (e == cudaErrorInvalidValue) return false;
+    check(e, "FFT TMA column pass launch");
+    return true;
+}
+
 // Launches one bound pass of a plan on its kernel family.
 void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cudaStream_t stream) {
     const bool aligned = (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0);
@@ -477,6 +505,8 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
         check(launch_piped(ps.piped_id, bp.pp, grid, src, dst, stream), "FFT pipelined pass launch");
     } else if (ps.cluster_id >= 0) {
         check(launch_cluster(ps.cluster_id, bp.cp, src, dst, stream), "FFT cluster pass launch");
+    } else if (ps.tma && aligned && launch_tma(plan, bp, src, dst, stream)) {
+        // launched on the TMA-staged kernel
     } else if (ps.fixed_id >= 0) {
         check(launch_fixed(ps.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, ps.threads,
                            static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
@@ -548,6 +578,7 @@ struct Knobs {
     const char* name;
     bool no_fixed, no_piped, no_cluster;
     int cluster_p, force_w, force_maxv;
+    bool use_tma;
 };
 
 std::string tune_key(const PlanRequest& r, int device) {
@@ -610,16 +641,17 @@ PlanRequest apply(PlanRequest r, const Knobs& k) {
     r.cluster_p = k.cluster_p;
     r.force_w = k.force_w;
     r.force_maxv = k.force_maxv;
+    r.use_tma = k.use_tma || r.use_tma;
     return r;
 }
 
 PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
     static const Knobs kCandidates[] = {
-        {"default", false, false, false, 0, 0, 0},    {"generic", true, false, false, 0, 0, 0},
-        {"no_pipeline", false, true, false, 0, 0, 0}, {"cluster8", false, false, false, 8, 0, 0},
-        {"cluster16", false, false, false, 16, 0, 0}, {"w1", false, false, false, 0, 1, 0},
-        {"w2", false, false, false, 0, 2, 0},         {"w4", false, false, false, 0, 4, 0},
-        {"maxv16", true, false, false, 0, 0, 16},
+        {"default", false, false, false, 0, 0, 0, false},    {"generic", true, false, false, 0, 0, 0, false},
+        {"no_pipeline", false, true, false, 0, 0, 0, false}, {"cluster8", false, false, false, 8, 0, 0, false},
+        {"cluster16", false, false, false, 16, 0, 0, false}, {"w1", false, false, false, 0, 1, 0, false},
+        {"w2", false, false, false, 0, 2, 0, false},         {"w4", false, false, false, 0, 4, 0, false},
+        {"maxv16", true, false, false, 0, 0, 16, false},     {"tma", false, false, false, 0, 0, 0, true},
     };
     const std::string key = tune_key(req, device);
     auto& cache = tune_cache();

@@ -323,3 +323,25 @@ def test_multidim_full_configs(sf, torch):
     y = uniform_complex(2048 * 2048, 12, np.complex128)
     out, _ = run(sf, torch, y, [2048, 2048], 1, -1, 0, True)
     assert rel_l2(out, fp64_fft(y, [2048, 2048], 1, -1)) < spec_tol(2048 * 2048, True)
+
+
+@pytest.mark.parametrize("shape,batch,dbl", [([65536], 6, True), ([65536], 5, False), ([16384], 7, True),
+                                             ([131072], 2, False)], ids=str)
+def test_tma_staged_column_pass(shape, batch, dbl, monkeypatch):
+    """Four-step plans with the column pass on the TMA-staged kernel (tensor-map box loads into
+    shared memory, opt-in), forward and backward, against FP64."""
+    import torch
+    import syclfft_b200 as sf
+    monkeypatch.setenv("SYCLFFT_B200_TMA", "1")
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 31 + n, dt)
+    for d in (sf.direction.forward, sf.direction.backward):
+        p = sf.plan_many_dft("double" if dbl else "float", shape, batch, d)
+        assert any(ps.get("tma") for ps in p.describe()["passes"]), p.describe()
+        xi = torch.from_numpy(x).cuda()
+        out = torch.empty_like(xi)
+        p.execute(xi, out).synchronize()
+        ref = fp64_fft(x, shape, batch, int(d))
+        tol = (1e-12 if dbl else 1e-5) * math.log2(n)
+        assert rel_l2(out.cpu().numpy(), ref) <= tol

@@ -218,6 +218,32 @@ template <int R, class C> SFB_HD void twiddle_powers(C* u, C w) {
     for (int r = 1; r < R; ++r) u[r] = cmul(u[r], p[r - 1]);
 }
 
+// Radix 15 twiddles u[r] *= w^r with few live registers: the powers of the balanced tree
+// (w^r = w^h * w^(r-h), at most 4 roundings deep) are formed right before their use, so only
+// w, w^2, w^4, w^8 and w^12 stay live instead of all fourteen.
+template <class C> SFB_HD void twiddle_powers15(C* u, C w) {
+    const C w2 = cmul(w, w);
+    const C w4 = cmul(w2, w2);
+    const C w8 = cmul(w4, w4);
+    u[1] = cmul(u[1], w);
+    u[2] = cmul(u[2], w2);
+    u[3] = cmul(u[3], cmul(w2, w));
+    u[4] = cmul(u[4], w4);
+    u[5] = cmul(u[5], cmul(w4, w));
+    const C w6 = cmul(w4, w2);
+    u[6] = cmul(u[6], w6);
+    u[7] = cmul(u[7], cmul(w6, w));
+    u[8] = cmul(u[8], w8);
+    u[9] = cmul(u[9], cmul(w8, w));
+    const C w10 = cmul(w8, w2);
+    u[10] = cmul(u[10], w10);
+    u[11] = cmul(u[11], cmul(w10, w));
+    const C w12 = cmul(w8, w4);
+    u[12] = cmul(u[12], w12);
+    u[13] = cmul(u[13], cmul(w12, w));
+    u[14] = cmul(u[14], cmul(w12, w2));
+}
+
 template <int R, class T, class C> SFB_HD void dft(C* v) {
     if constexpr (R == 1) {
         (void)v;

@@ -170,7 +170,8 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             const int jm = j % NS;
             if constexpr (NS > 1 && R > 1) {
                 // base-twiddle table: one W_(NS*R)^jm per butterfly, powers in registers
-                twiddle_powers<R>(u, __ldg(X.twb + TWOFF + jm));
+                if constexpr (R == 15) twiddle_powers15(u, __ldg(X.twb + TWOFF + jm));
+                else twiddle_powers<R>(u, __ldg(X.twb + TWOFF + jm));
             }
             dft<R, T>(u);
             if constexpr (LAST && (FEAT & (kFeatTStore | kFeatMid))) {

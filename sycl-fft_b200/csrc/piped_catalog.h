@@ -11,5 +11,5 @@
 #pragma once
 
 #define SFB_PIPED_CATALOG(X)                 \
-    X(0, 0, 13440, 896, 896, 16, 8, 3, 5, 7) \
+    X(0, 0, 13440, 896, 896, 16, 8, 15, 7) \
     X(1, 0, 8192, 512, 512, 16, 16, 16, 2)

@@ -552,6 +552,148 @@ def run_config(args):
     return 0
 
 
+def run_table(args):
+    """Every configuration's rows on one GPU, one JSON line (the source of BASELINE.md):
+    P  the provider's plain per-plan execute (estimate planning), device-resident, CUDA events;
+    A  autotuned plans (planning_mode::measure) replayed from a captured CUDA graph;
+    C  cuFFT through torch.fft as a black box (informational);
+    CPU the CPU restatement of the reference's portable provider on a bounded sample, all host
+        threads; accuracy of P: relative L2 and max error against FP64 on sampled lines."""
+    import numpy as np
+    import torch
+    import syclfft_b200 as sf
+    from oracle import portable
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    portable.build()
+    threads = portable.max_threads()
+    portable.set_threads(threads)
+    peak, _ = measured_peaks()
+    N = sf.normalization
+    cases = [
+        # (row, shape, batch, double, in_place, normalization, directions, input, cpu sample lines)
+        ("1: c64 N=1024 B=1 fwd oop", [1024], 1, False, False, "none", (-1,), "uniform", 1),
+        ("2a: c64 4096x16384 fwd+bwd ip ortho", [4096], 16384, False, True, "orthogonal", (-1, 1), "uniform", 256),
+        ("2b: c64 13440x4096", [13440], 4096, False, True, "orthogonal", (-1, 1), "uniform", 64),
+        ("2c: c128 65536x512", [65536], 512, True, True, "orthogonal", (-1, 1), "uniform", 8),
+        ("3: c64 N=1009 x256 oop fwd-norm", [1009], 256, False, False, "forward", (-1,), "gaussian", 64),
+        ("3: c128 N=1009 x256", [1009], 256, True, False, "forward", (-1,), "gaussian", 64),
+        ("3: c64 N=4099 x256", [4099], 256, False, False, "forward", (-1,), "gaussian", 16),
+        ("3: c128 N=4099 x256", [4099], 256, True, False, "forward", (-1,), "gaussian", 16),
+        ("3: c64 N=65537 x256", [65537], 256, False, False, "forward", (-1,), "gaussian", 2),
+        ("3: c128 N=65537 x256", [65537], 256, True, False, "forward", (-1,), "gaussian", 2),
+        ("4a: 3D c64 256^3 ip fwd+bwd bwd-norm", [256, 256, 256], 1, False, True, "backward", (-1, 1), "waves", 1),
+        ("4b: 2D c128 2048^2 oop fwd+bwd", [2048, 2048], 1, True, False, "none", (-1, 1), "waves", 1),
+    ]
+
+    def timed(fn, reps=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    rows = []
+    for row, shape, batch, dbl, ip, norm, dirs, kind, cpu_lines in cases:
+        n = math.prod(shape)
+        dt = np.complex128 if dbl else np.complex64
+        rng = np.random.default_rng(n + batch)
+        if kind == "waves":
+            x = _plane_wave_input(shape, n, dt)
+        elif kind == "gaussian":
+            x = (rng.standard_normal(n * batch) + 1j * rng.standard_normal(n * batch)).astype(dt)
+        else:
+            x = (rng.uniform(-1, 1, n * batch) + 1j * rng.uniform(-1, 1, n * batch)).astype(dt)
+        fl = flops(shape, batch) * len(dirs)
+        nbytes = 2 * n * batch * (16 if dbl else 8) * len(dirs)
+        scalar = "double" if dbl else "float"
+        out = {"row": row}
+        for form, planning in (("P", sf.planning_mode.estimate), ("A", sf.planning_mode.measure)):
+            opts = sf.plan_options(placement=sf.placement.in_place if ip else sf.placement.out_of_place,
+                                   normalization=getattr(N, norm), planning=planning)
+            plans = [sf.plan_many_dft(scalar, shape, batch, sf.direction(d), opts) for d in dirs]
+            a = torch.from_numpy(x).to(dev)
+            b = a if ip else torch.empty_like(a)
+            c = a if ip else torch.empty_like(a)
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+
+            def step():
+                plans[0].execute(a) if ip else plans[0].execute(a, b)
+                if len(plans) > 1:
+                    plans[1].execute(a) if ip else plans[1].execute(b, c)
+
+            if form == "P":
+                if len(dirs) == 1 or not ip:
+                    step()
+                    got = (a if ip else b).cpu().numpy() if len(dirs) == 1 else b.cpu().numpy()
+                else:
+                    plans[0].execute(a)
+                    got = a.cpu().numpy()
+                    a.copy_(torch.from_numpy(x).to(dev))
+                lines = min(batch, 8)
+                xs = x[: lines * n].astype(np.complex128)
+                if shape == [1009]:
+                    k = np.arange(n)
+                    ref = (xs.reshape(lines, n) @ np.exp(-2j * np.pi * np.outer(k, k) / n)).reshape(-1)
+                else:
+                    ref = np.fft.fftn(xs.reshape([lines] + shape), axes=tuple(range(1, len(shape) + 1))).reshape(-1)
+                scale = {"none": 1.0, "forward": 1.0 / n, "backward": 1.0, "orthogonal": n ** -0.5}[norm]
+                ref = ref * scale
+                d = got[: lines * n].astype(np.complex128) - ref
+                out["rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(ref))
+                out["max_rel"] = float(np.abs(d).max() / np.abs(ref).max())
+                with torch.cuda.stream(s):
+                    ms = timed(step)
+            else:
+                with torch.cuda.stream(s):
+                    step()
+                torch.cuda.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=s):
+                    step()
+                ms = timed(g.replay)
+                out["A_tuning"] = [p.describe().get("tuning") for p in plans][0]
+                del g
+            out[form] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1), "gbs": round(nbytes / ms / 1e6, 1),
+                         "frac": round(nbytes / ms / 1e6 / peak, 4)}
+            del plans, a, b, c
+        # C: cuFFT via torch (informational)
+        xt = torch.from_numpy(x).to(dev).view([batch] + shape)
+        tn = {"none": "backward", "forward": "forward", "backward": "backward", "orthogonal": "ortho"}[norm]
+        dims = tuple(range(1, len(shape) + 1))
+
+        def cufft():
+            y = torch.fft.fftn(xt, dim=dims, norm=tn)
+            if len(dirs) > 1:
+                torch.fft.ifftn(y, dim=dims, norm=tn)
+
+        ms = timed(cufft)
+        out["C_torch_cufft"] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1)}
+        del xt
+        # CPU restatement on a sample of lines
+        cb = max(1, min(batch, cpu_lines))
+        xs = x[: cb * n]
+        cps = [portable.OraclePlan(shape, cb, d, norm, dbl) for d in dirs]
+        t0 = time.perf_counter()
+        y = cps[0].execute(xs)
+        if len(cps) > 1:
+            cps[1].execute(y)
+        t = time.perf_counter() - t0
+        out["CPU"] = {"gflops": round(flops(shape, cb) * len(dirs) / t / 1e9, 2), "sample_lines": cb, "s": round(t, 3)}
+        rows.append(out)
+        print(json.dumps(out), file=sys.stderr, flush=True)
+    torch.cuda.empty_cache()
+    print(json.dumps({"metric": "per-configuration rows (P, A, C, CPU) and accuracy", "cpu_threads": threads,
+                      "peak_gbs": peak, "rows": rows}), flush=True)
+    return 0
+
+
 def run_serve(args):
     """Serving configuration: the mixed request stream through the continuous-batching loop
     and through per-request plain executes; one JSON line with both."""
@@ -603,6 +745,7 @@ def main():
     ap.add_argument("--split", action="store_true",
                     help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
+    ap.add_argument("--table", action="store_true", help="every configuration's rows (BASELINE.md)")
     ap.add_argument("--config", type=int, choices=[3, 4], default=0,
                     help="run a secondary configuration instead (3: Bluestein primes, 4: 3D/2D)")
     ap.add_argument("--requests", type=int, default=20000)
@@ -617,6 +760,8 @@ def main():
         return run_serve(args)
     if args.config:
         return run_config(args)
+    if args.table:
+        return run_table(args)
     return run_ours(args)
 
 

@@ -386,6 +386,15 @@ struct Builder {
 
     // Choose N1 * N2 = n with both factors fitting one CTA; most balanced, N2 >= N1.
     bool split(int64_t n, int64_t& n1, int64_t& n2) {
+        // a requested column length (tuning), when it divides n and both factors fit a CTA
+        if (req.force_n1 > 1 && n % req.force_n1 == 0) {
+            const int64_t a = req.force_n1, b = n / a;
+            if (fits(a, kModeC) && fits(b, kModeK) && fits(b, kModeC)) {
+                n1 = a;
+                n2 = b;
+                return true;
+            }
+        }
         int64_t best1 = 0;
         double best_score = 1e300;
         for (int64_t d = 2; d * d <= n; ++d) {

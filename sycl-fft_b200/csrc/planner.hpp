@@ -118,6 +118,7 @@ struct PlanRequest {
     // tuning knobs (0 = heuristic)
     int force_maxv = 0;
     int force_w = 0;
+    int force_n1 = 0;        // four-step column length (0: the most balanced split)
     int smem_limit = 0;      // bytes, 0 = device default (227 KB)
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
     bool no_cluster = false; // force the two-pass four-step for long lines

@@ -293,6 +293,8 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
+    // SYCLFFT_B200_SPLIT_N1=<n1>: four-step column length, where it divides the axis.
+    if (const char* k = std::getenv("SYCLFFT_B200_SPLIT_N1")) req.force_n1 = std::atoi(k);
     // SYCLFFT_B200_TMA=1: four-step column passes on the TMA-staged kernels.
     if (const char* k = std::getenv("SYCLFFT_B200_TMA")) req.use_tma = std::strcmp(k, "1") == 0;
     // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
@@ -579,6 +581,7 @@ struct Knobs {
     bool no_fixed, no_piped, no_cluster;
     int cluster_p, force_w, force_maxv;
     bool use_tma;
+    int force_n1;
 };
 
 std::string tune_key(const PlanRequest& r, int device) {
@@ -642,6 +645,7 @@ PlanRequest apply(PlanRequest r, const Knobs& k) {
     r.force_w = k.force_w;
     r.force_maxv = k.force_maxv;
     r.use_tma = k.use_tma || r.use_tma;
+    if (k.force_n1) r.force_n1 = k.force_n1;
     return r;
 }
 
@@ -652,6 +656,9 @@ PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
         {"cluster16", false, false, false, 16, 0, 0, false}, {"w1", false, false, false, 0, 1, 0, false},
         {"w2", false, false, false, 0, 2, 0, false},         {"w4", false, false, false, 0, 4, 0, false},
         {"maxv16", true, false, false, 0, 0, 16, false},     {"tma", false, false, false, 0, 0, 0, true},
+        {"split64", false, false, false, 0, 0, 0, false, 64},   {"split128", false, false, false, 0, 0, 0, false, 128},
+        {"split256", false, false, false, 0, 0, 0, false, 256}, {"split512", false, false, false, 0, 0, 0, false, 512},
+        {"split1024", false, false, false, 0, 0, 0, false, 1024},
     };
     const std::string key = tune_key(req, device);
     auto& cache = tune_cache();

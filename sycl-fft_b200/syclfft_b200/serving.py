@@ -268,16 +268,20 @@ class Server:
         self.torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- data
-    def _fill(self, r: Request, stream):
+    def _fill(self, r: Request, stream=None):
         """Input and output buffers of a request from the arena (r.buf_off, reserved at
-        admission), the input filled with uniform[-1, 1) from the request's seed on `stream`."""
+        admission), the input filled with uniform[-1, 1) from the request's seed on `stream`
+        (default: the current stream)."""
         torch = self.torch
         fdt = torch.float64 if r.double else torch.float32
         buf = self.arena.view(r.buf_off, r.nbytes, fdt)
         if self._gen is None:
             self._gen = torch.Generator(device=f"cuda:{self.dev}")
-        with torch.cuda.stream(stream):
+        if stream is None:
             r.inp = synthetic_input(r, buf[: 2 * r.elements], self._gen)
+        else:
+            with torch.cuda.stream(stream):
+                r.inp = synthetic_input(r, buf[: 2 * r.elements], self._gen)
         r.out = torch.view_as_complex(buf[2 * r.elements:].view(-1, 2))
 
     def _reserve(self, r: Request):
@@ -432,10 +436,10 @@ class Server:
             for key, rs in bins.items():
                 si = hash(key) % S
                 s = self.streams[si]
-                for r in rs:
-                    self._fill(r, s)
                 used_plans = []
                 with torch.cuda.stream(s):
+                    for r in rs:
+                        self._fill(r)
                     if key[0] == "g":
                         self._execute_group((key[1], key[2]), rs, s)
                     else:

@@ -289,22 +289,33 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     launches_per_step = sum(f.launches() + b.launches() for _, _, _, _, f, b in plans)
 
-    def step(record=None):
+    def step(s, record=None):
         for i, (label, lengths, batch, dbl, f, b) in enumerate(plans):
             if record is not None:
-                record[i][0].record(stream)
-            f.execute(bufs[i])
+                record[i][0].record(s)
+            f.execute(bufs[i], stream=s)
             if record is not None:
-                record[i][1].record(stream)
-            b.execute(bufs[i])
+                record[i][1].record(s)
+            b.execute(bufs[i], stream=s)
             if record is not None:
-                record[i][2].record(stream)
+                record[i][2].record(s)
 
     for _ in range(args.warmup):
-        step()
+        step(stream)
     torch.cuda.synchronize()
-    # per-execute events across the timed region (for the roofline of the dominant kernel)
-    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in plans] for _ in range(args.steps)]
+    # The batched form: one step (every plan's forward and backward execute) captured once into
+    # a CUDA graph and replayed, so the timed region has no host launch work between kernels.
+    graph = None
+    if not args.no_graph:
+        cap = torch.cuda.Stream(dev)
+        cap.wait_stream(stream)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=cap):
+            step(cap)
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local)
     barrier()
@@ -313,11 +324,22 @@ def run_ours(args):
     time.sleep(0.3)
     start.record(stream)
     for k in range(args.steps):
-        step(ev[k])
+        if graph is not None:
+            graph.replay()
+        else:
+            step(stream)
     end.record(stream)
     torch.cuda.synchronize()
     clk = clocks.stop()
+    graph = None  # released before any process-group teardown
     barrier()
+    # per-execute events on plain launches of the same step (for the per-plan times and the
+    # roofline of the dominant kernel)
+    n_ev = min(args.steps, 100)
+    ev = [[[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in plans] for _ in range(n_ev)]
+    for k in range(n_ev):
+        step(stream, ev[k])
+    torch.cuda.synchronize()
     elapsed_ms = max_over_ranks([start.elapsed_time(end)], world, dev)[0]
     total_flops = step_flops(workload) * args.steps * world
     value = total_flops / (elapsed_ms / 1e3) / 1e9
@@ -325,8 +347,8 @@ def run_ours(args):
     # per-plan execute times inside the timed region
     per_plan = {}
     for i, (label, lengths, batch, dbl, f, b) in enumerate(plans):
-        fw = [ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)]
-        bw = [ev[k][i][1].elapsed_time(ev[k][i][2]) for k in range(args.steps)]
+        fw = [ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(n_ev)]
+        bw = [ev[k][i][1].elapsed_time(ev[k][i][2]) for k in range(n_ev)]
         nbytes = 2 * math.prod(lengths) * batch * (16 if dbl else 8)
         per_plan[label] = {"fwd_ms": statistics.mean(fw), "bwd_ms": statistics.mean(bw),
                            "launches_per_execute": f.launches(),
@@ -407,6 +429,7 @@ def run_ours(args):
                        "placement": "in_place", "normalization": "orthogonal", "directions": "forward+backward",
                        "parallelism": f"replicas x{world} (independent batches per GPU)",
                        "l2": "inputs larger than L2 (no flush)",
+                       "execution": "plain launches" if args.no_graph else "CUDA graph of one step, replayed",
                        "split_precision": args.split},
             "gbs_alg": round(alg_bytes_step * world * args.steps / (elapsed_ms / 1e3) / 1e9, 1),
             "per_plan": per_plan,
@@ -742,6 +765,8 @@ def main():
     ap.add_argument("--only", default="", help="run one plan of the workload (profiling)")
     ap.add_argument("--batch-div", type=int, default=1, help="divide batch counts (profiling small cases)")
     ap.add_argument("--plan", default="", help="replace the workload: N[xM[xK]]:batch:c64|c128[,...]")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="time plain launches of the step instead of its captured CUDA graph")
     ap.add_argument("--split", action="store_true",
                     help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")

@@ -43,6 +43,10 @@ struct plan_options {
     syclfft_b200::normalization normalization = syclfft_b200::normalization::none;
     planning_mode planning = planning_mode::estimate;
     provider preferred_provider = provider::automatic;
+    // B200 extension, no counterpart in syclfft::plan_options: complex<float> plans run the
+    // radix-16 butterflies of eligible axes (256 / 4096 points) as BF16 hi/lo products with
+    // FP32 accumulation on the tensor cores (about 1e-5 relative L2); ignored for double.
+    bool split_precision = false;
 };
 
 struct provider_status {

@@ -94,9 +94,12 @@ std::vector<std::string> provider_search_paths() {
     return result;
 }
 
+using syclfft_b200_create_ex_fn = void* (*)(const syclfft_b200_plan_config_v1*, uint32_t, char*, size_t);
+
 struct loaded_provider {
     const syclfft_b200_provider_v1* api{};
     std::shared_ptr<void> module;
+    syclfft_b200_create_ex_fn create_ex{};  // optional extension (split precision)
 };
 
 // provider_loader.cpp:178-232: first module in the search path that exports the entry
@@ -123,7 +126,8 @@ loaded_provider load_b200_provider() {
         const auto* api = reinterpret_cast<syclfft_b200_get_provider_v1_fn>(symbol)();
         if (!api || api->abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION)
             throw exception(error_code::plugin_error, "Provider 'syclfft_provider_b200' has an incompatible ABI");
-        return {api, std::move(module)};
+        auto create_ex = reinterpret_cast<syclfft_b200_create_ex_fn>(dlsym(raw, "syclfft_b200_create_ex"));
+        return {api, std::move(module), create_ex};
     }
     throw exception(error_code::provider_unavailable, "Unable to load provider 'syclfft_provider_b200': " + errors);
 }
@@ -192,7 +196,14 @@ public:
         config.normalization = static_cast<uint32_t>(options_.normalization);
         config.measure = options_.planning == planning_mode::measure ? 1 : 0;
         config.device = queue_.device;
-        handle_ = module_.api->create(&config, error.data(), error.size());
+        if (options_.split_precision && std::is_same_v<Scalar, float>) {
+            if (!module_.create_ex)
+                throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_ex");
+            handle_ = module_.create_ex(&config, SYCLFFT_B200_CREATE_SYNC | SYCLFFT_B200_CREATE_SPLIT_BF16,
+                                        error.data(), error.size());
+        } else {
+            handle_ = module_.api->create(&config, error.data(), error.size());
+        }
         if (!handle_) {
             throw exception(error_code::planning_failed, error[0] ? error.data() : "B200 plan creation failed");
         }

@@ -660,6 +660,10 @@ PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
         {"split256", false, false, false, 0, 0, 0, false, 256}, {"split512", false, false, false, 0, 0, 0, false, 512},
         {"split1024", false, false, false, 0, 0, 0, false, 1024},
     };
+    // one tuner at a time in the process: the cache is shared, and concurrent timings would
+    // measure each other
+    static std::mutex tune_mu;
+    std::lock_guard<std::mutex> tune_lock(tune_mu);
     const std::string key = tune_key(req, device);
     auto& cache = tune_cache();
     auto hit = cache.find(key);

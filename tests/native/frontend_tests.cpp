@@ -267,6 +267,27 @@ try {
                   "event-span dependency ordering failed");
         cudaStreamDestroy(producer);
     }
+    {
+        // B200 extension: split-precision tensor-core plans through the same plan API
+        const std::size_t n = 256, batch = 16, count = n * batch;
+        std::vector<std::complex<float>> source(count);
+        for (std::size_t i = 0; i < count; ++i)
+            source[i] = {static_cast<float>((i * 11 + 2) % 17) / 8.f, static_cast<float>((i * 3 + 1) % 13) / 7.f};
+        const auto expected = reference_many(source, {n}, batch, sf::direction::forward);
+        device_buffer<std::complex<float>> input(count), output(count);
+        input.write(source);
+        auto opts = make_plan_options(sf::placement::out_of_place, sf::normalization::none, sf::provider::b200);
+        opts.split_precision = true;
+        auto fft = sf::plan_many_dft<float>(sf::queue{}, {n}, batch, sf::direction::forward, opts);
+        fft.execute(input.get(), output.get()).wait_and_throw();
+        const auto actual = output.read();
+        double num = 0, den = 0;
+        for (std::size_t i = 0; i < count; ++i) {
+            num += std::norm(std::complex<double>(actual[i]) - std::complex<double>(expected[i]));
+            den += std::norm(std::complex<double>(expected[i]));
+        }
+        check(std::sqrt(num / den) < 2e-5, "split-precision plan mismatch");
+    }
     // sycl_tests.cpp:508-538
     expect_error(sf::error_code::provider_unavailable, [&] {
         (void)sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward,

@@ -609,6 +609,8 @@ def run_table(args):
         ("4b: 2D c128 2048^2 oop fwd+bwd", [2048, 2048], 1, True, False, "none", (-1, 1), "waves", 1),
     ]
 
+    cases = [c for c in cases if c[0].startswith(args.table_rows)]
+
     def timed(fn, reps=20):
         for _ in range(3):
             fn()
@@ -711,10 +713,72 @@ def run_table(args):
         out["CPU"] = {"gflops": round(flops(shape, cb) * len(dirs) / t / 1e9, 2), "sample_lines": cb, "s": round(t, 3)}
         rows.append(out)
         print(json.dumps(out), file=sys.stderr, flush=True)
+    rows.extend(_real_rows(sf, torch, dev, peak, timed, args.table_rows))
     torch.cuda.empty_cache()
     print(json.dumps({"metric": "per-configuration rows (P, A, C, CPU) and accuracy", "cpu_threads": threads,
                       "peak_gbs": peak, "rows": rows}), flush=True)
     return 0
+
+
+def _real_rows(sf, torch, dev, peak, timed, prefix=""):
+    """Real transforms (R2C then C2R, backward normalization): P = the provider's plans, C = torch.fft
+    rfft/irfft (cuFFT). GFLOP/s counts 2.5 N log2 N per real transform; bytes are the algorithmic
+    N reals + (N/2 + 1) complex per line and direction. The reference has no real transform, so
+    there is no CPU row."""
+    import numpy as np
+    rows = []
+    for row, n, batch, dbl in (("R: r2c+c2r f32 N=16384 x8192", 16384, 8192, False),
+                               ("R: r2c+c2r f32 N=26880 x4096", 26880, 4096, False),
+                               ("R: r2c+c2r f64 N=131072 x512", 131072, 512, True)):
+        if not row.startswith(prefix):
+            continue
+        rs, cs = (8, 16) if dbl else (4, 8)
+        h = n // 2 + 1
+        fl = 2 * 2.5 * n * math.log2(n) * batch
+        nbytes = 2 * (n * rs + h * cs) * batch
+        rng = np.random.default_rng(n)
+        x = rng.uniform(-1, 1, (batch, n)).astype(np.float64 if dbl else np.float32)
+        scalar = "double" if dbl else "float"
+        opts = sf.plan_options(normalization=sf.normalization.backward)
+        f = sf.plan_dft_r2c_1d(scalar, n, batch, opts)
+        b = sf.plan_dft_c2r_1d(scalar, n, batch, opts)
+        a = torch.from_numpy(x).to(dev)
+        spec = torch.empty(batch * h, dtype=f.dtype, device=dev)
+        back = torch.empty_like(a)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+
+        def step():
+            f.execute(a, spec, stream=s)
+            b.execute(spec, back, stream=s)
+
+        out = {"row": row}
+        with torch.cuda.stream(s):
+            step()
+        torch.cuda.synchronize()
+        lines = min(batch, 8)
+        ref = np.fft.rfft(x[:lines].astype(np.float64), axis=1)
+        got = spec[: lines * h].cpu().numpy().reshape(lines, h)
+        d = got - ref
+        out["rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(ref))
+        out["max_rel"] = float(np.abs(d).max() / np.abs(ref).max())
+        out["round_trip_rel_l2"] = float(torch.linalg.vector_norm(back - a) / torch.linalg.vector_norm(a))
+        with torch.cuda.stream(s):
+            ms = timed(step)
+        out["P"] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1), "gbs": round(nbytes / ms / 1e6, 1),
+                    "frac": round(nbytes / ms / 1e6 / peak, 4), "launches": f.launches() + b.launches()}
+
+        def cufft():
+            y = torch.fft.rfft(a, dim=1, norm="backward")
+            torch.fft.irfft(y, n=n, dim=1, norm="backward")
+
+        ms = timed(cufft)
+        out["C_torch_cufft"] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1)}
+        out["CPU"] = None
+        rows.append(out)
+        print(json.dumps(out), file=sys.stderr, flush=True)
+        del f, b, a, spec, back
+    return rows
 
 
 def run_serve(args):
@@ -771,6 +835,7 @@ def main():
                     help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
     ap.add_argument("--table", action="store_true", help="every configuration's rows (BASELINE.md)")
+    ap.add_argument("--table-rows", default="", help="with --table: only the rows whose name starts with this")
     ap.add_argument("--config", type=int, choices=[3, 4], default=0,
                     help="run a secondary configuration instead (3: Bluestein primes, 4: 3D/2D)")
     ap.add_argument("--requests", type=int, default=20000)

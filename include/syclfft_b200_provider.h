@@ -110,6 +110,17 @@ SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
 #define SYCLFFT_B200_CREATE_SPLIT_BF16 4u
 SYCLFFT_B200_EXPORT void *syclfft_b200_create_ex(const syclfft_b200_plan_config_v1 *config, uint32_t flags, char *err,
                                                  size_t cap);
+/* Real transforms (no counterpart in the reference, whose v0.1 scope is complex-to-complex):
+ * one-dimensional batched, out of place, even length N = lengths[0]. R2C (direction -1):
+ * N reals per line in, N/2 + 1 complex per line out; C2R (direction +1): N/2 + 1 complex in
+ * (imaginary parts of the first and last bins ignored), N reals out. Computed as a complex
+ * FFT of length N/2 plus one post- / pre-process pass; normalization as for complex plans,
+ * relative to N. The handle is used with the provider's execute/destroy, execute_batch and
+ * execute_ex (normalization only), describe_plan and plan_launches. */
+#define SYCLFFT_B200_REAL_R2C 1
+#define SYCLFFT_B200_REAL_C2R 2
+SYCLFFT_B200_EXPORT void *syclfft_b200_create_real(const syclfft_b200_plan_config_v1 *config, int32_t kind,
+                                                   uint32_t flags, char *err, size_t cap);
 /* Like execute, for the first `batch` transforms only (1 <= batch <= the plan's
  * batch_count): a plan made for up to B transforms serves any smaller batch with the same
  * resident tables and scratch. */

@@ -29,6 +29,7 @@
 #include "piped_launch.hpp"
 #include "tc_launch.hpp"
 #include "tma_launch.hpp"
+#include "real_launch.hpp"
 #include "bluestein_launch.hpp"
 #include "planner.hpp"
 
@@ -189,6 +190,13 @@ struct DevicePlan {
     cudaEvent_t ready = nullptr;  // tables complete (recorded on the memory stream at creation)
     bool stream_scratch = false;  // scratch comes from the executing stream's arena
     std::mutex mu;
+    // Real transforms (syclfft_b200_create_real): a complex plan of half the length, with the
+    // post-process (R2C) or pre-process (C2R) of real_kernel.cu around it.
+    int real_kind = 0;              // 0 complex, 1 R2C, 2 C2R
+    int64_t real_n = 0;             // real length N (even)
+    std::unique_ptr<DevicePlan> inner;
+    void* real_buf = nullptr;       // half-length spectra: batch x N/2 complex
+    void* real_tw = nullptr;        // W_N^k, k = 0..N/2
 
     ~DevicePlan() {
         int prev = 0;
@@ -203,10 +211,14 @@ struct DevicePlan {
             if (done) cudaStreamWaitEvent(ms, done, 0);
             if (scratch) cudaFreeAsync(scratch, ms);
             if (table_mem) cudaFreeAsync(table_mem, ms);
+            if (real_buf) cudaFreeAsync(real_buf, ms);
+            if (real_tw) cudaFreeAsync(real_tw, ms);
         } else {
             if (done) cudaEventSynchronize(done);
             if (scratch) cudaFree(scratch);
             if (table_mem) cudaFree(table_mem);
+            if (real_buf) cudaFree(real_buf);
+            if (real_tw) cudaFree(real_tw);
         }
         if (done) cudaEventDestroy(done);
         if (ready) cudaEventDestroy(ready);
@@ -466,6 +478,90 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
     }
 }
 
+// Real transform of even length N over a complex plan of length N/2 (see real_kernel.cu).
+DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, uint32_t flags) {
+    if (kind != SYCLFFT_B200_REAL_R2C && kind != SYCLFFT_B200_REAL_C2R)
+        throw std::invalid_argument("real transform kind must be R2C or C2R");
+    if (cfg.rank != 1) throw std::invalid_argument("real transforms are one-dimensional (batched)");
+    const uint64_t n = cfg.lengths[0];
+    if (n < 2 || n % 2) throw std::invalid_argument("real transforms need an even length >= 2");
+    if (cfg.in_place) throw std::invalid_argument("real transforms are out of place");
+    const int dir = kind == SYCLFFT_B200_REAL_R2C ? -1 : 1;
+    if (cfg.direction != dir)
+        throw std::invalid_argument(dir < 0 ? "R2C transforms are forward" : "C2R transforms are backward");
+    if (cfg.normalization > 3) throw std::invalid_argument("Invalid normalization");
+    syclfft_b200_plan_config_v1 ic = cfg;
+    ic.lengths[0] = n / 2;
+    ic.in_place = 0;
+    ic.normalization = 0;
+    std::unique_ptr<DevicePlan> inner(create_plan(ic, flags | SYCLFFT_B200_CREATE_SYNC));
+    auto plan = std::make_unique<DevicePlan>();
+    plan->device = inner->device;
+    plan->sms = inner->sms;
+    plan->spec.req = inner->spec.req;
+    plan->spec.req.shape = {n};
+    plan->spec.req.direction = dir;
+    plan->spec.req.normalization = static_cast<int>(cfg.normalization);
+    plan->spec.transform_size = n;
+    plan->spec.elements = n * cfg.batch_count;
+    plan->status = inner->status;
+    plan->real_kind = kind;
+    plan->real_n = static_cast<int64_t>(n);
+    const bool dbl = plan->spec.req.dbl;
+    const size_t cs = dbl ? 16 : 8;
+    const uint64_t h = n / 2;
+    plan->spec.scratch_elements = inner->spec.scratch_elements + h * cfg.batch_count;
+    DeviceGuard guard(plan->device);
+    cudaStream_t ms = memory_stream(plan->device);
+    std::vector<unsigned char> tw((h + 1) * cs);
+    for (uint64_t k = 0; k <= h; ++k) {
+        const std::complex<double> w = cis_neg(static_cast<int64_t>(k), static_cast<int64_t>(n));
+        if (dbl) {
+            reinterpret_cast<double*>(tw.data())[2 * k] = w.real();
+            reinterpret_cast<double*>(tw.data())[2 * k + 1] = w.imag();
+        } else {
+            reinterpret_cast<float*>(tw.data())[2 * k] = static_cast<float>(w.real());
+            reinterpret_cast<float*>(tw.data())[2 * k + 1] = static_cast<float>(w.imag());
+        }
+    }
+    check(cudaMallocAsync(&plan->real_tw, tw.size(), ms), "cudaMallocAsync(real twiddles)");
+    check(cudaMemcpyAsync(plan->real_tw, tw.data(), tw.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(real twiddles)");
+    check(cudaMallocAsync(&plan->real_buf, h * cfg.batch_count * cs, ms), "cudaMallocAsync(real spectra)");
+    check(cudaStreamSynchronize(ms), "real plan tables");
+    check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+    plan->inner = std::move(inner);
+    return plan.release();
+}
+
+void execute_real(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch, int direction,
+                  int normalization) {
+    const uint64_t planned = plan->spec.req.batch;
+    if (batch == 0) batch = planned;
+    if (batch > planned) throw std::invalid_argument("batch exceeds the plan's batch count");
+    if (in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
+    const int dir = plan->spec.req.direction;
+    if (direction != 0 && direction != dir) throw std::invalid_argument("a real plan runs in its own direction");
+    const int norm = normalization < 0 ? plan->spec.req.normalization : normalization;
+    const double scale = normalization_scale(norm, dir, plan->spec.transform_size);
+    std::lock_guard<std::mutex> lock(plan->mu);
+    DeviceGuard guard(plan->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+    const bool dbl = plan->spec.req.dbl;
+    const int64_t h = plan->real_n / 2;
+    const int64_t lines = static_cast<int64_t>(batch);
+    if (plan->real_kind == SYCLFFT_B200_REAL_R2C) {
+        execute_plan(plan->inner.get(), in, plan->real_buf, stream, batch, 0, -1);
+        check(launch_r2c_post(dbl, plan->real_buf, out, h, lines, plan->real_tw, scale, stream), "R2C post-process");
+    } else {
+        check(launch_c2r_pre(dbl, in, plan->real_buf, h, lines, plan->real_tw, scale, stream), "C2R pre-process");
+        execute_plan(plan->inner.get(), plan->real_buf, out, stream, batch, 0, -1);
+    }
+    check(cap != cudaStreamCaptureStatusNone ? cudaEventRecordWithFlags(plan->done, stream, cudaEventRecordExternal)
+                                             : cudaEventRecord(plan->done, stream),
+          "cudaEventRecord");
+}
+
 // TMA-staged four-step column pass; false when the tensor map cannot describe the buffer
 // (the caller then runs the plain size-specialised kernel).
 bool launch_tma(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cudaStream_t stream) {
@@ -523,6 +619,10 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
 void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch,
                   int direction, int normalization) {
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
+    if (plan->real_kind) {
+        execute_real(plan, in, out, stream, batch, direction, normalization);
+        return;
+    }
     const uint64_t planned = plan->spec.req.batch;
     if (batch == 0) batch = planned;
     if (batch > planned) throw std::invalid_argument("batch exceeds the plan's batch count");
@@ -789,7 +889,14 @@ SYCLFFT_B200_EXPORT const syclfft_b200_provider_v1* syclfft_b200_get_provider_v1
 SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, size_t cap) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
     if (!p || !buf || cap == 0) return -1;
-    const std::string s = sfb::describe_plan(p->spec);
+    std::string s;
+    if (p->real_kind) {
+        // a real plan: its complex plan of half the length and the pre-/post-process pass
+        s = std::string("{\"real\":\"") + (p->real_kind == SYCLFFT_B200_REAL_R2C ? "r2c" : "c2r") +
+            "\",\"n\":" + std::to_string(p->real_n) + ",\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
+    } else {
+        s = sfb::describe_plan(p->spec);
+    }
     if (s.size() + 1 > cap) return -1;
     std::memcpy(buf, s.c_str(), s.size() + 1);
     return static_cast<int>(s.size());
@@ -797,6 +904,7 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
+    if (p && p->real_kind) return static_cast<int>(p->inner->passes.size()) + 1;
     return p ? static_cast<int>(p->passes.size()) : -1;
 }
 
@@ -807,6 +915,17 @@ SYCLFFT_B200_EXPORT void* syclfft_b200_create_ex(const syclfft_b200_plan_config_
     try {
         if (!cfg) throw std::invalid_argument("null plan configuration");
         return sfb::create_plan(*cfg, flags);
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return nullptr;
+    }
+}
+
+SYCLFFT_B200_EXPORT void* syclfft_b200_create_real(const syclfft_b200_plan_config_v1* cfg, int32_t kind, uint32_t flags,
+                                                   char* err, size_t cap) {
+    try {
+        if (!cfg) throw std::invalid_argument("null plan configuration");
+        return sfb::create_real_plan(*cfg, kind, flags);
     } catch (const std::exception& e) {
         sfb::set_error(err, cap, e.what());
         return nullptr;

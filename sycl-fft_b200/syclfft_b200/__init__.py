@@ -10,6 +10,7 @@ a CUDA event (the stand-in for sycl::event).
 """
 from .api import (  # noqa: F401
     Plan,
+    RealPlan,
     SyclfftError,
     direction,
     error_code,
@@ -18,6 +19,8 @@ from .api import (  # noqa: F401
     plan_dft_1d,
     plan_dft_2d,
     plan_dft_3d,
+    plan_dft_c2r_1d,
+    plan_dft_r2c_1d,
     plan_many_dft,
     plan_options,
     planning_mode,
@@ -27,7 +30,7 @@ from .api import (  # noqa: F401
 from . import _provider  # noqa: F401
 
 __all__ = [
-    "Plan", "SyclfftError", "direction", "error_code", "normalization", "placement", "plan_dft_1d",
-    "plan_dft_2d", "plan_dft_3d", "plan_many_dft", "plan_options", "planning_mode", "provider",
+    "Plan", "RealPlan", "SyclfftError", "direction", "error_code", "normalization", "placement", "plan_dft_1d",
+    "plan_dft_2d", "plan_dft_3d", "plan_dft_r2c_1d", "plan_dft_c2r_1d", "plan_many_dft", "plan_options", "planning_mode", "provider",
     "query_providers",
 ]

@@ -19,6 +19,8 @@ ABI_VERSION = 1
 CREATE_STREAM_SCRATCH = 1
 CREATE_SYNC = 2
 CREATE_SPLIT_BF16 = 4
+REAL_R2C = 1
+REAL_C2R = 2
 SCALAR_FLOAT = 1
 SCALAR_DOUBLE = 2
 ERR_CAP = 1024
@@ -84,6 +86,7 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_group_execute",
     "syclfft_b200_group_destroy",
     "syclfft_b200_execute_noalloc_c2c_f32",
+    "syclfft_b200_create_real",
 )
 
 _lib = None
@@ -128,6 +131,9 @@ def load(path: str | None = None):
                                                ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
     lib.syclfft_b200_group_destroy.restype = None
     lib.syclfft_b200_group_destroy.argtypes = [ctypes.c_void_p]
+    lib.syclfft_b200_create_real.restype = ctypes.c_void_p
+    lib.syclfft_b200_create_real.argtypes = [ctypes.POINTER(PlanConfigV1), ctypes.c_int32, ctypes.c_uint32,
+                                             ctypes.c_char_p, ctypes.c_size_t]
     lib.syclfft_b200_execute_noalloc_c2c_f32.restype = ctypes.c_int
     lib.syclfft_b200_execute_noalloc_c2c_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                          ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32,

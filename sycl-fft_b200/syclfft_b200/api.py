@@ -264,6 +264,114 @@ class Plan:
             pass
 
 
+class RealPlan(Plan):
+    """Batched one-dimensional real transform of even length n (B200 extension; the reference's
+    plan API is complex-to-complex only). kind "r2c": forward, n reals per line in, n/2 + 1
+    complex per line out. kind "c2r": backward, n/2 + 1 complex per line in (imaginary parts of
+    bins 0 and n/2 ignored, as numpy.fft.irfft does), n reals out. Out of place only; the
+    normalization option scales relative to n exactly as for a complex plan of length n.
+    Buffers are float32/float64 and complex64/complex128 tensors (or raw device pointers)."""
+
+    def __init__(self, scalar: str, n: int, batch_count: int, kind: str, options: plan_options | None = None,
+                 device: int | None = None):
+        options = options or plan_options()
+        if scalar not in ("float", "double"):
+            raise SyclfftError(error_code.unsupported_precision, "syclfft supports float and double precision")
+        if kind not in ("r2c", "c2r"):
+            raise SyclfftError(error_code.invalid_argument, "real transform kind must be 'r2c' or 'c2r'")
+        n = int(n)
+        self._lengths = [n]
+        self._batch = int(batch_count)
+        self._elements = _checked_element_count(self._lengths, self._batch)
+        if n % 2:
+            raise SyclfftError(error_code.invalid_argument, "real transforms need an even length")
+        if options.placement != placement.out_of_place:
+            raise SyclfftError(error_code.invalid_argument, "real transforms are out of place")
+        self._kind = kind
+        self._direction = direction.forward if kind == "r2c" else direction.backward
+        self._options = options
+        self._double = scalar == "double"
+        if options.preferred_provider not in (provider.automatic, provider.b200):
+            raise SyclfftError(error_code.provider_unavailable,
+                               f"{provider(options.preferred_provider).name} provider is not part of this build")
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise SyclfftError(error_code.provider_unavailable, "no CUDA device is available")
+        self._device = torch.cuda.current_device() if device is None else int(device)
+        try:
+            self._lib = _provider.load()
+        except OSError as e:
+            raise SyclfftError(error_code.provider_unavailable, str(e)) from None
+        self._api = _provider.provider(self._lib)
+        err = ctypes.create_string_buffer(_provider.ERR_CAP)
+        if not self._api.supports(self._device, err, _provider.ERR_CAP):
+            raise SyclfftError(error_code.provider_unavailable, err.value.decode() or "device not supported")
+        cfg = _provider.make_config(self._lengths, self._batch, int(self._direction), self._double, False,
+                                    int(options.normalization), options.planning == planning_mode.measure,
+                                    self._device)
+        self._cfg = cfg
+        flags = _provider.CREATE_SYNC
+        if options.split_precision and not self._double:
+            flags |= _provider.CREATE_SPLIT_BF16
+        h = self._lib.syclfft_b200_create_real(ctypes.byref(cfg), _provider.REAL_R2C if kind == "r2c"
+                                               else _provider.REAL_C2R, flags, err, _provider.ERR_CAP)
+        if not h:
+            raise SyclfftError(error_code.planning_failed, err.value.decode() or "B200 plan creation failed")
+        self._handle = h
+        self._lock = threading.Lock()
+        self._last_event = None
+
+    @property
+    def kind(self):
+        return self._kind
+
+    @property
+    def real_dtype(self):
+        return _torch().float64 if self._double else _torch().float32
+
+    def _layout(self, name):
+        """(dtype, elements) of the input or output buffer."""
+        n, b = self._lengths[0], self._batch
+        real = (self.real_dtype, n * b)
+        spec = (self.dtype, (n // 2 + 1) * b)
+        if self._kind == "r2c":
+            return real if name == "input" else spec
+        return spec if name == "input" else real
+
+    def _pointer(self, t, name):
+        torch = _torch()
+        if t is None or (isinstance(t, int) and t == 0):
+            raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
+        if isinstance(t, int):
+            return t
+        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} is not a device allocation in the plan context")
+        if t.device.index != self._device:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
+        dtype, count = self._layout(name)
+        if t.dtype != dtype:
+            raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {dtype}")
+        if not t.is_contiguous() or t.numel() < count:
+            raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {count} elements")
+        return t.data_ptr()
+
+    def move(self) -> "RealPlan":
+        other = object.__new__(RealPlan)
+        other.__dict__.update(self.__dict__)
+        self._handle = None
+        return other
+
+
+def plan_dft_r2c_1d(scalar, n, batch_count=1, options=None, device=None) -> RealPlan:
+    """Forward real-to-complex transform(s) of length n: n reals -> n/2 + 1 complex per line."""
+    return RealPlan(scalar, n, batch_count, "r2c", options, device)
+
+
+def plan_dft_c2r_1d(scalar, n, batch_count=1, options=None, device=None) -> RealPlan:
+    """Backward complex-to-real transform(s) of length n: n/2 + 1 complex -> n reals per line."""
+    return RealPlan(scalar, n, batch_count, "c2r", options, device)
+
+
 def plan_many_dft(scalar, lengths, batch_count, dir, options=None, device=None) -> Plan:
     return Plan(scalar, lengths, batch_count, dir, options, device)
 

@@ -714,6 +714,7 @@ def run_table(args):
         rows.append(out)
         print(json.dumps(out), file=sys.stderr, flush=True)
     rows.extend(_real_rows(sf, torch, dev, peak, timed, args.table_rows))
+    rows.extend(_layout_rows(sf, torch, dev, peak, timed, args.table_rows))
     torch.cuda.empty_cache()
     print(json.dumps({"metric": "per-configuration rows (P, A, C, CPU) and accuracy", "cpu_threads": threads,
                       "peak_gbs": peak, "rows": rows}), flush=True)
@@ -778,6 +779,53 @@ def _real_rows(sf, torch, dev, peak, timed, prefix=""):
         rows.append(out)
         print(json.dumps(out), file=sys.stderr, flush=True)
         del f, b, a, spec, back
+    return rows
+
+
+def _layout_rows(sf, torch, dev, peak, timed, prefix=""):
+    """Strided layouts: transforms down the columns of a row-major matrix (input stride = row
+    length, distance 1), written as contiguous rows or back into the columns in place. P = the
+    provider's strided plan; C = torch.fft.fft along dim 0 (cuFFT's strided plan). Bytes are the
+    algorithmic 2 E cs."""
+    import numpy as np
+    rows = []
+    for row, n, cols, ip in (("S: c64 4096-pt columns of 4096x16384 -> rows", 4096, 16384, False),
+                             ("S: c64 4096-pt columns of 4096x16384 in place", 4096, 16384, True),
+                             ("S: c64 1024-pt columns of 1024x65536 -> rows", 1024, 65536, False)):
+        if not row.startswith(prefix):
+            continue
+        fl = 5 * n * math.log2(n) * cols
+        nbytes = 2 * n * cols * 8
+        lay = sf.data_layout((cols,), 1, (cols,) if ip else (1,), 1 if ip else n)
+        opts = sf.plan_options(placement=sf.placement.in_place if ip else sf.placement.out_of_place)
+        p = sf.plan_many_dft("float", [n], cols, sf.direction.forward, opts, layout=lay)
+        g = torch.Generator(device=dev)
+        g.manual_seed(n)
+        a = torch.randn(n * cols, dtype=torch.complex64, device=dev, generator=g)
+        keep = a.clone()
+        o = None if ip else torch.empty_like(a)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        out = {"row": row}
+        with torch.cuda.stream(s):
+            p.execute(a) if ip else p.execute(a, o)
+        torch.cuda.synchronize()
+        res = (a.view(n, cols).t() if ip else o.view(cols, n))[:8].cpu().numpy()
+        ref = np.fft.fft(keep.view(n, cols)[:, :8].cpu().numpy().astype(np.complex128), axis=0).T
+        d = res - ref
+        out["rel_l2"] = float(np.linalg.norm(d) / np.linalg.norm(ref))
+        out["max_rel"] = float(np.abs(d).max() / np.abs(ref).max())
+        with torch.cuda.stream(s):
+            ms = timed(lambda: p.execute(a) if ip else p.execute(a, o))
+        out["P"] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1), "gbs": round(nbytes / ms / 1e6, 1),
+                    "frac": round(nbytes / ms / 1e6 / peak, 4), "launches": p.launches()}
+        xm = keep.view(n, cols)
+        ms = timed(lambda: torch.fft.fft(xm, dim=0))
+        out["C_torch_cufft"] = {"ms": round(ms, 4), "gflops": round(fl / ms / 1e6, 1)}
+        out["CPU"] = None
+        rows.append(out)
+        print(json.dumps(out), file=sys.stderr, flush=True)
+        del p, a, keep, o
     return rows
 
 

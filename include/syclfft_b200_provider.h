@@ -121,6 +121,24 @@ SYCLFFT_B200_EXPORT void *syclfft_b200_create_ex(const syclfft_b200_plan_config_
 #define SYCLFFT_B200_REAL_C2R 2
 SYCLFFT_B200_EXPORT void *syclfft_b200_create_real(const syclfft_b200_plan_config_v1 *config, int32_t kind,
                                                    uint32_t flags, char *err, size_t cap);
+/* Strided ("advanced") layouts (no counterpart in the reference, whose v0.1 scope is contiguous
+ * batches): element (b, i0, .., i_{rank-1}) of the input is read at
+ * b * in_distance + sum_k i_k * in_strides[k] complex elements from the input pointer, and the
+ * output written at the same formula with the out_ fields. Strides >= 1; distances >= 1 when
+ * batch_count > 1; the output layout must not overlap itself; an in-place plan needs equal
+ * input and output layouts. A side that is already contiguous and batch-major is read or
+ * written directly; a strided side is gathered into / scattered from the plan's scratch by a
+ * tiled pass. Used with execute/destroy, execute_batch, execute_ex, describe_plan and
+ * plan_launches like any plan. */
+typedef struct syclfft_b200_layout_v1 {
+    int64_t in_strides[3];
+    int64_t in_distance;
+    int64_t out_strides[3];
+    int64_t out_distance;
+} syclfft_b200_layout_v1;
+SYCLFFT_B200_EXPORT void *syclfft_b200_create_strided(const syclfft_b200_plan_config_v1 *config,
+                                                      const syclfft_b200_layout_v1 *layout, uint32_t flags,
+                                                      char *err, size_t cap);
 /* Like execute, for the first `batch` transforms only (1 <= batch <= the plan's
  * batch_count): a plan made for up to B transforms serves any smaller batch with the same
  * resident tables and scratch. */

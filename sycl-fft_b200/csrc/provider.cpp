@@ -30,6 +30,7 @@
 #include "tc_launch.hpp"
 #include "tma_launch.hpp"
 #include "real_launch.hpp"
+#include "layout_launch.hpp"
 #include "bluestein_launch.hpp"
 #include "planner.hpp"
 
@@ -197,6 +198,12 @@ struct DevicePlan {
     std::unique_ptr<DevicePlan> inner;
     void* real_buf = nullptr;       // half-length spectra: batch x N/2 complex
     void* real_tw = nullptr;        // W_N^k, k = 0..N/2
+    // Strided layouts (syclfft_b200_create_strided): the contiguous plan `inner` with gather /
+    // scatter passes (layout_kernel.cu) on the sides that are not contiguous.
+    bool strided = false;
+    Layout in_layout, out_layout;
+    bool in_contig = true, out_contig = true;
+    void* pack_buf = nullptr;       // contiguous batch x prod(L) complex
 
     ~DevicePlan() {
         int prev = 0;
@@ -213,12 +220,14 @@ struct DevicePlan {
             if (table_mem) cudaFreeAsync(table_mem, ms);
             if (real_buf) cudaFreeAsync(real_buf, ms);
             if (real_tw) cudaFreeAsync(real_tw, ms);
+            if (pack_buf) cudaFreeAsync(pack_buf, ms);
         } else {
             if (done) cudaEventSynchronize(done);
             if (scratch) cudaFree(scratch);
             if (table_mem) cudaFree(table_mem);
             if (real_buf) cudaFree(real_buf);
             if (real_tw) cudaFree(real_tw);
+            if (pack_buf) cudaFree(pack_buf);
         }
         if (done) cudaEventDestroy(done);
         if (ready) cudaEventDestroy(ready);
@@ -533,6 +542,132 @@ DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, u
     return plan.release();
 }
 
+Layout make_layout(const syclfft_b200_plan_config_v1& cfg, const int64_t* strides, int64_t dist) {
+    Layout l;
+    l.rank = static_cast<int>(cfg.rank);
+    for (int k = 0; k < l.rank; ++k) {
+        l.len[k] = static_cast<int64_t>(cfg.lengths[k]);
+        l.stride[k] = strides[k];
+    }
+    l.dist = dist;
+    l.batch = static_cast<int64_t>(cfg.batch_count);
+    return l;
+}
+
+bool layout_contiguous(const Layout& l) {
+    int64_t step = 1;
+    for (int k = l.rank - 1; k >= 0; --k) {
+        if (l.len[k] > 1 && l.stride[k] != step) return false;
+        step *= l.len[k];
+    }
+    return l.batch == 1 || l.dist == step;
+}
+
+bool layout_same(const Layout& a, const Layout& b) {
+    for (int k = 0; k < a.rank; ++k)
+        if (a.len[k] > 1 && a.stride[k] != b.stride[k]) return false;
+    return a.batch == 1 || a.dist == b.dist;
+}
+
+// Checks strides and distances; for the output side also that no two elements share an address
+// (sufficient test: sorted by stride, each stride exceeds the span of the smaller ones).
+void check_layout(const Layout& l, bool output) {
+    const char* side = output ? "output" : "input";
+    std::vector<std::pair<int64_t, int64_t>> dims;  // (stride, extent)
+    for (int k = 0; k < l.rank; ++k) {
+        if (l.stride[k] < 1) throw std::invalid_argument(std::string(side) + " strides must be >= 1");
+        if (l.len[k] > 1) dims.push_back({l.stride[k], l.len[k]});
+    }
+    if (l.batch > 1) {
+        if (l.dist < 1) throw std::invalid_argument(std::string(side) + " distance must be >= 1");
+        dims.push_back({l.dist, l.batch});
+    }
+    long double span = 0;  // largest offset, in long double so huge strides cannot wrap
+    for (auto& d : dims) span += static_cast<long double>(d.first) * static_cast<long double>(d.second - 1);
+    if (span >= static_cast<long double>(INT64_MAX / 16))
+        throw std::invalid_argument(std::string(side) + " layout exceeds the addressable range");
+    if (!output) return;
+    std::sort(dims.begin(), dims.end());
+    int64_t reach = 0;  // largest offset reachable by the dimensions so far
+    for (auto& d : dims) {
+        if (d.first <= reach) throw std::invalid_argument("output layout overlaps itself");
+        reach += d.first * (d.second - 1);
+    }
+}
+
+DevicePlan* create_strided_plan(const syclfft_b200_plan_config_v1& cfg, const syclfft_b200_layout_v1& lay,
+                                uint32_t flags) {
+    if (cfg.rank == 0 || cfg.rank > 3) throw std::invalid_argument("FFT rank must be between 1 and 3");
+    for (uint32_t k = 0; k < cfg.rank; ++k)
+        if (cfg.lengths[k] == 0) throw std::invalid_argument("FFT dimensions must be non-zero");
+    if (cfg.batch_count == 0) throw std::invalid_argument("FFT batch count must be non-zero");
+    const Layout in = make_layout(cfg, lay.in_strides, lay.in_distance);
+    const Layout out = make_layout(cfg, lay.out_strides, lay.out_distance);
+    check_layout(in, false);
+    check_layout(out, true);
+    if (cfg.in_place && !layout_same(in, out))
+        throw std::invalid_argument("an in-place plan needs equal input and output layouts");
+    const bool ic = layout_contiguous(in), oc = layout_contiguous(out);
+    if (ic && oc) return create_plan(cfg, flags);
+    syclfft_b200_plan_config_v1 c = cfg;
+    c.in_place = (!ic && !oc) ? 1 : 0;  // both strided: transform the gathered copy in place
+    std::unique_ptr<DevicePlan> inner(create_plan(c, flags | SYCLFFT_B200_CREATE_SYNC));
+    auto plan = std::make_unique<DevicePlan>();
+    plan->device = inner->device;
+    plan->sms = inner->sms;
+    plan->spec.req = inner->spec.req;
+    plan->spec.req.in_place = cfg.in_place != 0;
+    plan->spec.transform_size = inner->spec.transform_size;
+    plan->spec.elements = inner->spec.elements;
+    plan->status = inner->status;
+    plan->strided = true;
+    plan->in_layout = in;
+    plan->out_layout = out;
+    plan->in_contig = ic;
+    plan->out_contig = oc;
+    const size_t cs = plan->spec.req.dbl ? 16 : 8;
+    plan->spec.scratch_elements = inner->spec.scratch_elements + inner->spec.elements;
+    DeviceGuard guard(plan->device);
+    cudaStream_t ms = memory_stream(plan->device);
+    check(cudaMallocAsync(&plan->pack_buf, inner->spec.elements * cs, ms), "cudaMallocAsync(layout scratch)");
+    check(cudaStreamSynchronize(ms), "layout scratch");
+    check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+    plan->inner = std::move(inner);
+    return plan.release();
+}
+
+void execute_strided(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch, int direction,
+                     int normalization) {
+    const uint64_t planned = plan->spec.req.batch;
+    if (batch == 0) batch = planned;
+    if (batch > planned) throw std::invalid_argument("batch exceeds the plan's batch count");
+    if (plan->spec.req.in_place ? in != out : in == out)
+        throw std::invalid_argument(plan->spec.req.in_place ? "In-place plan must be executed with execute(inout)"
+                                                            : "Out-of-place plan requires distinct allocations");
+    std::lock_guard<std::mutex> lock(plan->mu);
+    DeviceGuard guard(plan->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+    const bool dbl = plan->spec.req.dbl;
+    Layout li = plan->in_layout, lo = plan->out_layout;
+    li.batch = lo.batch = static_cast<int64_t>(batch);
+    DevicePlan* inner = plan->inner.get();
+    if (!plan->in_contig && !plan->out_contig) {
+        check(launch_layout_gather(dbl, in, li, plan->pack_buf, stream), "layout gather");
+        execute_plan(inner, plan->pack_buf, plan->pack_buf, stream, batch, direction, normalization);
+        check(launch_layout_scatter(dbl, plan->pack_buf, out, lo, stream), "layout scatter");
+    } else if (!plan->in_contig) {
+        check(launch_layout_gather(dbl, in, li, plan->pack_buf, stream), "layout gather");
+        execute_plan(inner, plan->pack_buf, out, stream, batch, direction, normalization);
+    } else {
+        execute_plan(inner, in, plan->pack_buf, stream, batch, direction, normalization);
+        check(launch_layout_scatter(dbl, plan->pack_buf, out, lo, stream), "layout scatter");
+    }
+    check(cap != cudaStreamCaptureStatusNone ? cudaEventRecordWithFlags(plan->done, stream, cudaEventRecordExternal)
+                                             : cudaEventRecord(plan->done, stream),
+          "cudaEventRecord");
+}
+
 void execute_real(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch, int direction,
                   int normalization) {
     const uint64_t planned = plan->spec.req.batch;
@@ -621,6 +756,10 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
     if (plan->real_kind) {
         execute_real(plan, in, out, stream, batch, direction, normalization);
+        return;
+    }
+    if (plan->strided) {
+        execute_strided(plan, in, out, stream, batch, direction, normalization);
         return;
     }
     const uint64_t planned = plan->spec.req.batch;
@@ -894,6 +1033,14 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
         // a real plan: its complex plan of half the length and the pre-/post-process pass
         s = std::string("{\"real\":\"") + (p->real_kind == SYCLFFT_B200_REAL_R2C ? "r2c" : "c2r") +
             "\",\"n\":" + std::to_string(p->real_n) + ",\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
+    } else if (p->strided) {
+        auto side = [](const sfb::Layout& l, bool contig) {
+            std::string r = "{\"strides\":[";
+            for (int k = 0; k < l.rank; ++k) r += (k ? "," : "") + std::to_string(l.stride[k]);
+            return r + "],\"distance\":" + std::to_string(l.dist) + ",\"contiguous\":" + (contig ? "1" : "0") + "}";
+        };
+        s = "{\"layout\":{\"in\":" + side(p->in_layout, p->in_contig) + ",\"out\":" +
+            side(p->out_layout, p->out_contig) + "},\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
     } else {
         s = sfb::describe_plan(p->spec);
     }
@@ -905,6 +1052,8 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
     if (p && p->real_kind) return static_cast<int>(p->inner->passes.size()) + 1;
+    if (p && p->strided)
+        return static_cast<int>(p->inner->passes.size()) + (p->in_contig ? 0 : 1) + (p->out_contig ? 0 : 1);
     return p ? static_cast<int>(p->passes.size()) : -1;
 }
 
@@ -926,6 +1075,18 @@ SYCLFFT_B200_EXPORT void* syclfft_b200_create_real(const syclfft_b200_plan_confi
     try {
         if (!cfg) throw std::invalid_argument("null plan configuration");
         return sfb::create_real_plan(*cfg, kind, flags);
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return nullptr;
+    }
+}
+
+SYCLFFT_B200_EXPORT void* syclfft_b200_create_strided(const syclfft_b200_plan_config_v1* cfg,
+                                                      const syclfft_b200_layout_v1* layout, uint32_t flags, char* err,
+                                                      size_t cap) {
+    try {
+        if (!cfg || !layout) throw std::invalid_argument("null plan configuration or layout");
+        return sfb::create_strided_plan(*cfg, *layout, flags);
     } catch (const std::exception& e) {
         sfb::set_error(err, cap, e.what());
         return nullptr;

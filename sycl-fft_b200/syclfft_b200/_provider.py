@@ -49,6 +49,15 @@ _EXECUTE = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctyp
 _SCRATCH = ctypes.CFUNCTYPE(ctypes.c_uint64, ctypes.c_void_p)
 
 
+class LayoutV1(ctypes.Structure):
+    _fields_ = [
+        ("in_strides", ctypes.c_int64 * 3),
+        ("in_distance", ctypes.c_int64),
+        ("out_strides", ctypes.c_int64 * 3),
+        ("out_distance", ctypes.c_int64),
+    ]
+
+
 class GroupItemV1(ctypes.Structure):
     _fields_ = [
         ("in_", ctypes.c_void_p),
@@ -87,6 +96,7 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_group_destroy",
     "syclfft_b200_execute_noalloc_c2c_f32",
     "syclfft_b200_create_real",
+    "syclfft_b200_create_strided",
 )
 
 _lib = None
@@ -134,6 +144,9 @@ def load(path: str | None = None):
     lib.syclfft_b200_create_real.restype = ctypes.c_void_p
     lib.syclfft_b200_create_real.argtypes = [ctypes.POINTER(PlanConfigV1), ctypes.c_int32, ctypes.c_uint32,
                                              ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_create_strided.restype = ctypes.c_void_p
+    lib.syclfft_b200_create_strided.argtypes = [ctypes.POINTER(PlanConfigV1), ctypes.POINTER(LayoutV1), ctypes.c_uint32,
+                                                ctypes.c_char_p, ctypes.c_size_t]
     lib.syclfft_b200_execute_noalloc_c2c_f32.restype = ctypes.c_int
     lib.syclfft_b200_execute_noalloc_c2c_f32.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                                          ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32,

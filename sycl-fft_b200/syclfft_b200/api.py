@@ -84,6 +84,60 @@ class plan_options:
     split_precision: bool = False
 
 
+@dataclass
+class data_layout:
+    """B200 extension (the reference's plans read and write contiguous batch-major arrays only):
+    element (b, i0, .., i_{rank-1}) of the input sits at b * in_distance + sum_k i_k * in_strides[k]
+    complex elements from the input's start, and likewise for the output. FFTW's advanced
+    interface (istride/idist, ostride/odist) generalised to one stride per axis."""
+    in_strides: tuple
+    in_distance: int
+    out_strides: tuple
+    out_distance: int
+
+    @staticmethod
+    def contiguous(lengths):
+        strides, step = [], 1
+        for n in reversed([int(v) for v in lengths]):
+            strides.insert(0, step)
+            step *= n
+        return data_layout(tuple(strides), step, tuple(strides), step)
+
+    def _side(self, output):
+        return (tuple(int(v) for v in (self.out_strides if output else self.in_strides)),
+                int(self.out_distance if output else self.in_distance))
+
+    def extent(self, lengths, batch, output):
+        """Elements a buffer must hold for this side: 1 + the largest offset."""
+        strides, dist = self._side(output)
+        return 1 + sum((int(n) - 1) * s for n, s in zip(lengths, strides)) + (int(batch) - 1) * dist
+
+    def check(self, lengths, batch, in_place):
+        for output in (False, True):
+            strides, dist = self._side(output)
+            side = "output" if output else "input"
+            if len(strides) != len(lengths):
+                raise SyclfftError(error_code.invalid_argument, f"{side} layout needs one stride per axis")
+            if any(s < 1 for s in strides):
+                raise SyclfftError(error_code.invalid_argument, f"{side} strides must be >= 1")
+            if batch > 1 and dist < 1:
+                raise SyclfftError(error_code.invalid_argument, f"{side} distance must be >= 1")
+        # the output must not write two elements to one address: sorted by stride, each stride
+        # has to exceed the span of the smaller ones
+        strides, dist = self._side(True)
+        dims = sorted([(s, int(n)) for s, n in zip(strides, lengths) if int(n) > 1] +
+                      ([(dist, int(batch))] if batch > 1 else []))
+        reach = 0
+        for s, n in dims:
+            if s <= reach:
+                raise SyclfftError(error_code.invalid_argument, "output layout overlaps itself")
+            reach += s * (n - 1)
+        if in_place:
+            same = all(a == b for a, b, n in zip(self.in_strides, self.out_strides, lengths) if int(n) > 1)
+            if not same or (batch > 1 and self.in_distance != self.out_distance):
+                raise SyclfftError(error_code.invalid_argument, "an in-place plan needs equal input and output layouts")
+
+
 def _torch():
     import torch
     return torch
@@ -108,13 +162,18 @@ class Plan:
     """syclfft::plan<Scalar> over the B200 provider. `scalar` is "float" or "double"."""
 
     def __init__(self, scalar: str, lengths, batch_count: int, dir, options: plan_options | None = None,
-                 device: int | None = None):
+                 device: int | None = None, layout: data_layout | None = None):
         options = options or plan_options()
         if scalar not in ("float", "double"):
             raise SyclfftError(error_code.unsupported_precision, "syclfft supports float and double precision")
         self._lengths = [int(v) for v in lengths]
         self._batch = int(batch_count)
         self._elements = _checked_element_count(self._lengths, self._batch)
+        self._extent = {"input": self._elements, "output": self._elements}
+        if layout is not None:
+            layout.check(self._lengths, self._batch, options.placement == placement.in_place)
+            self._extent = {"input": layout.extent(self._lengths, self._batch, False),
+                            "output": layout.extent(self._lengths, self._batch, True)}
         try:
             self._direction = direction(int(dir))
         except ValueError:
@@ -142,9 +201,18 @@ class Plan:
                                     options.placement == placement.in_place, int(options.normalization),
                                     options.planning == planning_mode.measure, self._device)
         self._cfg = cfg
-        if options.split_precision and not self._double:
-            h = self._lib.syclfft_b200_create_ex(ctypes.byref(cfg), _provider.CREATE_SYNC | _provider.CREATE_SPLIT_BF16,
-                                                 err, _provider.ERR_CAP)
+        flags = _provider.CREATE_SYNC | (_provider.CREATE_SPLIT_BF16 if options.split_precision else 0)
+        if layout is not None:
+            lay = _provider.LayoutV1()
+            for k, v in enumerate(layout.in_strides):
+                lay.in_strides[k] = int(v)
+            for k, v in enumerate(layout.out_strides):
+                lay.out_strides[k] = int(v)
+            lay.in_distance, lay.out_distance = int(layout.in_distance), int(layout.out_distance)
+            h = self._lib.syclfft_b200_create_strided(ctypes.byref(cfg), ctypes.byref(lay), flags, err,
+                                                      _provider.ERR_CAP)
+        elif options.split_precision and not self._double:
+            h = self._lib.syclfft_b200_create_ex(ctypes.byref(cfg), flags, err, _provider.ERR_CAP)
         else:
             h = self._api.create(ctypes.byref(cfg), err, _provider.ERR_CAP)
         if not h:
@@ -202,8 +270,9 @@ class Plan:
             raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
         if t.dtype != self.dtype:
             raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {self.dtype}")
-        if not t.is_contiguous() or t.numel() < self._elements:
-            raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {self._elements} elements")
+        need = self._extent[name]
+        if not t.is_contiguous() or t.numel() < need:
+            raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {need} elements")
         return t.data_ptr()
 
     def execute(self, a, b=None, dependencies=None, stream=None):
@@ -372,8 +441,9 @@ def plan_dft_c2r_1d(scalar, n, batch_count=1, options=None, device=None) -> Real
     return RealPlan(scalar, n, batch_count, "c2r", options, device)
 
 
-def plan_many_dft(scalar, lengths, batch_count, dir, options=None, device=None) -> Plan:
-    return Plan(scalar, lengths, batch_count, dir, options, device)
+def plan_many_dft(scalar, lengths, batch_count, dir, options=None, device=None, layout=None) -> Plan:
+    """plan_many_dft (syclfft.hpp:90-130); `layout` (B200 extension) gives strided input/output."""
+    return Plan(scalar, lengths, batch_count, dir, options, device, layout)
 
 
 def plan_dft_1d(scalar, n, dir, options=None, device=None) -> Plan:

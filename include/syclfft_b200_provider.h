@@ -128,7 +128,10 @@ SYCLFFT_B200_EXPORT void *syclfft_b200_create_real(const syclfft_b200_plan_confi
  * batch_count > 1; the output layout must not overlap itself; an in-place plan needs equal
  * input and output layouts. A side that is already contiguous and batch-major is read or
  * written directly; a strided side is gathered into / scattered from the plan's scratch by a
- * tiled pass. Used with execute/destroy, execute_batch, execute_ex, describe_plan and
+ * tiled pass. When both sides hold the batch as the innermost index of a dense array
+ * (distance 1, stride of the last axis = batch_count: transforms down the columns of a
+ * row-major matrix), the axis passes run on that array directly and execute_batch must run
+ * the whole batch. Used with execute/destroy, execute_batch, execute_ex, describe_plan and
  * plan_launches like any plan. */
 typedef struct syclfft_b200_layout_v1 {
     int64_t in_strides[3];

@@ -1230,7 +1230,8 @@ PlanSpec make_plan(const PlanRequest& req) {
     plan.req = req;
     plan.elements = checked_element_count(req.shape, req.batch);
     plan.transform_size = 1;
-    for (auto v : req.shape) plan.transform_size *= v;
+    for (size_t ax = 0; ax < req.shape.size(); ++ax)
+        if (!((req.skip_axes >> ax) & 1u)) plan.transform_size *= req.shape[ax];
     plan.scale = normalization_scale(req.normalization, req.direction, plan.transform_size);
     if (plan.elements > (uint64_t(1) << 40)) throw std::invalid_argument("FFT too large for one device");
     Builder b{plan, req, req.dbl ? 16 : 8, req.smem_limit > 0 ? req.smem_limit : kSmemDefault, {}};
@@ -1239,7 +1240,7 @@ PlanSpec make_plan(const PlanRequest& req) {
     const int64_t E = static_cast<int64_t>(plan.elements);
     for (int ax = rank - 1; ax >= 0; --ax) {
         const int64_t L = static_cast<int64_t>(req.shape[ax]);
-        if (L == 1) continue;
+        if (L == 1 || ((req.skip_axes >> ax) & 1u)) continue;
         int64_t s = 1;
         for (int j = ax + 1; j < rank; ++j) s *= static_cast<int64_t>(req.shape[j]);
         b.axis(ax, L, s, E / (L * s), cur);

@@ -130,6 +130,9 @@ struct PlanRequest {
     // complex<float> only: run the radix-16 butterflies of eligible single-pass axes as BF16
     // hi/lo matrix products on the tensor cores (FP32 accumulation); other passes stay FP32
     bool split_bf16 = false;
+    // bit ax set: axis ax is an index of the batch, not transformed (interleaved-batch layouts:
+    // transforms down the columns of a dense array run as the other axes' passes alone)
+    uint32_t skip_axes = 0;
 };
 
 // A Bluestein axis whose chirp and chirp spectrum the provider generates on the device

@@ -203,6 +203,7 @@ struct DevicePlan {
     bool strided = false;
     Layout in_layout, out_layout;
     bool in_contig = true, out_contig = true;
+    bool interleaved = false;       // both sides the dense [L.., batch] array: `inner` runs on it directly
     void* pack_buf = nullptr;       // contiguous batch x prod(L) complex
 
     ~DevicePlan() {
@@ -270,7 +271,7 @@ void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned
     }
 }
 
-DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags = 0);
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags = 0, uint32_t skip_axes = 0);
 void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch = 0,
                   int direction = 0, int normalization = -1);
 
@@ -298,7 +299,7 @@ DevicePlan* spectrum_plan(int device, int64_t M) {
 DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::string& tuning);
 PlanRequest tune(const PlanRequest& req, int device, std::string* report);
 
-DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) {
+DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags, uint32_t skip_axes) {
     if (cfg.abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION) throw std::runtime_error("B200 provider ABI mismatch");
     if (cfg.scalar != SYCLFFT_B200_SCALAR_FLOAT && cfg.scalar != SYCLFFT_B200_SCALAR_DOUBLE)
         throw std::invalid_argument("unsupported scalar type");
@@ -311,6 +312,7 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags) 
     req.shape.assign(cfg.lengths, cfg.lengths + cfg.rank);
     req.batch = cfg.batch_count;
     req.split_bf16 = !req.dbl && (flags & SYCLFFT_B200_CREATE_SPLIT_BF16) != 0;
+    req.skip_axes = skip_axes;
     // SYCLFFT_B200_KERNELS=generic: plan every pass on the runtime-parameterised kernel
     // (used to test and compare it against the size-specialised kernels).
     if (const char* k = std::getenv("SYCLFFT_B200_KERNELS")) req.no_fixed = std::strcmp(k, "generic") == 0;
@@ -569,6 +571,17 @@ bool layout_same(const Layout& a, const Layout& b) {
     return a.batch == 1 || a.dist == b.dist;
 }
 
+// The batch is the innermost, unit-stride index and the axes are dense C order around it.
+bool layout_interleaved(const Layout& l) {
+    if (l.dist != 1) return false;
+    int64_t step = l.batch;
+    for (int k = l.rank - 1; k >= 0; --k) {
+        if (l.len[k] > 1 && l.stride[k] != step) return false;
+        step *= l.len[k];
+    }
+    return true;
+}
+
 // Checks strides and distances; for the output side also that no two elements share an address
 // (sufficient test: sorted by stride, each stride exceeds the span of the smaller ones).
 void check_layout(const Layout& l, bool output) {
@@ -609,6 +622,37 @@ DevicePlan* create_strided_plan(const syclfft_b200_plan_config_v1& cfg, const sy
         throw std::invalid_argument("an in-place plan needs equal input and output layouts");
     const bool ic = layout_contiguous(in), oc = layout_contiguous(out);
     if (ic && oc) return create_plan(cfg, flags);
+    if (cfg.rank < 3 && cfg.batch_count > 1 && layout_same(in, out) && layout_interleaved(in)) {
+        // The batch is the innermost index of a dense array [L.., batch]: plan that array with
+        // its last axis left untransformed, so the axis passes read and write it in place of a
+        // gather / scatter (transforms down the columns of a row-major matrix, FFTW's
+        // stride = batch, distance = 1).
+        syclfft_b200_plan_config_v1 c = cfg;
+        c.rank = cfg.rank + 1;
+        c.lengths[cfg.rank] = cfg.batch_count;
+        c.batch_count = 1;
+        std::unique_ptr<DevicePlan> inner(create_plan(c, flags | SYCLFFT_B200_CREATE_SYNC, 1u << cfg.rank));
+        auto plan = std::make_unique<DevicePlan>();
+        plan->device = inner->device;
+        plan->sms = inner->sms;
+        plan->spec.req = inner->spec.req;
+        plan->spec.req.shape.assign(cfg.lengths, cfg.lengths + cfg.rank);
+        plan->spec.req.batch = cfg.batch_count;
+        plan->spec.req.skip_axes = 0;
+        plan->spec.transform_size = inner->spec.transform_size;
+        plan->spec.elements = inner->spec.elements;
+        plan->spec.scratch_elements = inner->spec.scratch_elements;
+        plan->status = inner->status;
+        plan->strided = true;
+        plan->interleaved = true;
+        plan->in_layout = in;
+        plan->out_layout = out;
+        plan->in_contig = plan->out_contig = false;
+        DeviceGuard guard(plan->device);
+        check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+        plan->inner = std::move(inner);
+        return plan.release();
+    }
     syclfft_b200_plan_config_v1 c = cfg;
     c.in_place = (!ic && !oc) ? 1 : 0;  // both strided: transform the gathered copy in place
     std::unique_ptr<DevicePlan> inner(create_plan(c, flags | SYCLFFT_B200_CREATE_SYNC));
@@ -652,7 +696,11 @@ void execute_strided(DevicePlan* plan, const void* in, void* out, cudaStream_t s
     Layout li = plan->in_layout, lo = plan->out_layout;
     li.batch = lo.batch = static_cast<int64_t>(batch);
     DevicePlan* inner = plan->inner.get();
-    if (!plan->in_contig && !plan->out_contig) {
+    if (plan->interleaved) {
+        if (batch != planned)
+            throw std::invalid_argument("a plan over an interleaved batch (distance 1) runs its whole batch");
+        execute_plan(inner, in, out, stream, 0, direction, normalization);
+    } else if (!plan->in_contig && !plan->out_contig) {
         check(launch_layout_gather(dbl, in, li, plan->pack_buf, stream), "layout gather");
         execute_plan(inner, plan->pack_buf, plan->pack_buf, stream, batch, direction, normalization);
         check(launch_layout_scatter(dbl, plan->pack_buf, out, lo, stream), "layout scatter");
@@ -830,6 +878,7 @@ std::string tune_key(const PlanRequest& r, int device) {
     k << prop.name << "|" << (r.dbl ? "z" : (r.split_bf16 ? "c-tc" : "c")) << "|" << (r.in_place ? "ip" : "oop")
       << "|b" << r.batch;
     for (auto v : r.shape) k << "|" << v;
+    if (r.skip_axes) k << "|skip" << r.skip_axes;
     return k.str();
 }
 
@@ -1040,7 +1089,8 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
             return r + "],\"distance\":" + std::to_string(l.dist) + ",\"contiguous\":" + (contig ? "1" : "0") + "}";
         };
         s = "{\"layout\":{\"in\":" + side(p->in_layout, p->in_contig) + ",\"out\":" +
-            side(p->out_layout, p->out_contig) + "},\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
+            side(p->out_layout, p->out_contig) + ",\"interleaved\":" + (p->interleaved ? "1" : "0") +
+            "},\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
     } else {
         s = sfb::describe_plan(p->spec);
     }
@@ -1053,7 +1103,8 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
     if (p && p->real_kind) return static_cast<int>(p->inner->passes.size()) + 1;
     if (p && p->strided)
-        return static_cast<int>(p->inner->passes.size()) + (p->in_contig ? 0 : 1) + (p->out_contig ? 0 : 1);
+        return static_cast<int>(p->inner->passes.size()) +
+               (p->interleaved ? 0 : (p->in_contig ? 0 : 1) + (p->out_contig ? 0 : 1));
     return p ? static_cast<int>(p->passes.size()) : -1;
 }
 

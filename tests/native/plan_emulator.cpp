@@ -189,9 +189,11 @@ extern "C" int emu_describe(int dbl, int dir, int norm, int in_place, unsigned r
     }
 }
 
-extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
-                       uint64_t batch, int force_maxv, int smem_limit, const double* in, double* out,
-                       char* desc, size_t desc_cap, char* err, size_t cap) {
+namespace {
+
+int run_request(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape, uint64_t batch,
+                int force_maxv, int smem_limit, unsigned skip_axes, const double* in, double* out, char* desc,
+                size_t desc_cap, char* err, size_t cap) {
     try {
         PlanRequest req;
         req.dbl = dbl != 0;
@@ -202,6 +204,7 @@ extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, 
         req.batch = batch;
         req.force_maxv = force_maxv;
         req.smem_limit = smem_limit;
+        req.skip_axes = skip_axes;
         PlanSpec plan = make_plan(req);
         set_err(desc, desc_cap, describe_plan(plan));
         const int64_t E = static_cast<int64_t>(plan.elements);
@@ -225,4 +228,21 @@ extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, 
         set_err(err, cap, e.what());
         return 1;
     }
+}
+
+}  // namespace
+
+extern "C" int emu_run(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
+                       uint64_t batch, int force_maxv, int smem_limit, const double* in, double* out,
+                       char* desc, size_t desc_cap, char* err, size_t cap) {
+    return run_request(dbl, dir, norm, in_place, rank, shape, batch, force_maxv, smem_limit, 0u, in, out, desc,
+                       desc_cap, err, cap);
+}
+
+// Like emu_run with axes left untransformed (bit ax of skip_axes: PlanRequest::skip_axes).
+extern "C" int emu_run_skip(int dbl, int dir, int norm, int in_place, unsigned rank, const uint64_t* shape,
+                            uint64_t batch, unsigned skip_axes, const double* in, double* out, char* desc,
+                            size_t desc_cap, char* err, size_t cap) {
+    return run_request(dbl, dir, norm, in_place, rank, shape, batch, 0, 0, skip_axes, in, out, desc, desc_cap, err,
+                       cap);
 }

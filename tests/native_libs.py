@@ -46,6 +46,24 @@ def emulate(x, shape, batch, direction, norm=0, double=False, in_place=False, fo
     return out, json.loads(desc.value.decode())
 
 
+def emulate_skip(x, shape, batch, direction, skip_axes, norm=0, double=False, in_place=False):
+    """emulate() with the axes in the bit mask `skip_axes` left untransformed."""
+    L = _load("libplan_emulator.so")
+    L.emu_run_skip.argtypes = [ctypes.c_int] * 4 + [ctypes.c_uint, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint,
+                                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                                    ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
+    sh = (ctypes.c_uint64 * 3)(*(list(shape) + [0] * (3 - len(shape))))
+    xin = np.ascontiguousarray(np.asarray(x, dtype=np.complex128))
+    out = np.zeros_like(xin)
+    desc = ctypes.create_string_buffer(1 << 18)
+    err = ctypes.create_string_buffer(1024)
+    rc = L.emu_run_skip(int(double), int(direction), int(norm), int(in_place), len(shape), sh, int(batch),
+                        int(skip_axes), xin.ctypes.data, out.ctypes.data, desc, 1 << 18, err, 1024)
+    if rc:
+        raise RuntimeError(err.value.decode())
+    return out, json.loads(desc.value.decode())
+
+
 def describe(shape, batch, direction=-1, norm=0, double=False, in_place=False, smem_limit=232448, split_bf16=False):
     """The planner's plan for a request (no execution), as the provider describes it."""
     L = _load("libplan_emulator.so")

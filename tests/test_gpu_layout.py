@@ -92,6 +92,8 @@ CASES = [
     ([16, 24], 4, L([1, 16], 384, [24, 1], 400), 1, 0, True, False),   # transposed input, padded out
     ([8, 12, 10], 2, L([130, 10, 1], 1100, [120, 10, 1], 960), -1, 3, False, False),  # padded 3D
     ([6, 5, 4], 3, L([1, 6, 30], 120, [20, 4, 1], 120), 1, 2, True, False),  # fully reversed axis order
+    ([12, 10], 3, L([30, 3], 1, [30, 3], 1), -1, 0, False, False),  # 2D over 3 interleaved arrays (direct)
+    ([1024], 300, L([300], 1, [300], 1), 1, 3, True, True),         # columns in place, double (direct)
 ]
 
 
@@ -100,6 +102,13 @@ def test_strided_layout_parity(torch, sf, shape, batch, lay, d, norm, dbl, in_pl
     p = run_layout(torch, sf, shape, batch, lay, d, norm, dbl, in_place)
     desc = p.describe()
     assert "layout" in desc and "inner" in desc
+    # an interleaved batch (distance 1, dense columns) on both sides runs the axis passes
+    # straight on the user's array: no gather / scatter launches
+    rank_dense = lay.in_distance == 1 and lay.in_strides == lay.out_strides and lay.out_distance == 1 and all(
+        s == batch * math.prod(shape[k + 1:]) for k, s in enumerate(lay.in_strides) if shape[k] > 1)
+    assert desc["layout"]["interleaved"] == (1 if rank_dense else 0)
+    if rank_dense:
+        assert p.launches() == len(desc["inner"]["passes"])
 
 
 def test_large_column_transform(torch, sf):
@@ -127,11 +136,13 @@ def test_contiguous_layout_is_a_plain_plan(torch, sf):
 
 
 def test_partial_batch(torch, sf):
+    """The first b of B transforms (execute_batch) through a gathered layout: columns of a
+    matrix with 20 columns, 16 of them transformed."""
     import ctypes
     from syclfft_b200 import _provider
-    n, batch, run = 128, 16, 5
-    lay = sf.data_layout((batch,), 1, (batch,), 1)
-    x = torch.randn(n * batch, dtype=torch.complex64, device="cuda")
+    n, batch, pitch, run = 128, 16, 20, 5
+    lay = sf.data_layout((pitch,), 1, (pitch,), 1)
+    x = torch.randn(n * pitch, dtype=torch.complex64, device="cuda")
     out = torch.zeros_like(x)
     p = sf.plan_many_dft("float", [n], batch, sf.direction.forward, layout=lay)
     err = ctypes.create_string_buffer(_provider.ERR_CAP)
@@ -139,10 +150,15 @@ def test_partial_batch(torch, sf):
                                            torch.cuda.current_stream().cuda_stream, err, _provider.ERR_CAP)
     assert rc == 0, err.value
     torch.cuda.synchronize()
-    xm, om = x.view(n, batch).cpu().numpy(), out.view(n, batch).cpu().numpy()
+    xm, om = x.view(n, pitch).cpu().numpy(), out.view(n, pitch).cpu().numpy()
     ref = np.fft.fft(xm[:, :run].astype(np.complex128), axis=0)
     assert rel_l2(om[:, :run], ref) <= 1e-5 * 7
     assert np.all(om[:, run:] == 0)
+    # an interleaved-batch plan (stride = batch, distance 1) runs its whole batch only
+    q = sf.plan_many_dft("float", [n], batch, sf.direction.forward, layout=sf.data_layout((batch,), 1, (batch,), 1))
+    rc = q._lib.syclfft_b200_execute_batch(q._handle, x.data_ptr(), out.data_ptr(), run,
+                                           torch.cuda.current_stream().cuda_stream, err, _provider.ERR_CAP)
+    assert rc != 0 and b"whole batch" in err.value
 
 
 def test_layout_errors(torch, sf):

@@ -49,6 +49,21 @@ struct plan_options {
     bool split_precision = false;
 };
 
+// B200 extension (the reference's plans read and write contiguous batch-major arrays only):
+// element (b, i0, .., i_{rank-1}) of the input is at b * in_distance + sum_k i_k * in_strides[k]
+// complex elements from the input pointer, and likewise for the output. One stride per axis,
+// strides >= 1, distances >= 1 when batch_count > 1; the output layout must not overlap
+// itself and an in-place plan needs equal layouts (invalid_argument otherwise).
+struct data_layout {
+    std::vector<std::ptrdiff_t> in_strides;
+    std::ptrdiff_t in_distance = 0;
+    std::vector<std::ptrdiff_t> out_strides;
+    std::ptrdiff_t out_distance = 0;
+};
+
+// B200 extension: kind of a real transform (real_plan).
+enum class real_kind { r2c, c2r };
+
 struct provider_status {
     provider id{};
     std::string name;
@@ -130,6 +145,45 @@ public:
 
     plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, syclfft_b200::direction dir,
          plan_options options);
+    // B200 extension: strided input / output (data_layout)
+    plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, syclfft_b200::direction dir,
+         plan_options options, const data_layout& layout);
+
+private:
+    class impl;
+    std::unique_ptr<impl> impl_;
+};
+
+// B200 extension, no counterpart in the reference (its v0.1 scope is complex-to-complex):
+// batched one-dimensional real transforms of even length n, out of place. r2c (forward): n
+// reals per transform in, n/2 + 1 complex out. c2r (backward): n/2 + 1 complex in (the
+// imaginary parts of bins 0 and n/2 are ignored), n reals out. plan_options::normalization
+// scales relative to n as for a complex plan of length n; placement must be out_of_place.
+template <class Scalar>
+class SYCLFFT_B200_CXX_EXPORT real_plan {
+    static_assert(std::is_same_v<Scalar, float> || std::is_same_v<Scalar, double>,
+                  "syclfft supports float and double precision");
+
+public:
+    using scalar_type = Scalar;
+    using complex_type = complex<Scalar>;
+
+    real_plan(const real_plan&) = delete;
+    real_plan& operator=(const real_plan&) = delete;
+    real_plan(real_plan&&) noexcept;
+    real_plan& operator=(real_plan&&) noexcept;
+    ~real_plan();
+
+    // r2c plans (invalid_argument on a c2r plan)
+    event execute(const Scalar* input, complex_type* output, const std::vector<event>& dependencies = {});
+    // c2r plans (invalid_argument on an r2c plan)
+    event execute(const complex_type* input, Scalar* output, const std::vector<event>& dependencies = {});
+
+    [[nodiscard]] std::size_t length() const noexcept;
+    [[nodiscard]] std::size_t batch_count() const noexcept;
+    [[nodiscard]] real_kind kind() const noexcept;
+
+    real_plan(queue q, std::size_t n, std::size_t batch_count, real_kind kind, plan_options options);
 
 private:
     class impl;
@@ -148,6 +202,23 @@ template <class Scalar>
 plan<Scalar> plan_many_dft(queue q, std::initializer_list<std::size_t> lengths, std::size_t batch_count,
                            direction dir, plan_options options = {}) {
     return plan<Scalar>(q, {lengths.begin(), lengths.end()}, batch_count, dir, options);
+}
+
+// B200 extension: strided layouts (data_layout)
+template <class Scalar>
+plan<Scalar> plan_many_dft(queue q, const std::vector<std::size_t>& lengths, std::size_t batch_count,
+                           direction dir, plan_options options, const data_layout& layout) {
+    return plan<Scalar>(q, lengths, batch_count, dir, options, layout);
+}
+
+template <class Scalar>
+real_plan<Scalar> plan_dft_r2c_1d(queue q, std::size_t n, std::size_t batch_count = 1, plan_options options = {}) {
+    return real_plan<Scalar>(q, n, batch_count, real_kind::r2c, options);
+}
+
+template <class Scalar>
+real_plan<Scalar> plan_dft_c2r_1d(queue q, std::size_t n, std::size_t batch_count = 1, plan_options options = {}) {
+    return real_plan<Scalar>(q, n, batch_count, real_kind::c2r, options);
 }
 
 template <class Scalar>
@@ -178,5 +249,7 @@ SYCLFFT_B200_CXX_EXPORT std::vector<std::string> provider_search_paths();
 
 extern template class plan<float>;
 extern template class plan<double>;
+extern template class real_plan<float>;
+extern template class real_plan<double>;
 
 }  // namespace syclfft_b200

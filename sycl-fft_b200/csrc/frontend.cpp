@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstdlib>
@@ -95,11 +96,16 @@ std::vector<std::string> provider_search_paths() {
 }
 
 using syclfft_b200_create_ex_fn = void* (*)(const syclfft_b200_plan_config_v1*, uint32_t, char*, size_t);
+using syclfft_b200_create_real_fn = void* (*)(const syclfft_b200_plan_config_v1*, int32_t, uint32_t, char*, size_t);
+using syclfft_b200_create_strided_fn = void* (*)(const syclfft_b200_plan_config_v1*, const syclfft_b200_layout_v1*,
+                                                 uint32_t, char*, size_t);
 
 struct loaded_provider {
     const syclfft_b200_provider_v1* api{};
     std::shared_ptr<void> module;
-    syclfft_b200_create_ex_fn create_ex{};  // optional extension (split precision)
+    syclfft_b200_create_ex_fn create_ex{};            // optional extensions: split precision,
+    syclfft_b200_create_real_fn create_real{};        // real transforms,
+    syclfft_b200_create_strided_fn create_strided{};  // strided layouts
 };
 
 // provider_loader.cpp:178-232: first module in the search path that exports the entry
@@ -127,9 +133,67 @@ loaded_provider load_b200_provider() {
         if (!api || api->abi_version != SYCLFFT_B200_PROVIDER_ABI_VERSION)
             throw exception(error_code::plugin_error, "Provider 'syclfft_provider_b200' has an incompatible ABI");
         auto create_ex = reinterpret_cast<syclfft_b200_create_ex_fn>(dlsym(raw, "syclfft_b200_create_ex"));
-        return {api, std::move(module), create_ex};
+        auto create_real = reinterpret_cast<syclfft_b200_create_real_fn>(dlsym(raw, "syclfft_b200_create_real"));
+        auto create_strided =
+            reinterpret_cast<syclfft_b200_create_strided_fn>(dlsym(raw, "syclfft_b200_create_strided"));
+        return {api, std::move(module), create_ex, create_real, create_strided};
     }
     throw exception(error_code::provider_unavailable, "Unable to load provider 'syclfft_provider_b200': " + errors);
+}
+
+// sycl.cpp:72-85: non-null and an allocation the plan's device can access
+void validate_device_pointer(const void* pointer, const char* name, int device) {
+    if (!pointer) throw exception(error_code::invalid_pointer, std::string(name) + " must be non-null");
+    cudaPointerAttributes attr{};
+    const cudaError_t e = cudaPointerGetAttributes(&attr, pointer);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw exception(error_code::invalid_pointer, std::string(name) + " is not a CUDA allocation");
+    }
+    if (attr.type == cudaMemoryTypeUnregistered)
+        throw exception(error_code::invalid_pointer,
+                        std::string(name) + " is not a device-accessible allocation in the plan context");
+    if (attr.type == cudaMemoryTypeDevice && attr.device != device)
+        throw exception(error_code::invalid_pointer, std::string(name) + " belongs to another device");
+}
+
+// data_layout rules: one stride per axis, strides >= 1, distances >= 1 for more than one
+// transform, an output that never writes two elements to one address (sorted by stride, each
+// stride exceeds the span of the smaller ones), equal layouts in place.
+syclfft_b200_layout_v1 checked_layout(const data_layout& l, const std::vector<std::size_t>& lengths,
+                                      std::size_t batch, bool in_place) {
+    syclfft_b200_layout_v1 out{};
+    for (int side = 0; side < 2; ++side) {
+        const auto& strides = side ? l.out_strides : l.in_strides;
+        const std::ptrdiff_t dist = side ? l.out_distance : l.in_distance;
+        const std::string name = side ? "output" : "input";
+        if (strides.size() != lengths.size())
+            throw exception(error_code::invalid_argument, name + " layout needs one stride per axis");
+        for (std::size_t k = 0; k < strides.size(); ++k) {
+            if (strides[k] < 1) throw exception(error_code::invalid_argument, name + " strides must be >= 1");
+            (side ? out.out_strides : out.in_strides)[k] = strides[k];
+        }
+        if (batch > 1 && dist < 1) throw exception(error_code::invalid_argument, name + " distance must be >= 1");
+        (side ? out.out_distance : out.in_distance) = dist;
+    }
+    std::vector<std::pair<std::ptrdiff_t, std::size_t>> dims;
+    for (std::size_t k = 0; k < lengths.size(); ++k)
+        if (lengths[k] > 1) dims.push_back({l.out_strides[k], lengths[k]});
+    if (batch > 1) dims.push_back({l.out_distance, batch});
+    std::sort(dims.begin(), dims.end());
+    long double reach = 0;
+    for (const auto& d : dims) {
+        if (static_cast<long double>(d.first) <= reach)
+            throw exception(error_code::invalid_argument, "output layout overlaps itself");
+        reach += static_cast<long double>(d.first) * static_cast<long double>(d.second - 1);
+    }
+    if (in_place) {
+        bool same = batch <= 1 || l.in_distance == l.out_distance;
+        for (std::size_t k = 0; k < lengths.size(); ++k)
+            if (lengths[k] > 1 && l.in_strides[k] != l.out_strides[k]) same = false;
+        if (!same) throw exception(error_code::invalid_argument, "an in-place plan needs equal input and output layouts");
+    }
+    return out;
 }
 
 }  // namespace detail
@@ -161,7 +225,7 @@ template <class Scalar>
 class plan<Scalar>::impl {
 public:
     impl(queue q, std::vector<std::size_t> lengths, std::size_t batch, syclfft_b200::direction dir,
-         plan_options opts)
+         plan_options opts, const data_layout* layout = nullptr)
         : queue_(q),
           lengths_(std::move(lengths)),
           batch_count_(batch),
@@ -196,7 +260,15 @@ public:
         config.normalization = static_cast<uint32_t>(options_.normalization);
         config.measure = options_.planning == planning_mode::measure ? 1 : 0;
         config.device = queue_.device;
-        if (options_.split_precision && std::is_same_v<Scalar, float>) {
+        if (layout) {
+            const syclfft_b200_layout_v1 lay = detail::checked_layout(*layout, lengths_, batch_count_,
+                                                                      options_.placement == placement::in_place);
+            if (!module_.create_strided)
+                throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_strided");
+            uint32_t flags = SYCLFFT_B200_CREATE_SYNC;
+            if (options_.split_precision && std::is_same_v<Scalar, float>) flags |= SYCLFFT_B200_CREATE_SPLIT_BF16;
+            handle_ = module_.create_strided(&config, &lay, flags, error.data(), error.size());
+        } else if (options_.split_precision && std::is_same_v<Scalar, float>) {
             if (!module_.create_ex)
                 throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_ex");
             handle_ = module_.create_ex(&config, SYCLFFT_B200_CREATE_SYNC | SYCLFFT_B200_CREATE_SPLIT_BF16,
@@ -218,19 +290,7 @@ public:
     }
 
     void validate_pointer(const void* pointer, const char* name) const {
-        // sycl.cpp:72-85: non-null and an allocation the plan's device can access
-        if (!pointer) throw exception(error_code::invalid_pointer, std::string(name) + " must be non-null");
-        cudaPointerAttributes attr{};
-        const cudaError_t e = cudaPointerGetAttributes(&attr, pointer);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            throw exception(error_code::invalid_pointer, std::string(name) + " is not a CUDA allocation");
-        }
-        if (attr.type == cudaMemoryTypeUnregistered)
-            throw exception(error_code::invalid_pointer,
-                            std::string(name) + " is not a device-accessible allocation in the plan context");
-        if (attr.type == cudaMemoryTypeDevice && attr.device != queue_.device)
-            throw exception(error_code::invalid_pointer, std::string(name) + " belongs to another device");
+        detail::validate_device_pointer(pointer, name, queue_.device);
     }
 
     event execute(const complex_type* input, complex_type* output, const std::vector<event>& dependencies,
@@ -277,6 +337,11 @@ template <class Scalar>
 plan<Scalar>::plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, syclfft_b200::direction dir,
                    plan_options options)
     : impl_(std::make_unique<impl>(q, std::move(lengths), batch_count, dir, options)) {}
+
+template <class Scalar>
+plan<Scalar>::plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, syclfft_b200::direction dir,
+                   plan_options options, const data_layout& layout)
+    : impl_(std::make_unique<impl>(q, std::move(lengths), batch_count, dir, options, &layout)) {}
 
 template <class Scalar>
 plan<Scalar>::plan(plan&&) noexcept = default;
@@ -364,5 +429,132 @@ std::vector<provider_status> query_providers(const queue& q) {
 
 template class plan<float>;
 template class plan<double>;
+
+// ---------------------------------------------------------------- real_plan
+template <class Scalar>
+class real_plan<Scalar>::impl {
+public:
+    impl(queue q, std::size_t n, std::size_t batch, real_kind kind, plan_options opts)
+        : queue_(q), n_(n), batch_count_(batch), kind_(kind), options_(opts) {
+        (void)detail::checked_element_count({n_}, batch_count_);
+        if (n_ % 2) throw exception(error_code::invalid_argument, "real transforms need an even length");
+        if (options_.placement != placement::out_of_place)
+            throw exception(error_code::invalid_argument, "real transforms are out of place");
+        if (kind_ != real_kind::r2c && kind_ != real_kind::c2r)
+            throw exception(error_code::invalid_argument, "real transform kind must be r2c or c2r");
+        if (options_.preferred_provider != provider::automatic && options_.preferred_provider != provider::b200) {
+            throw exception(error_code::provider_unavailable,
+                            std::string(detail::provider_name(options_.preferred_provider)) +
+                                " provider is not part of this build");
+        }
+        module_ = detail::load_b200_provider();
+        if (!module_.create_real)
+            throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_real");
+        if (queue_.device < 0) {
+            const cudaError_t e = cudaGetDevice(&queue_.device);
+            if (e != cudaSuccess) throw exception(error_code::provider_unavailable, cudaGetErrorString(e));
+        }
+        std::array<char, 1024> error{};
+        if (!module_.api->supports(queue_.device, error.data(), error.size())) {
+            throw exception(error_code::provider_unavailable,
+                            error[0] ? error.data() : "B200 provider rejected the device");
+        }
+        syclfft_b200_plan_config_v1 config{};
+        config.abi_version = SYCLFFT_B200_PROVIDER_ABI_VERSION;
+        config.scalar = std::is_same_v<Scalar, double> ? SYCLFFT_B200_SCALAR_DOUBLE : SYCLFFT_B200_SCALAR_FLOAT;
+        config.direction = kind_ == real_kind::r2c ? -1 : 1;
+        config.rank = 1;
+        config.lengths[0] = n_;
+        config.batch_count = batch_count_;
+        config.in_place = 0;
+        config.normalization = static_cast<uint32_t>(options_.normalization);
+        config.measure = options_.planning == planning_mode::measure ? 1 : 0;
+        config.device = queue_.device;
+        uint32_t flags = SYCLFFT_B200_CREATE_SYNC;
+        if (options_.split_precision && std::is_same_v<Scalar, float>) flags |= SYCLFFT_B200_CREATE_SPLIT_BF16;
+        handle_ = module_.create_real(&config, kind_ == real_kind::r2c ? SYCLFFT_B200_REAL_R2C : SYCLFFT_B200_REAL_C2R,
+                                      flags, error.data(), error.size());
+        if (!handle_)
+            throw exception(error_code::planning_failed, error[0] ? error.data() : "B200 plan creation failed");
+    }
+
+    ~impl() {
+        try {
+            if (last_event_) last_event_->wait_and_throw();
+        } catch (...) {
+        }
+        if (handle_) module_.api->destroy(handle_);
+    }
+
+    event execute(const void* input, void* output, const std::vector<event>& dependencies, real_kind called) {
+        if (called != kind_)
+            throw exception(error_code::invalid_argument, kind_ == real_kind::r2c
+                                                              ? "an r2c plan takes real input and complex output"
+                                                              : "a c2r plan takes complex input and real output");
+        detail::validate_device_pointer(input, "input", queue_.device);
+        detail::validate_device_pointer(output, "output", queue_.device);
+        if (input == output) throw exception(error_code::invalid_argument, "Out-of-place plan requires distinct allocations");
+        std::scoped_lock lock(mutex_);
+        auto stream = reinterpret_cast<cudaStream_t>(queue_.stream);
+        for (const auto& dep : dependencies) {
+            if (dep.valid()) cudaStreamWaitEvent(stream, reinterpret_cast<cudaEvent_t>(dep.native()), 0);
+        }
+        if (last_event_ && last_event_->valid())
+            cudaStreamWaitEvent(stream, reinterpret_cast<cudaEvent_t>(last_event_->native()), 0);
+        std::array<char, 1024> error{};
+        const int rc = module_.api->execute(handle_, input, output, queue_.stream, error.data(), error.size());
+        if (rc != 0 || error[0])
+            throw exception(error_code::execution_failed, error[0] ? error.data() : "B200 execution failed");
+        event done = event::record(queue_.stream);
+        last_event_ = done;
+        return done;
+    }
+
+    queue queue_;
+    std::size_t n_{};
+    std::size_t batch_count_{};
+    real_kind kind_{real_kind::r2c};
+    plan_options options_{};
+    detail::loaded_provider module_;
+    void* handle_{};
+    std::optional<event> last_event_;
+    std::mutex mutex_;
+};
+
+template <class Scalar>
+real_plan<Scalar>::real_plan(queue q, std::size_t n, std::size_t batch_count, real_kind kind, plan_options options)
+    : impl_(std::make_unique<impl>(q, n, batch_count, kind, options)) {}
+template <class Scalar>
+real_plan<Scalar>::real_plan(real_plan&&) noexcept = default;
+template <class Scalar>
+real_plan<Scalar>& real_plan<Scalar>::operator=(real_plan&&) noexcept = default;
+template <class Scalar>
+real_plan<Scalar>::~real_plan() = default;
+
+template <class Scalar>
+event real_plan<Scalar>::execute(const Scalar* input, complex_type* output, const std::vector<event>& dependencies) {
+    SYCLFFT_B200_REQUIRE_IMPL();
+    return impl_->execute(input, output, dependencies, real_kind::r2c);
+}
+template <class Scalar>
+event real_plan<Scalar>::execute(const complex_type* input, Scalar* output, const std::vector<event>& dependencies) {
+    SYCLFFT_B200_REQUIRE_IMPL();
+    return impl_->execute(input, output, dependencies, real_kind::c2r);
+}
+template <class Scalar>
+std::size_t real_plan<Scalar>::length() const noexcept {
+    return impl_ ? impl_->n_ : 0;
+}
+template <class Scalar>
+std::size_t real_plan<Scalar>::batch_count() const noexcept {
+    return impl_ ? impl_->batch_count_ : 0;
+}
+template <class Scalar>
+real_kind real_plan<Scalar>::kind() const noexcept {
+    return impl_ ? impl_->kind_ : real_kind::r2c;
+}
+
+template class real_plan<float>;
+template class real_plan<double>;
 
 }  // namespace syclfft_b200

@@ -288,6 +288,93 @@ try {
         }
         check(std::sqrt(num / den) < 2e-5, "split-precision plan mismatch");
     }
+    {
+        // B200 extension: real transforms (r2c against the direct DFT of the real lines, then
+        // c2r with backward normalization back to the input)
+        const std::size_t n = 64, batch = 3, h = n / 2 + 1;
+        std::vector<float> real(n * batch);
+        std::vector<std::complex<float>> as_complex(n * batch);
+        for (std::size_t i = 0; i < n * batch; ++i) {
+            real[i] = static_cast<float>((i * 7 + 3) % 11) / 5.f - 1.f;
+            as_complex[i] = {real[i], 0.f};
+        }
+        const auto full = reference_many(as_complex, {n}, batch, sf::direction::forward);
+        device_buffer<float> x(n * batch), back(n * batch);
+        device_buffer<std::complex<float>> spec(h * batch);
+        x.write(real);
+        auto opts = make_plan_options(sf::placement::out_of_place, sf::normalization::backward);
+        auto r2c = sf::plan_dft_r2c_1d<float>(sf::queue{}, n, batch, opts);
+        auto c2r = sf::plan_dft_c2r_1d<float>(sf::queue{}, n, batch, opts);
+        check(r2c.kind() == sf::real_kind::r2c && c2r.length() == n && c2r.batch_count() == batch, "real plan shape");
+        auto done = r2c.execute(x.get(), spec.get());
+        c2r.execute(spec.get(), back.get(), {done}).wait_and_throw();
+        const auto s = spec.read();
+        const auto y = back.read();
+        double num = 0, den = 0, rnum = 0, rden = 0;
+        for (std::size_t b = 0; b < batch; ++b)
+            for (std::size_t k = 0; k < h; ++k) {
+                num += std::norm(std::complex<double>(s[b * h + k]) - std::complex<double>(full[b * n + k]));
+                den += std::norm(std::complex<double>(full[b * n + k]));
+            }
+        for (std::size_t i = 0; i < n * batch; ++i) {
+            rnum += (double(y[i]) - real[i]) * (double(y[i]) - real[i]);
+            rden += double(real[i]) * real[i];
+        }
+        check(std::sqrt(num / den) < 1e-5, "r2c plan mismatch");
+        check(std::sqrt(rnum / rden) < 1e-5, "c2r round trip mismatch");
+        expect_error(sf::error_code::invalid_argument, [&] { c2r.execute(x.get(), spec.get()); });
+        expect_error(sf::error_code::invalid_argument, [] { (void)sf::plan_dft_r2c_1d<double>(sf::queue{}, 7); });
+    }
+    {
+        // B200 extension: strided layouts -- 16-point transforms down the 6 columns of a 16 x 6
+        // matrix written as contiguous rows, and 32-point transforms down 5 interleaved
+        // columns in place
+        const std::size_t n = 16, cols = 6;
+        std::vector<std::complex<float>> matrix(n * cols), gathered(n * cols);
+        for (std::size_t i = 0; i < n * cols; ++i)
+            matrix[i] = {static_cast<float>((i * 5 + 1) % 9) / 4.f, static_cast<float>((i * 3 + 2) % 7) / 3.f};
+        for (std::size_t c = 0; c < cols; ++c)
+            for (std::size_t k = 0; k < n; ++k) gathered[c * n + k] = matrix[k * cols + c];
+        const auto expected = reference_many(gathered, {n}, cols, sf::direction::forward);
+        device_buffer<std::complex<float>> in(n * cols), out(n * cols);
+        in.write(matrix);
+        sf::data_layout lay{{static_cast<std::ptrdiff_t>(cols)}, 1, {1}, static_cast<std::ptrdiff_t>(n)};
+        auto fft = sf::plan_many_dft<float>(sf::queue{}, {n}, cols, sf::direction::forward, make_plan_options(), lay);
+        fft.execute(in.get(), out.get()).wait_and_throw();
+        const auto got = out.read();
+        double num = 0, den = 0;
+        for (std::size_t i = 0; i < n * cols; ++i) {
+            num += std::norm(std::complex<double>(got[i]) - std::complex<double>(expected[i]));
+            den += std::norm(std::complex<double>(expected[i]));
+        }
+        check(std::sqrt(num / den) < 1e-5, "column layout mismatch");
+
+        const std::size_t m = 32, b = 5;
+        std::vector<std::complex<float>> inter(m * b), cols_in(m * b);
+        for (std::size_t i = 0; i < m * b; ++i)
+            inter[i] = {static_cast<float>((i * 13 + 4) % 17) / 8.f, static_cast<float>((i * 2 + 5) % 11) / 5.f};
+        for (std::size_t c = 0; c < b; ++c)
+            for (std::size_t k = 0; k < m; ++k) cols_in[c * m + k] = inter[k * b + c];
+        const auto want = reference_many(cols_in, {m}, b, sf::direction::backward);
+        device_buffer<std::complex<float>> io(m * b);
+        io.write(inter);
+        sf::data_layout il{{static_cast<std::ptrdiff_t>(b)}, 1, {static_cast<std::ptrdiff_t>(b)}, 1};
+        auto ip = sf::plan_many_dft<float>(sf::queue{}, {m}, b, sf::direction::backward,
+                                           make_plan_options(sf::placement::in_place), il);
+        ip.execute(io.get()).wait_and_throw();
+        const auto r = io.read();
+        num = den = 0;
+        for (std::size_t c = 0; c < b; ++c)
+            for (std::size_t k = 0; k < m; ++k) {
+                num += std::norm(std::complex<double>(r[k * b + c]) - std::complex<double>(want[c * m + k]));
+                den += std::norm(std::complex<double>(want[c * m + k]));
+            }
+        check(std::sqrt(num / den) < 1e-5, "interleaved in-place layout mismatch");
+        expect_error(sf::error_code::invalid_argument, [&] {
+            sf::data_layout overlap{{1}, 1, {1}, 4};  // 8-point output rows 4 apart overlap
+            (void)sf::plan_many_dft<float>(sf::queue{}, {8}, 3, sf::direction::forward, make_plan_options(), overlap);
+        });
+    }
     // sycl_tests.cpp:508-538
     expect_error(sf::error_code::provider_unavailable, [&] {
         (void)sf::plan_dft_1d<float>(sf::queue{}, 8, sf::direction::forward,

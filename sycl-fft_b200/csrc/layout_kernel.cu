@@ -4,7 +4,7 @@
 // Element (b, i0, .., i_{r-1}) of a layout sits at b * dist + sum_k i_k * stride_k (in complex
 // elements). The index space is viewed as a matrix: rows = (b, i0, .., i_{r-2}) with the last
 // of them fastest, columns = i_{r-1}. The contiguous side is row-major with C = L_{r-1}
-// columns. A 32 x 32 tile goes through shared memory, so both sides are coalesced whichever
+// columns. A 32-row tile goes through shared memory, so both sides are coalesced whichever
 // of the two matrix directions the strided side is dense in: "column mode" (warp lanes along
 // i_{r-1}) when stride_{r-1} is the smaller step, "row mode" (lanes along the fastest row
 // index) otherwise, e.g. transforms down the columns of a row-major matrix.
@@ -26,10 +26,13 @@ struct RowMap {
     int64_t dist;
     __device__ int64_t offset(int64_t row) const {
         int64_t off = 0;
-        for (int k = rank - 2; k >= 0; --k) {
-            const int64_t q = row / len[k];
-            off += (row - q * len[k]) * stride[k];
-            row = q;
+#pragma unroll
+        for (int k = 1; k >= 0; --k) {  // compile-time indices: the arrays stay in registers
+            if (k <= rank - 2) {
+                const int64_t q = row / len[k];
+                off += (row - q * len[k]) * stride[k];
+                row = q;
+            }
         }
         return off + row * dist;
     }
@@ -49,17 +52,25 @@ RowMap row_map(const Layout& l) {
 // Step between consecutive rows' fastest index (the stride of i_{r-2}, or the batch distance).
 int64_t row_step(const Layout& l) { return l.rank >= 2 ? l.stride[l.rank - 2] : l.dist; }
 
+// Tile of kTile rows x TC columns (TC = 64 for complex<float>, 32 for complex<double>: 16 KB
+// per tile either way), 8 loads or stores per thread per phase.
+template <class T>
+__host__ __device__ constexpr int tile_cols() {
+    return sizeof(T) == 4 ? 64 : 32;
+}
+
 template <class T, bool kGather, bool kRowMode>
 __global__ void __launch_bounds__(kTile* kRowsPerPass)
     layout_kernel(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, RowMap map, int64_t col_stride,
                   int64_t rows, int64_t cols) {
     using C = cplx<T>;
-    __shared__ C tile[kTile][kTile + 1];
-    const int64_t col_tiles = (cols + kTile - 1) / kTile;
+    constexpr int TC = tile_cols<T>();
+    __shared__ C tile[kTile][TC + 1];
+    const int64_t col_tiles = (cols + TC - 1) / TC;
     const int64_t tiles = col_tiles * ((rows + kTile - 1) / kTile);
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int64_t r0 = (t / col_tiles) * kTile, c0 = (t % col_tiles) * kTile;
+        const int64_t r0 = (t / col_tiles) * kTile, c0 = (t % col_tiles) * TC;
         // strided side: read (gather) or write (scatter) through the layout
         // contiguous side: row-major rows x cols, lanes along the columns
         if (kGather) {
@@ -67,37 +78,61 @@ __global__ void __launch_bounds__(kTile* kRowsPerPass)
                 const int64_t r = r0 + tx;
                 if (r < rows) {
                     const int64_t base = map.offset(r);
-                    for (int j = ty; j < kTile; j += kRowsPerPass)
+#pragma unroll
+                    for (int j = ty; j < TC; j += kRowsPerPass)
                         if (c0 + j < cols) tile[tx][j] = src[base + (c0 + j) * col_stride];
                 }
             } else {
+#pragma unroll
                 for (int i = ty; i < kTile; i += kRowsPerPass) {
                     const int64_t r = r0 + i;
-                    if (r < rows && c0 + tx < cols) tile[i][tx] = src[map.offset(r) + (c0 + tx) * col_stride];
+                    if (r < rows) {
+                        const int64_t base = map.offset(r);
+#pragma unroll
+                        for (int j = tx; j < TC; j += kTile)
+                            if (c0 + j < cols) tile[i][j] = src[base + (c0 + j) * col_stride];
+                    }
                 }
             }
             __syncthreads();
+#pragma unroll
             for (int i = ty; i < kTile; i += kRowsPerPass) {
                 const int64_t r = r0 + i;
-                if (r < rows && c0 + tx < cols) dst[r * cols + c0 + tx] = tile[i][tx];
+                if (r < rows) {
+#pragma unroll
+                    for (int j = tx; j < TC; j += kTile)
+                        if (c0 + j < cols) dst[r * cols + c0 + j] = tile[i][j];
+                }
             }
         } else {
+#pragma unroll
             for (int i = ty; i < kTile; i += kRowsPerPass) {
                 const int64_t r = r0 + i;
-                if (r < rows && c0 + tx < cols) tile[i][tx] = src[r * cols + c0 + tx];
+                if (r < rows) {
+#pragma unroll
+                    for (int j = tx; j < TC; j += kTile)
+                        if (c0 + j < cols) tile[i][j] = src[r * cols + c0 + j];
+                }
             }
             __syncthreads();
             if (kRowMode) {
                 const int64_t r = r0 + tx;
                 if (r < rows) {
                     const int64_t base = map.offset(r);
-                    for (int j = ty; j < kTile; j += kRowsPerPass)
+#pragma unroll
+                    for (int j = ty; j < TC; j += kRowsPerPass)
                         if (c0 + j < cols) dst[base + (c0 + j) * col_stride] = tile[tx][j];
                 }
             } else {
+#pragma unroll
                 for (int i = ty; i < kTile; i += kRowsPerPass) {
                     const int64_t r = r0 + i;
-                    if (r < rows && c0 + tx < cols) dst[map.offset(r) + (c0 + tx) * col_stride] = tile[i][tx];
+                    if (r < rows) {
+                        const int64_t base = map.offset(r);
+#pragma unroll
+                        for (int j = tx; j < TC; j += kTile)
+                            if (c0 + j < cols) dst[base + (c0 + j) * col_stride] = tile[i][j];
+                    }
                 }
             }
         }
@@ -111,7 +146,8 @@ cudaError_t launch_one(const void* src, void* dst, const Layout& l, cudaStream_t
     for (int k = 0; k + 1 < l.rank; ++k) rows *= l.len[k];
     const int64_t cols = l.len[l.rank - 1];
     if (rows <= 0 || cols <= 0) return cudaSuccess;
-    const int64_t tiles = ((rows + kTile - 1) / kTile) * ((cols + kTile - 1) / kTile);
+    constexpr int TC = tile_cols<T>();
+    const int64_t tiles = ((rows + kTile - 1) / kTile) * ((cols + TC - 1) / TC);
     const int grid = static_cast<int>(tiles < 148 * 8 ? tiles : 148 * 8);
     const dim3 block(kTile, kRowsPerPass);
     const RowMap map = row_map(l);

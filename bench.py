@@ -728,7 +728,8 @@ def _real_rows(sf, torch, dev, peak, timed, prefix=""):
     there is no CPU row."""
     import numpy as np
     rows = []
-    for row, n, batch, dbl in (("R: r2c+c2r f32 N=16384 x8192", 16384, 8192, False),
+    for row, n, batch, dbl in (("R: r2c+c2r f32 N=8192 x16384 (one pass)", 8192, 16384, False),
+                               ("R: r2c+c2r f32 N=16384 x8192", 16384, 8192, False),
                                ("R: r2c+c2r f32 N=26880 x4096", 26880, 4096, False),
                                ("R: r2c+c2r f64 N=131072 x512", 131072, 512, True)):
         if not row.startswith(prefix):

@@ -68,7 +68,30 @@ enum : int {
     kFeatTw4Conj = 32,
     kFeatConv = 64,
     kFeatSmemIn = 128,  // the first stage reads the tile from shared memory (TMA-staged passes)
+    // Real transforms of length 2N over this length-N FFT (kModeK only; the W_2N^k table of
+    // N+1 entries in `postmul` / `premul`):
+    kFeatRealPost = 512,  // R2C: the spectrum Z goes to shared memory, then X[k] for k = 0..N from
+                          // the pairs (Z[k], Z[N-k]), N+1 bins per line stored
+    kFeatRealPre = 1024,  // C2R: the first stage forms Z[k] from the bins (X[k], X[N-k]) on load
 };
+
+// X[k] = 1/2 [(Z[k] + conj Z[N-k]) - i W_2N^k (Z[k] - conj Z[N-k])] * scale; a = Z[k], c = Z[N-k]
+template <class C, class T>
+__device__ __forceinline__ C real_post_pair(C a, C c, C w, T half) {
+    const C e = cmake<C>(a.x + c.x, a.y - c.y);
+    const C d = cmake<C>(a.x - c.x, a.y + c.y);
+    const T p = w.x * d.x - w.y * d.y, q = w.x * d.y + w.y * d.x;  // w * D
+    return cmake<C>((e.x + q) * half, (e.y - p) * half);
+}
+
+// Z[k] = (X[k] + conj X[N-k]) + i conj(W_2N^k) (X[k] - conj X[N-k]); a = X[k], c = X[N-k]
+template <class C, class T = decltype(C::x)>
+__device__ __forceinline__ C real_pre_pair(C a, C c, C w) {
+    const C e = cmake<C>(a.x + c.x, a.y - c.y);
+    const C d = cmake<C>(a.x - c.x, a.y + c.y);
+    const T p = w.x * d.x + w.y * d.y, q = w.x * d.y - w.y * d.x;  // conj(w) * D
+    return cmake<C>(e.x - q, e.y + p);
+}
 
 template <class T>
 struct FixedCtx {
@@ -136,6 +159,23 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                     }
                     v[i * R + r] = a;
                 }
+            } else if constexpr (FIRST && (FEAT & kFeatRealPre)) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int k = j + r * NR;
+                    C a = cmake<C>(T(0), T(0));
+                    if (X.line_ok) {
+                        C xa = X.gin[k];
+                        C xc = X.gin[N - k];  // the line holds N+1 bins
+                        if (k == 0) {
+                            xa.y = T(0);  // bins 0 and N of a real signal are real
+                            xc.y = T(0);
+                        }
+                        a = real_pre_pair(xa, xc, __ldg(X.premul + k));
+                        if (X.conj_in) a.y = -a.y;
+                    }
+                    v[i * R + r] = a;
+                }
             } else if constexpr (FIRST) {
                 if (X.line_ok) {
 #pragma unroll
@@ -174,7 +214,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 else twiddle_powers<R>(u, __ldg(X.twb + TWOFF + jm));
             }
             dft<R, T>(u);
-            if constexpr (LAST && (FEAT & (kFeatTStore | kFeatMid))) {
+            if constexpr (LAST && (FEAT & (kFeatTStore | kFeatMid | kFeatRealPost))) {
                 // natural order into shared memory: the transposed store, or the second FFT
                 // of a Bluestein convolution (after the spectrum multiply), follows
                 if constexpr (FEAT & kFeatMid) {
@@ -237,7 +277,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             }
         }
     }
-    if constexpr (!LAST || (FEAT & (kFeatTStore | kFeatMid))) __syncthreads();
+    if constexpr (!LAST || (FEAT & (kFeatTStore | kFeatMid | kFeatRealPost))) __syncthreads();
 }
 
 template <class T, int N, int TPL, bool MODEC, int W, int FEAT, int NS, int TWOFF, bool FIRST, int R, int... Rest>
@@ -319,6 +359,20 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         return;
     }
     fixed_stages<T, N, TPL, MODEC, W, FEAT, 1, 0, true, Rs...>(X);
+    if constexpr (FEAT & kFeatRealPost) {
+        static_assert(!MODEC, "real transforms use contiguous lines");
+        // pairs (k, N-k) of this line's spectrum in shared memory -> N+1 bins at X.gout
+        if (X.line_ok) {
+            const T half = T(0.5) * X.scale;
+            for (int k = X.t; k <= N / 2; k += TPL) {
+                const int kk = N - k;
+                const C a = X.sm[pidx<T>(k)];
+                const C c = X.sm[pidx<T>(kk == N ? 0 : kk)];
+                X.gout[k] = real_post_pair(a, c, __ldg(X.postmul + k), half);
+                if (kk != k) X.gout[kk] = real_post_pair(c, a, __ldg(X.postmul + kk), half);
+            }
+        }
+    }
     if constexpr ((FEAT & kFeatTStore) && !MODEC) {
         // Rows blockIdx.x*W .. +W-1 are consecutive k1 of one line (the planner keeps
         // rows % W == 0): walk (row fastest, element) so every store is a W-wide segment.

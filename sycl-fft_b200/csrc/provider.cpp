@@ -197,7 +197,9 @@ struct DevicePlan {
     int64_t real_n = 0;             // real length N (even)
     std::unique_ptr<DevicePlan> inner;
     void* real_buf = nullptr;       // half-length spectra: batch x N/2 complex
-    void* real_tw = nullptr;        // W_N^k, k = 0..N/2
+    void* real_tw = nullptr;        // W_N^k, k = 0..N/2 (then the fused kernel's base twiddles)
+    const RealFusedEntry* real_fused = nullptr;  // one-pass kernel for N/2 (real_kernel.cu), or none
+    int64_t real_base_off = 0;      // complex elements from real_tw to the base twiddles
     // Strided layouts (syclfft_b200_create_strided): the contiguous plan `inner` with gather /
     // scatter passes (layout_kernel.cu) on the sides that are not contiguous.
     bool strided = false;
@@ -521,23 +523,40 @@ DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, u
     const bool dbl = plan->spec.req.dbl;
     const size_t cs = dbl ? 16 : 8;
     const uint64_t h = n / 2;
-    plan->spec.scratch_elements = inner->spec.scratch_elements + h * cfg.batch_count;
+    // One pass when N/2 has a fused kernel (not for split-precision plans, whose inner FFT runs
+    // on the tensor cores); SYCLFFT_B200_REAL_FUSED=0 keeps the two-pass form.
+    const char* fused_env = std::getenv("SYCLFFT_B200_REAL_FUSED");
+    const bool split = !dbl && (flags & SYCLFFT_B200_CREATE_SPLIT_BF16) != 0;
+    if (!split && !(fused_env && std::strcmp(fused_env, "0") == 0))
+        plan->real_fused = find_real_fused(dbl, static_cast<int64_t>(h));
+    plan->spec.scratch_elements = plan->real_fused ? 0 : inner->spec.scratch_elements + h * cfg.batch_count;
     DeviceGuard guard(plan->device);
     cudaStream_t ms = memory_stream(plan->device);
-    std::vector<unsigned char> tw((h + 1) * cs);
-    for (uint64_t k = 0; k <= h; ++k) {
-        const std::complex<double> w = cis_neg(static_cast<int64_t>(k), static_cast<int64_t>(n));
+    std::vector<std::complex<double>> table;
+    for (uint64_t k = 0; k <= h; ++k) table.push_back(cis_neg(static_cast<int64_t>(k), static_cast<int64_t>(n)));
+    plan->real_base_off = static_cast<int64_t>(table.size());
+    if (plan->real_fused) {
+        int64_t ns = 1;  // base twiddles of the fused kernel's stages: W_(ns*R)^jm, jm < ns
+        for (int s = 0; s < plan->real_fused->nstages; ++s) {
+            const int R = plan->real_fused->radices[s];
+            for (int64_t jm = 0; jm < ns; ++jm) table.push_back(cis_neg(jm, ns * R));
+            ns *= R;
+        }
+    }
+    std::vector<unsigned char> tw(table.size() * cs);
+    for (size_t k = 0; k < table.size(); ++k) {
         if (dbl) {
-            reinterpret_cast<double*>(tw.data())[2 * k] = w.real();
-            reinterpret_cast<double*>(tw.data())[2 * k + 1] = w.imag();
+            reinterpret_cast<double*>(tw.data())[2 * k] = table[k].real();
+            reinterpret_cast<double*>(tw.data())[2 * k + 1] = table[k].imag();
         } else {
-            reinterpret_cast<float*>(tw.data())[2 * k] = static_cast<float>(w.real());
-            reinterpret_cast<float*>(tw.data())[2 * k + 1] = static_cast<float>(w.imag());
+            reinterpret_cast<float*>(tw.data())[2 * k] = static_cast<float>(table[k].real());
+            reinterpret_cast<float*>(tw.data())[2 * k + 1] = static_cast<float>(table[k].imag());
         }
     }
     check(cudaMallocAsync(&plan->real_tw, tw.size(), ms), "cudaMallocAsync(real twiddles)");
     check(cudaMemcpyAsync(plan->real_tw, tw.data(), tw.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(real twiddles)");
-    check(cudaMallocAsync(&plan->real_buf, h * cfg.batch_count * cs, ms), "cudaMallocAsync(real spectra)");
+    if (!plan->real_fused)
+        check(cudaMallocAsync(&plan->real_buf, h * cfg.batch_count * cs, ms), "cudaMallocAsync(real spectra)");
     check(cudaStreamSynchronize(ms), "real plan tables");
     check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
     plan->inner = std::move(inner);
@@ -733,7 +752,16 @@ void execute_real(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     const bool dbl = plan->spec.req.dbl;
     const int64_t h = plan->real_n / 2;
     const int64_t lines = static_cast<int64_t>(batch);
-    if (plan->real_kind == SYCLFFT_B200_REAL_R2C) {
+    // the real side is read / written as complex pairs
+    const uintptr_t align = dbl ? 16 : 8;
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % align)
+        throw std::invalid_argument("real-transform buffers must be aligned to the complex element size");
+    if (plan->real_fused) {
+        const void* base = static_cast<const unsigned char*>(plan->real_tw) + plan->real_base_off * (dbl ? 16 : 8);
+        check(launch_real_fused(*plan->real_fused, plan->real_kind == SYCLFFT_B200_REAL_R2C, in, out, lines,
+                                plan->real_tw, base, scale, stream),
+              "fused real transform");
+    } else if (plan->real_kind == SYCLFFT_B200_REAL_R2C) {
         execute_plan(plan->inner.get(), in, plan->real_buf, stream, batch, 0, -1);
         check(launch_r2c_post(dbl, plan->real_buf, out, h, lines, plan->real_tw, scale, stream), "R2C post-process");
     } else {
@@ -1081,7 +1109,8 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
     if (p->real_kind) {
         // a real plan: its complex plan of half the length and the pre-/post-process pass
         s = std::string("{\"real\":\"") + (p->real_kind == SYCLFFT_B200_REAL_R2C ? "r2c" : "c2r") +
-            "\",\"n\":" + std::to_string(p->real_n) + ",\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
+            "\",\"n\":" + std::to_string(p->real_n) + ",\"fused\":" + (p->real_fused ? "1" : "0") +
+            ",\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
     } else if (p->strided) {
         auto side = [](const sfb::Layout& l, bool contig) {
             std::string r = "{\"strides\":[";
@@ -1101,7 +1130,7 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
-    if (p && p->real_kind) return static_cast<int>(p->inner->passes.size()) + 1;
+    if (p && p->real_kind) return p->real_fused ? 1 : static_cast<int>(p->inner->passes.size()) + 1;
     if (p && p->strided)
         return static_cast<int>(p->inner->passes.size()) +
                (p->interleaved ? 0 : (p->in_contig ? 0 : 1) + (p->out_contig ? 0 : 1));

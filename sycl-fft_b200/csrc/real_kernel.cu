@@ -9,9 +9,17 @@
 //                             x[2m] = Re z[m], x[2m+1] = Im z[m].
 // Each thread handles the pair (k, H - k), so both of its values are read once; the
 // normalization scale is fused.
+//
+// Where the half length H has a size-specialised single-CTA kernel (the catalog below), the
+// pre-/post-process is fused into it instead (kFeatRealPre / kFeatRealPost of
+// fixed_kernel.cuh): one HBM pass per real transform.
+#include <atomic>
+#include <type_traits>
+
 #include <cuda_runtime.h>
 
 #include "butterfly.cuh"
+#include "fixed_kernel.cuh"
 #include "real_launch.hpp"
 
 namespace sfb {
@@ -74,12 +82,94 @@ __global__ void c2r_pre_kernel(const cplx<T>* __restrict__ X, cplx<T>* __restric
     }
 }
 
+// X(ID, DOUBLE, H, TPL, MAXT, RADICES...): the fixed_catalog.h line kernels of these lengths.
+#define SFB_REAL_FUSED_CATALOG(X)      \
+    X(0, 0, 256, 16, 256, 16, 16)      \
+    X(1, 0, 512, 32, 256, 16, 16, 2)   \
+    X(2, 0, 1024, 64, 256, 16, 16, 4)  \
+    X(3, 0, 2048, 128, 256, 16, 16, 8) \
+    X(4, 0, 4096, 256, 256, 16, 16, 16) \
+    X(5, 1, 256, 32, 256, 8, 8, 4)     \
+    X(6, 1, 512, 64, 256, 8, 8, 8)     \
+    X(7, 1, 1024, 128, 256, 8, 8, 8, 2) \
+    X(8, 1, 2048, 256, 256, 8, 8, 8, 4)
+
+template <int... Rs>
+struct StageCount {
+    static constexpr int value = sizeof...(Rs);
+};
+
+constexpr int kMaxDevices = 64;
+
+template <class T, int N, int TPL, int MAXT, int FEAT, int... Rs>
+cudaError_t launch_fused_t(const FixedParams& p, int64_t lines, const void* in, void* out, cudaStream_t stream) {
+    auto kernel = fft_fixed_kernel<T, N, TPL, false, 1, FEAT, MAXT, 64, Rs...>;
+    const int w = p.w;
+    const size_t smem = static_cast<size_t>(w) * kpitch<T, N>() * sizeof(cplx<T>);
+    if (smem > 48 * 1024) {
+        static std::atomic<int> configured[kMaxDevices];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        if (!configured[dev].load()) {
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            if (e != cudaSuccess) return e;
+            configured[dev].store(1);
+        }
+    }
+    const int64_t grid = (lines + w - 1) / w;
+    if (grid <= 0 || grid > INT32_MAX) return cudaErrorInvalidConfiguration;
+    kernel<<<static_cast<unsigned>(grid), w * TPL, smem, stream>>>(p, static_cast<const cplx<T>*>(in),
+                                                                   static_cast<cplx<T>*>(out));
+    return cudaGetLastError();
+}
+
 int grid_for(int64_t work) {
     const int64_t blocks = (work + 255) / 256;
     return static_cast<int>(blocks < 148 * 16 ? blocks : 148 * 16);
 }
 
 }  // namespace
+
+const RealFusedEntry* find_real_fused(bool dbl, int64_t h) {
+    static const RealFusedEntry entries[] = {
+#define SFB_X(ID, DBL, H, TPL, MAXT, ...) {ID, DBL, H, TPL, MAXT, StageCount<__VA_ARGS__>::value, {__VA_ARGS__}},
+        SFB_REAL_FUSED_CATALOG(SFB_X)
+#undef SFB_X
+    };
+    for (const auto& e : entries)
+        if (e.dbl == (dbl ? 1 : 0) && e.h == h) return &e;
+    return nullptr;
+}
+
+cudaError_t launch_real_fused(const RealFusedEntry& e, bool r2c, const void* in, void* out, int64_t lines,
+                              const void* tw_real, const void* tw_base, double scale, cudaStream_t stream) {
+    if (lines <= 0) return cudaSuccess;
+    FixedParams p{};
+    p.n_cols = lines;
+    p.w = e.maxt / e.tpl > 0 ? e.maxt / e.tpl : 1;
+    p.col_tiles = (lines + p.w - 1) / p.w;
+    p.in_pitch = r2c ? e.h : e.h + 1;
+    p.out_pitch = r2c ? e.h + 1 : e.h;
+    p.tw = tw_base;
+    p.conj_in = p.conj_out = r2c ? 0 : 1;  // C2R: the unnormalized inverse as conj(FFT(conj z))
+    p.scale = scale;
+    if (r2c) p.postmul = tw_real;
+    else p.premul = tw_real;
+    switch (e.id) {
+#define SFB_X(ID, DBL, H, TPL, MAXT, ...)                                                                    \
+    case ID:                                                                                                 \
+        return r2c ? launch_fused_t<std::conditional_t<(DBL) != 0, double, float>, H, TPL, MAXT, kFeatRealPost, \
+                                    __VA_ARGS__>(p, lines, in, out, stream)                                    \
+                   : launch_fused_t<std::conditional_t<(DBL) != 0, double, float>, H, TPL, MAXT, kFeatRealPre,  \
+                                    __VA_ARGS__>(p, lines, in, out, stream);
+        SFB_REAL_FUSED_CATALOG(SFB_X)
+#undef SFB_X
+        default:
+            return cudaErrorInvalidDeviceFunction;
+    }
+}
 
 cudaError_t launch_r2c_post(bool dbl, const void* z, void* x, int64_t h, int64_t lines, const void* tw, double scale,
                             cudaStream_t stream) {

@@ -14,4 +14,18 @@ cudaError_t launch_r2c_post(bool dbl, const void* z, void* x, int64_t h, int64_t
 cudaError_t launch_c2r_pre(bool dbl, const void* x, void* z, int64_t h, int64_t lines, const void* tw, double scale,
                            cudaStream_t stream);
 
+// A half length h with a fused single-pass real kernel: the stage radices of its FFT.
+struct RealFusedEntry {
+    int id, dbl;
+    int64_t h;
+    int tpl, maxt, nstages;
+    int radices[16];
+};
+const RealFusedEntry* find_real_fused(bool dbl, int64_t h);
+// One pass per real transform: R2C reads lines x 2h reals (as h complex) and writes lines x
+// (h+1) bins; C2R the reverse. tw_real: W_2h^k, k = 0..h; tw_base: the FFT's base twiddles
+// (per stage of radix R after ns points: W_(ns*R)^jm, jm < ns), both in the plan precision.
+cudaError_t launch_real_fused(const RealFusedEntry& e, bool r2c, const void* in, void* out, int64_t lines,
+                              const void* tw_real, const void* tw_base, double scale, cudaStream_t stream);
+
 }  // namespace sfb

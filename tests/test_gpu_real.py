@@ -49,7 +49,7 @@ def spectra(n, batch, seed, dbl):
     return s.astype(np.complex128 if dbl else np.complex64)
 
 
-SIZES = [2, 8, 30, 256, 1000, 2018, 4096, 8192, 13440, 26880, 131072]
+SIZES = [2, 8, 30, 256, 512, 1000, 2018, 2048, 4096, 8192, 13440, 26880, 131072]
 
 
 @pytest.mark.parametrize("dbl", [False, True])
@@ -182,3 +182,50 @@ def test_split_precision_inner_plan(torch, sf):
     p.execute(xt, out).synchronize()
     ref = np.fft.rfft(x.astype(np.float64), axis=1).reshape(-1)
     assert rel_l2(out.cpu().numpy(), ref) <= tol(n, False)
+
+
+# half lengths with a fused one-pass kernel: 256..4096 (float), 256..2048 (double)
+FUSED = [(512, False), (2048, False), (8192, False), (512, True), (4096, True)]
+
+
+@pytest.mark.parametrize("n,dbl", FUSED)
+def test_fused_matches_two_pass(torch, sf, n, dbl, monkeypatch):
+    """The one-pass real kernels (pre-/post-process inside the size-specialised FFT) against the
+    two-pass form (complex FFT of length n/2, then the separate pass) and FP64, both kinds,
+    with a normalization and a partial batch of lines."""
+    batch = 37
+    scalar = "double" if dbl else "float"
+    opts = sf.plan_options(normalization=sf.normalization.orthogonal)
+    x = real_lines(n, batch, 3 + n, dbl)
+    s = spectra(n, batch, 5 + n, dbl)
+    outs = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("SYCLFFT_B200_REAL_FUSED", mode)
+        f = sf.plan_dft_r2c_1d(scalar, n, batch, opts)
+        b = sf.plan_dft_c2r_1d(scalar, n, batch, opts)
+        assert f.describe()["fused"] == int(mode) and b.describe()["fused"] == int(mode)
+        if mode == "1":
+            assert f.launches() == 1 and b.launches() == 1
+        spec = torch.empty(batch * (n // 2 + 1), dtype=f.dtype, device="cuda")
+        back = torch.empty(batch * n, dtype=b.real_dtype, device="cuda")
+        f.execute(torch.from_numpy(x).cuda(), spec)
+        b.execute(torch.from_numpy(s).cuda(), back).synchronize()
+        outs[mode] = (spec.cpu().numpy(), back.cpu().numpy())
+    scale = 1 / math.sqrt(n)
+    ref_f = np.fft.rfft(x.astype(np.float64), axis=1).reshape(-1) * scale
+    ref_b = (np.fft.irfft(s.astype(np.complex128), n, axis=1) * n).reshape(-1) * scale
+    for mode in ("1", "0"):
+        assert rel_l2(outs[mode][0], ref_f) <= tol(n, dbl)
+        assert rel_l2(outs[mode][1], ref_b) <= tol(n, dbl)
+    assert rel_l2(outs["1"][0], outs["0"][0]) <= tol(n, dbl)
+
+
+def test_misaligned_real_buffers_are_rejected(torch, sf):
+    n, batch = 1024, 2
+    p = sf.plan_dft_r2c_1d("float", n, batch)
+    x = torch.zeros(n * batch + 1, dtype=torch.float32, device="cuda")
+    out = torch.zeros(batch * (n // 2 + 1), dtype=torch.complex64, device="cuda")
+    with pytest.raises(sf.SyclfftError) as e:
+        p.execute(x.data_ptr() + 4, out)   # a real array starting at an odd float
+    assert e.value.code == sf.error_code.execution_failed
+    assert "aligned" in str(e.value)

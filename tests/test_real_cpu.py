@@ -92,3 +92,30 @@ def test_real_plan_argument_checks_need_no_device():
     with pytest.raises(sf.SyclfftError) as e:
         sf.RealPlan("float", 8, 1, "r2r")
     assert e.value.code == sf.error_code.invalid_argument
+
+
+def _catalog(path, macro):
+    """Entries X(...) of a catalog macro, as tuples of ints."""
+    import os
+    import re
+    src = open(os.path.join(os.path.dirname(__file__), "..", "sycl-fft_b200", "csrc", path)).read()
+    body = src[src.index("#define " + macro):]
+    body = body[: body.index("\n\n")]
+    return [tuple(int(v) for v in m.split(",")) for m in re.findall(r"X\(([-0-9, ]+)\)", body)]
+
+
+def test_fused_real_catalog_matches_the_line_kernels():
+    """Each one-pass real kernel (real_kernel.cu) is the size-specialised line kernel of its half
+    length (fixed_catalog.h, contiguous lines, plain feature): same threads per line, same
+    radices, radices multiplying to the length; its lines per CTA fit the CTA-size bound."""
+    fixed = {(e[1], e[4]): e for e in _catalog("fixed_catalog.h", "SFB_FIXED_CATALOG") if e[2] == 0 and e[3] == 0}
+    fused = _catalog("real_kernel.cu", "SFB_REAL_FUSED_CATALOG")
+    assert fused
+    for e in fused:
+        _, dbl, h, tpl, maxt, *radices = e
+        f = fixed[(dbl, h)]
+        assert (f[5], list(f[8:])) == (tpl, radices), e
+        prod = 1
+        for r in radices:
+            prod *= r
+        assert prod == h and maxt % tpl == 0 and maxt // tpl >= 1

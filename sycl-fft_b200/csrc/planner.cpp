@@ -983,6 +983,11 @@ struct Builder {
         ps.cl_n1 = ce.n1;
         ps.cl_n2 = ce.n2;
         ps.cl_p = ce.p;
+        if (req.cluster_pipe && req.dbl && L == 65536 && ce.n1 == 256 && ce.n2 == 256 && ce.p == 16 &&
+            r1 == std::vector<int>{8, 8, 4} && r2 == r1) {
+            ps.cluster_pipe = true;
+            ps.tables.cl_base = base_table(r1);
+        }
         const int cw = ce.n2 / ce.p, rw = ce.n1 / ce.p;
         ps.threads = std::max(cw * ce.tpl1, rw * ce.tpl2);
         ps.smem_bytes = L / ce.p * cs;
@@ -1275,7 +1280,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"maxv\":" << ps.kc.maxv << ",\"maxt\":" << ps.kc.maxt << ",\"src\":" << int(ps.src)
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
-           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"tma\":" << (ps.tma ? 1 : 0) << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
+           << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"tma\":" << (ps.tma ? 1 : 0) << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster_pipe\":" << (ps.cluster_pipe ? 1 : 0) << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
            << ps.cl_p << "]}";
     }
     os << "]}";

@@ -31,6 +31,7 @@ enum class Buf : int { Input = 0, Output = 1, Scratch = 2 };
 struct TableIds {
     int tw1 = -1, tw2 = -1, premul = -1, pointwise = -1, postmul = -1, tw4_hi = -1, tw4_lo = -1;
     int tc_tw = -1;  // two-level W_N^k table of the tensor-core kernel
+    int cl_base = -1;  // base twiddles of the pipelined cluster kernel's 256-point FFTs
 };
 
 struct KernelChoice {
@@ -62,6 +63,7 @@ struct PassSpec {
     bool tma = false;        // four-step column pass with a TMA-staged variant of fixed_id (tma_cols_kernel.cuh)
     int blue_id = -1;        // size-specialised Bluestein kernel (bluestein_catalog.h)
     int blue_kind = -1;      // its kind: kBlueFused / kBlueColsFwd / kBlueRowsConv / kBlueColsInv
+    bool cluster_pipe = false;  // cluster pass on the pipelined 16-CTA kernel (cluster_pipe.cu)
 };
 
 // One entry of cluster_catalog.h as seen by the host.
@@ -133,6 +135,9 @@ struct PlanRequest {
     // bit ax set: axis ax is an index of the batch, not transformed (interleaved-batch layouts:
     // transforms down the columns of a dense array run as the other axes' passes alone)
     uint32_t skip_axes = 0;
+    // complex<double> 65536-point lines: the cluster pass (cluster_p = 16) on the pipelined
+    // cluster kernel (opt-in)
+    bool cluster_pipe = false;
 };
 
 // A Bluestein axis whose chirp and chirp spectrum the provider generates on the device

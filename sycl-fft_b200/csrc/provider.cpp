@@ -31,6 +31,7 @@
 #include "tma_launch.hpp"
 #include "real_launch.hpp"
 #include "layout_launch.hpp"
+#include "cluster_pipe.hpp"
 #include "bluestein_launch.hpp"
 #include "planner.hpp"
 
@@ -79,6 +80,7 @@ struct BoundPass {
     ClusterParams cp;  // used when spec.cluster_id >= 0
     PipedParams pp;    // used when spec.piped_id >= 0 and the buffers are 16-byte aligned
     TcParams tp;       // used when spec.tc_id >= 0
+    ClusterPipeParams kp;  // used when spec.cluster_pipe and the buffers are 16-byte aligned
 };
 
 TcParams to_tc(const PassParams& p, const void* tw, int* status) {
@@ -325,9 +327,16 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags, 
     // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
     if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
     // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
+    // =pipe: complex<double> 65536-point lines on the pipelined 16-CTA cluster kernel.
     if (const char* k = std::getenv("SYCLFFT_B200_CLUSTER")) {
-        if (std::strcmp(k, "off") == 0) req.no_cluster = true;
-        else req.cluster_p = std::atoi(k);
+        if (std::strcmp(k, "off") == 0) {
+            req.no_cluster = true;
+        } else if (std::strcmp(k, "pipe") == 0) {
+            req.cluster_p = 16;
+            req.cluster_pipe = true;
+        } else {
+            req.cluster_p = std::atoi(k);
+        }
     }
 
     int device = cfg.device;
@@ -423,6 +432,19 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         bp.p.tw4_lo = tab(ps.tables.tw4_lo);
         bp.fp = to_fixed(bp.p);
         bp.cp = to_cluster(bp.p);
+        if (ps.cluster_pipe) {
+            bp.kp.lines = bp.p.n_cols;
+            bp.kp.in_pitch = bp.p.in.cs;
+            bp.kp.out_pitch = bp.p.out.cs;
+            bp.kp.tw_base = tab(ps.tables.cl_base);
+            bp.kp.tw4_hi = bp.p.tw4_hi;
+            bp.kp.tw4_lo = bp.p.tw4_lo;
+            bp.kp.tw4_shift = bp.p.tw4_shift;
+            bp.kp.conj_in = bp.p.conj_in;
+            bp.kp.conj_out = bp.p.conj_out;
+            bp.kp.scale = bp.p.scale;
+            bp.kp.status = plan->status;
+        }
         bp.pp = to_piped(bp.p, plan->status);
         bp.tp = to_tc(bp.p, tab(ps.tables.tc_tw), plan->status);
         plan->passes.push_back(bp);
@@ -444,6 +466,7 @@ BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
     r.fp.n_cols = p.n_cols;
     r.fp.col_tiles = p.col_tiles;
     r.cp.lines = p.n_cols;
+    r.kp.lines = p.n_cols;
     r.pp.lines = p.n_cols;
     r.tp.n_outer = p.n_outer;
     r.tp.n_cols = p.n_cols;
@@ -474,6 +497,7 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
             bp.p.conj_in ^= 1;
             bp.fp.conj_in ^= 1;
             bp.cp.conj_in ^= 1;
+            bp.kp.conj_in ^= 1;
             bp.pp.conj_in ^= 1;
             bp.tp.conj_in ^= 1;
         }
@@ -481,12 +505,13 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
             bp.p.conj_out ^= 1;
             bp.fp.conj_out ^= 1;
             bp.cp.conj_out ^= 1;
+            bp.kp.conj_out ^= 1;
             bp.pp.conj_out ^= 1;
             bp.tp.conj_out ^= 1;
         }
     }
     if (last_pass && set_scale) {
-        bp.p.scale = bp.fp.scale = bp.cp.scale = bp.pp.scale = scale;
+        bp.p.scale = bp.fp.scale = bp.cp.scale = bp.kp.scale = bp.pp.scale = scale;
         bp.tp.scale = static_cast<float>(scale);
     }
 }
@@ -812,6 +837,8 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
         const int64_t lines = bp.pp.lines;
         const int grid = static_cast<int>(lines < plan->sms ? lines : plan->sms);
         check(launch_piped(ps.piped_id, bp.pp, grid, src, dst, stream), "FFT pipelined pass launch");
+    } else if (ps.cluster_pipe && aligned) {
+        check(launch_cluster_pipe(bp.kp, src, dst, stream), "FFT pipelined cluster pass launch");
     } else if (ps.cluster_id >= 0) {
         check(launch_cluster(ps.cluster_id, bp.cp, src, dst, stream), "FFT cluster pass launch");
     } else if (ps.tma && aligned && launch_tma(plan, bp, src, dst, stream)) {
@@ -907,6 +934,7 @@ std::string tune_key(const PlanRequest& r, int device) {
       << "|b" << r.batch;
     for (auto v : r.shape) k << "|" << v;
     if (r.skip_axes) k << "|skip" << r.skip_axes;
+    if (r.cluster_pipe) k << "|cpipe";
     return k.str();
 }
 

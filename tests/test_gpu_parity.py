@@ -345,3 +345,19 @@ def test_tma_staged_column_pass(shape, batch, dbl, monkeypatch):
         ref = fp64_fft(x, shape, batch, int(d))
         tol = (1e-12 if dbl else 1e-5) * math.log2(n)
         assert rel_l2(out.cpu().numpy(), ref) <= tol
+
+
+@pytest.mark.parametrize("in_place", [False, True])
+def test_pipelined_cluster_kernel(sf, torch, in_place, monkeypatch):
+    """complex<double> 65536-point lines in one pass on 16-CTA clusters (opt-in
+    SYCLFFT_B200_CLUSTER=pipe): both directions and a normalization against FP64, more lines than
+    resident clusters so every cluster walks several lines."""
+    monkeypatch.setenv("SYCLFFT_B200_CLUSTER", "pipe")
+    n, batch = 65536, 37
+    x = uniform_complex(n * batch, 65, np.complex128)
+    for d, norm in ((-1, 0), (1, 3)):
+        out, p = run(sf, torch, x, [n], batch, d, norm, True, in_place)
+        passes = p.describe()["passes"]
+        assert len(passes) == 1 and passes[0]["cluster_pipe"] == 1, passes
+        ref = fp64_fft(x, [n], batch, d, norm_scale(norm, d, n))
+        assert rel_l2(out, ref) <= spec_tol(n, True)

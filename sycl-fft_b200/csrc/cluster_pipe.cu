@@ -177,21 +177,37 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 constexpr int kMaxDevices = 64;
 
-cudaError_t configure(int* clusters_out) {
-    static std::atomic<int> configured[kMaxDevices];
+// Sets the kernel's attributes once per device and returns how many of its clusters fit the
+// device at once (cached per device; 0 until known).
+cudaError_t configure(int* resident) {
+    static std::atomic<int> clusters[kMaxDevices];
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!configured[dev].load()) {
+    int known = clusters[dev].load();
+    if (known <= 0) {
         e = cudaFuncSetAttribute(fft_cluster_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(kSmemBytes));
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(fft_cluster_pipe_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         if (e != cudaSuccess) return e;
-        configured[dev].store(1);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(kP, 1, 1);
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = kSmemBytes;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = kP;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaOccupancyMaxActiveClusters(&known, fft_cluster_pipe_kernel, &cfg);
+        if (e != cudaSuccess) return e;
+        clusters[dev].store(known);
     }
-    (void)clusters_out;
+    *resident = known;
     return cudaSuccess;
 }
 
@@ -199,8 +215,13 @@ cudaError_t configure(int* clusters_out) {
 
 cudaError_t launch_cluster_pipe(const ClusterPipeParams& prm, const void* in, void* out, cudaStream_t stream,
                                 int* max_clusters) {
-    cudaError_t e = configure(nullptr);
+    int clusters = 0;
+    cudaError_t e = configure(&clusters);
     if (e != cudaSuccess) return e;
+    if (max_clusters) {
+        *max_clusters = clusters;
+        return cudaSuccess;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.blockDim = dim3(kThreads, 1, 1);
     cfg.dynamicSmemBytes = kSmemBytes;
@@ -212,14 +233,6 @@ cudaError_t launch_cluster_pipe(const ClusterPipeParams& prm, const void* in, vo
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cfg.gridDim = dim3(kP, 1, 1);
-    int clusters = 0;
-    e = cudaOccupancyMaxActiveClusters(&clusters, fft_cluster_pipe_kernel, &cfg);
-    if (e != cudaSuccess) return e;
-    if (max_clusters) {
-        *max_clusters = clusters;
-        return cudaSuccess;
-    }
     if (clusters <= 0) return cudaErrorInvalidConfiguration;
     if (prm.lines <= 0) return cudaSuccess;
     const int64_t use = prm.lines < clusters ? prm.lines : clusters;

@@ -234,6 +234,10 @@ public:
           options_(opts) {
         if (direction_ != syclfft_b200::direction::forward && direction_ != syclfft_b200::direction::backward)
             throw exception(error_code::invalid_argument, "Invalid FFT direction");
+        // argument errors come before provider selection and device work, as the element count's
+        std::optional<syclfft_b200_layout_v1> lay;
+        if (layout)
+            lay = detail::checked_layout(*layout, lengths_, batch_count_, options_.placement == placement::in_place);
         if (options_.preferred_provider != provider::automatic && options_.preferred_provider != provider::b200) {
             throw exception(error_code::provider_unavailable,
                             std::string(detail::provider_name(options_.preferred_provider)) +
@@ -260,14 +264,12 @@ public:
         config.normalization = static_cast<uint32_t>(options_.normalization);
         config.measure = options_.planning == planning_mode::measure ? 1 : 0;
         config.device = queue_.device;
-        if (layout) {
-            const syclfft_b200_layout_v1 lay = detail::checked_layout(*layout, lengths_, batch_count_,
-                                                                      options_.placement == placement::in_place);
+        if (lay) {
             if (!module_.create_strided)
                 throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_strided");
             uint32_t flags = SYCLFFT_B200_CREATE_SYNC;
             if (options_.split_precision && std::is_same_v<Scalar, float>) flags |= SYCLFFT_B200_CREATE_SPLIT_BF16;
-            handle_ = module_.create_strided(&config, &lay, flags, error.data(), error.size());
+            handle_ = module_.create_strided(&config, &*lay, flags, error.data(), error.size());
         } else if (options_.split_precision && std::is_same_v<Scalar, float>) {
             if (!module_.create_ex)
                 throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_ex");

@@ -50,6 +50,47 @@ try {
             return 1;
         }
     }
+    if (mode == "argument-checks") {
+        // argument errors of the B200 extensions come before provider and device work
+        int failures = 0;
+        auto expect_invalid = [&](const char* what, auto&& fn) {
+            try {
+                fn();
+                std::cerr << what << ": accepted\n";
+                ++failures;
+            } catch (const sf::exception& ex) {
+                if (ex.code() != sf::error_code::invalid_argument) {
+                    std::cerr << what << ": " << ex.what() << '\n';
+                    ++failures;
+                }
+            }
+        };
+        expect_invalid("odd real length", [] { (void)sf::plan_dft_r2c_1d<float>(sf::queue{}, 7); });
+        expect_invalid("in-place real plan", [] {
+            sf::plan_options o;
+            o.placement = sf::placement::in_place;
+            (void)sf::plan_dft_c2r_1d<double>(sf::queue{}, 8, 1, o);
+        });
+        expect_invalid("overlapping output layout", [] {
+            (void)sf::plan_many_dft<float>(sf::queue{}, {8}, 3, sf::direction::forward, sf::plan_options{},
+                                           sf::data_layout{{1}, 8, {1}, 4});
+        });
+        expect_invalid("one stride for two axes", [] {
+            (void)sf::plan_many_dft<float>(sf::queue{}, {8, 8}, 2, sf::direction::forward, sf::plan_options{},
+                                           sf::data_layout{{8}, 64, {8, 1}, 64});
+        });
+        expect_invalid("zero stride", [] {
+            (void)sf::plan_many_dft<double>(sf::queue{}, {8}, 2, sf::direction::forward, sf::plan_options{},
+                                            sf::data_layout{{0}, 8, {1}, 8});
+        });
+        expect_invalid("in place with two layouts", [] {
+            sf::plan_options o;
+            o.placement = sf::placement::in_place;
+            (void)sf::plan_many_dft<float>(sf::queue{}, {8}, 4, sf::direction::forward, o,
+                                           sf::data_layout{{1}, 8, {4}, 1});
+        });
+        return failures == 0 ? 0 : 1;
+    }
     std::cerr << "unknown mode\n";
     return 1;
 } catch (const std::exception& ex) {

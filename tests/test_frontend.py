@@ -37,6 +37,13 @@ def test_module_without_entry_point_is_skipped():
     assert r.returncode == 0, r.stderr
 
 
+def test_extension_argument_checks_need_no_device():
+    """Real-transform and strided-layout argument errors (C++ front end) are invalid_argument,
+    raised before the provider is loaded or a device is touched."""
+    r = run(["plugin_tests", "argument-checks"], {"SYCLFFT_PLUGIN_PATH": ""})
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 @pytest.mark.gpu
 def test_reference_test_program_on_b200():
     r = run(["frontend_tests"], {"SYCLFFT_PLUGIN_PATH": ""})

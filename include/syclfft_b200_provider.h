@@ -111,12 +111,15 @@ SYCLFFT_B200_EXPORT const char *syclfft_b200_version(void);
 SYCLFFT_B200_EXPORT void *syclfft_b200_create_ex(const syclfft_b200_plan_config_v1 *config, uint32_t flags, char *err,
                                                  size_t cap);
 /* Real transforms (no counterpart in the reference, whose v0.1 scope is complex-to-complex):
- * one-dimensional batched, out of place, even length N = lengths[0]. R2C (direction -1):
- * N reals per line in, N/2 + 1 complex per line out; C2R (direction +1): N/2 + 1 complex in
- * (imaginary parts of the first and last bins ignored), N reals out. Computed as a complex
- * FFT of length N/2 plus one post- / pre-process pass; normalization as for complex plans,
- * relative to N. The handle is used with the provider's execute/destroy, execute_batch and
- * execute_ex (normalization only), describe_plan and plan_launches. */
+ * rank 1-3, batched, out of place, even last length N = lengths[rank-1] (numpy's rfftn /
+ * irfftn layouts). R2C (direction -1): prod(lengths) reals per transform in,
+ * prod(lengths[0..rank-2]) x (N/2 + 1) complex out; C2R (direction +1) the reverse, the
+ * imaginary parts of bins 0 and N/2 of every last-axis line ignored. The last axis is a
+ * complex FFT of length N/2 plus a pre- / post-process (fused into one pass where N/2 has a
+ * size-specialised kernel); the outer axes are complex FFTs of the spectrum. Normalization as
+ * for complex plans, relative to prod(lengths). The handle is used with the provider's
+ * execute/destroy, execute_batch and execute_ex (normalization only), describe_plan and
+ * plan_launches. */
 #define SYCLFFT_B200_REAL_R2C 1
 #define SYCLFFT_B200_REAL_C2R 2
 SYCLFFT_B200_EXPORT void *syclfft_b200_create_real(const syclfft_b200_plan_config_v1 *config, int32_t kind,

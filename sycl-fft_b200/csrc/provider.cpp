@@ -202,6 +202,13 @@ struct DevicePlan {
     void* real_tw = nullptr;        // W_N^k, k = 0..N/2 (then the fused kernel's base twiddles)
     const RealFusedEntry* real_fused = nullptr;  // one-pass kernel for N/2 (real_kernel.cu), or none
     int64_t real_base_off = 0;      // complex elements from real_tw to the base twiddles
+    // Real transforms of rank 2-3: `inner` is the 1D real plan of the last axis over every outer
+    // line, `outer` the complex plan over the outer axes (last axis untransformed), md_buf the
+    // C2R intermediate (batch x outer lines x (N/2+1) complex).
+    bool real_md = false;
+    int64_t real_outer = 1;
+    std::unique_ptr<DevicePlan> outer;
+    void* md_buf = nullptr;
     // Strided layouts (syclfft_b200_create_strided): the contiguous plan `inner` with gather /
     // scatter passes (layout_kernel.cu) on the sides that are not contiguous.
     bool strided = false;
@@ -226,6 +233,7 @@ struct DevicePlan {
             if (real_buf) cudaFreeAsync(real_buf, ms);
             if (real_tw) cudaFreeAsync(real_tw, ms);
             if (pack_buf) cudaFreeAsync(pack_buf, ms);
+            if (md_buf) cudaFreeAsync(md_buf, ms);
         } else {
             if (done) cudaEventSynchronize(done);
             if (scratch) cudaFree(scratch);
@@ -233,6 +241,7 @@ struct DevicePlan {
             if (real_buf) cudaFree(real_buf);
             if (real_tw) cudaFree(real_tw);
             if (pack_buf) cudaFree(pack_buf);
+            if (md_buf) cudaFree(md_buf);
         }
         if (done) cudaEventDestroy(done);
         if (ready) cudaEventDestroy(ready);
@@ -517,7 +526,7 @@ void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double
 }
 
 // Real transform of even length N over a complex plan of length N/2 (see real_kernel.cu).
-DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, uint32_t flags) {
+DevicePlan* create_real_plan_1d(const syclfft_b200_plan_config_v1& cfg, int kind, uint32_t flags) {
     if (kind != SYCLFFT_B200_REAL_R2C && kind != SYCLFFT_B200_REAL_C2R)
         throw std::invalid_argument("real transform kind must be R2C or C2R");
     if (cfg.rank != 1) throw std::invalid_argument("real transforms are one-dimensional (batched)");
@@ -585,6 +594,76 @@ DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, u
     check(cudaStreamSynchronize(ms), "real plan tables");
     check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
     plan->inner = std::move(inner);
+    return plan.release();
+}
+
+// Real transforms of rank 1-3 over the last axis (even length N): R2C is the 1D real plan of the
+// last axis over every outer line, then the complex FFT over the outer axes of the
+// [outer.., N/2+1] spectrum in place (numpy.fft.rfftn's order); C2R runs the inverse complex
+// FFT over the outer axes into a scratch spectrum first, then the 1D C2R of the last axis
+// (numpy.fft.irfftn's order: the imaginary parts of bins 0 and N/2 are dropped per line).
+// The normalization is relative to the whole transform size and applied by the last-axis pass.
+DevicePlan* create_real_plan(const syclfft_b200_plan_config_v1& cfg, int kind, uint32_t flags) {
+    if (cfg.rank == 0 || cfg.rank > 3) throw std::invalid_argument("FFT rank must be between 1 and 3");
+    if (cfg.rank == 1) return create_real_plan_1d(cfg, kind, flags);
+    if (kind != SYCLFFT_B200_REAL_R2C && kind != SYCLFFT_B200_REAL_C2R)
+        throw std::invalid_argument("real transform kind must be R2C or C2R");
+    const uint32_t r = cfg.rank;
+    for (uint32_t k = 0; k < r; ++k)
+        if (cfg.lengths[k] == 0) throw std::invalid_argument("FFT dimensions must be non-zero");
+    if (cfg.batch_count == 0) throw std::invalid_argument("FFT batch count must be non-zero");
+    const uint64_t n = cfg.lengths[r - 1];
+    if (n < 2 || n % 2) throw std::invalid_argument("real transforms need an even last length >= 2");
+    if (cfg.in_place) throw std::invalid_argument("real transforms are out of place");
+    const int dir = kind == SYCLFFT_B200_REAL_R2C ? -1 : 1;
+    if (cfg.direction != dir)
+        throw std::invalid_argument(dir < 0 ? "R2C transforms are forward" : "C2R transforms are backward");
+    if (cfg.normalization > 3) throw std::invalid_argument("Invalid normalization");
+    uint64_t outer = 1;
+    for (uint32_t k = 0; k + 1 < r; ++k) outer *= cfg.lengths[k];
+    const uint64_t h = n / 2 + 1;
+    // last axis: one line per (batch, outer index), scaled for the whole transform
+    syclfft_b200_plan_config_v1 c1 = cfg;
+    c1.rank = 1;
+    c1.lengths[0] = n;
+    c1.lengths[1] = c1.lengths[2] = 0;
+    c1.batch_count = cfg.batch_count * outer;
+    std::unique_ptr<DevicePlan> last(create_real_plan_1d(c1, kind, flags));
+    last->spec.transform_size = n * outer;
+    // outer axes of the [outer.., N/2+1] spectrum, the last axis left untransformed
+    syclfft_b200_plan_config_v1 co = cfg;
+    co.lengths[r - 1] = h;
+    co.normalization = 0;
+    co.in_place = kind == SYCLFFT_B200_REAL_R2C ? 1 : 0;
+    std::unique_ptr<DevicePlan> outer_plan(create_plan(co, flags | SYCLFFT_B200_CREATE_SYNC, 1u << (r - 1)));
+    auto plan = std::make_unique<DevicePlan>();
+    plan->device = last->device;
+    plan->sms = last->sms;
+    plan->spec.req = last->spec.req;
+    plan->spec.req.shape.assign(cfg.lengths, cfg.lengths + r);
+    plan->spec.req.batch = cfg.batch_count;
+    plan->spec.req.direction = dir;
+    plan->spec.req.normalization = static_cast<int>(cfg.normalization);
+    plan->spec.transform_size = n * outer;
+    plan->spec.elements = n * outer * cfg.batch_count;
+    plan->status = last->status;
+    plan->real_kind = kind;
+    plan->real_n = static_cast<int64_t>(n);
+    plan->real_md = true;
+    plan->real_outer = static_cast<int64_t>(outer);
+    const size_t cs = plan->spec.req.dbl ? 16 : 8;
+    const uint64_t spec_elems = cfg.batch_count * outer * h;
+    plan->spec.scratch_elements = last->spec.scratch_elements + outer_plan->spec.scratch_elements +
+                                  (kind == SYCLFFT_B200_REAL_C2R ? spec_elems : 0);
+    DeviceGuard guard(plan->device);
+    if (kind == SYCLFFT_B200_REAL_C2R) {
+        cudaStream_t ms = memory_stream(plan->device);
+        check(cudaMallocAsync(&plan->md_buf, spec_elems * cs, ms), "cudaMallocAsync(real spectrum scratch)");
+        check(cudaStreamSynchronize(ms), "real spectrum scratch");
+    }
+    check(cudaEventCreateWithFlags(&plan->done, cudaEventDisableTiming), "cudaEventCreate");
+    plan->inner = std::move(last);
+    plan->outer = std::move(outer_plan);
     return plan.release();
 }
 
@@ -768,6 +847,24 @@ void execute_real(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     if (in == out) throw std::invalid_argument("Out-of-place plan requires distinct allocations");
     const int dir = plan->spec.req.direction;
     if (direction != 0 && direction != dir) throw std::invalid_argument("a real plan runs in its own direction");
+    if (plan->real_md) {
+        std::lock_guard<std::mutex> lock(plan->mu);
+        DeviceGuard guard(plan->device);
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+        const uint64_t lines = batch * static_cast<uint64_t>(plan->real_outer);
+        if (plan->real_kind == SYCLFFT_B200_REAL_R2C) {
+            execute_real(plan->inner.get(), in, out, stream, lines, 0, normalization);
+            execute_plan(plan->outer.get(), out, out, stream, batch, 0, -1);
+        } else {
+            execute_plan(plan->outer.get(), in, plan->md_buf, stream, batch, 0, -1);
+            execute_real(plan->inner.get(), plan->md_buf, out, stream, lines, 0, normalization);
+        }
+        check(cap != cudaStreamCaptureStatusNone ? cudaEventRecordWithFlags(plan->done, stream, cudaEventRecordExternal)
+                                                 : cudaEventRecord(plan->done, stream),
+              "cudaEventRecord");
+        return;
+    }
     const int norm = normalization < 0 ? plan->spec.req.normalization : normalization;
     const double scale = normalization_scale(norm, dir, plan->spec.transform_size);
     std::lock_guard<std::mutex> lock(plan->mu);
@@ -1134,7 +1231,16 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
     if (!p || !buf || cap == 0) return -1;
     std::string s;
-    if (p->real_kind) {
+    if (p && p->real_md) {
+        std::string shape;
+        for (size_t k = 0; k < p->spec.req.shape.size(); ++k)
+            shape += (k ? "," : "") + std::to_string(p->spec.req.shape[k]);
+        const sfb::DevicePlan* last = p->inner.get();
+        s = std::string("{\"real\":\"") + (p->real_kind == SYCLFFT_B200_REAL_R2C ? "r2c" : "c2r") +
+            "\",\"n\":" + std::to_string(p->real_n) + ",\"shape\":[" + shape + "],\"fused\":" +
+            (last->real_fused ? "1" : "0") + ",\"inner\":" + sfb::describe_plan(last->inner->spec) +
+            ",\"outer\":" + sfb::describe_plan(p->outer->spec) + "}";
+    } else if (p->real_kind) {
         // a real plan: its complex plan of half the length and the pre-/post-process pass
         s = std::string("{\"real\":\"") + (p->real_kind == SYCLFFT_B200_REAL_R2C ? "r2c" : "c2r") +
             "\",\"n\":" + std::to_string(p->real_n) + ",\"fused\":" + (p->real_fused ? "1" : "0") +
@@ -1158,6 +1264,11 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
+    if (p && p->real_md) {
+        const sfb::DevicePlan* last = p->inner.get();
+        return (last->real_fused ? 1 : static_cast<int>(last->inner->passes.size()) + 1) +
+               static_cast<int>(p->outer->passes.size());
+    }
     if (p && p->real_kind) return p->real_fused ? 1 : static_cast<int>(p->inner->passes.size()) + 1;
     if (p && p->strided)
         return static_cast<int>(p->inner->passes.size()) +

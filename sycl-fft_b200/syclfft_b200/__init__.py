@@ -20,7 +20,9 @@ from .api import (  # noqa: F401
     plan_dft_1d,
     plan_dft_2d,
     plan_dft_3d,
+    plan_dft_c2r,
     plan_dft_c2r_1d,
+    plan_dft_r2c,
     plan_dft_r2c_1d,
     plan_many_dft,
     plan_options,
@@ -32,6 +34,6 @@ from . import _provider  # noqa: F401
 
 __all__ = [
     "Plan", "RealPlan", "SyclfftError", "data_layout", "direction", "error_code", "normalization", "placement", "plan_dft_1d",
-    "plan_dft_2d", "plan_dft_3d", "plan_dft_r2c_1d", "plan_dft_c2r_1d", "plan_many_dft", "plan_options", "planning_mode", "provider",
+    "plan_dft_2d", "plan_dft_3d", "plan_dft_r2c_1d", "plan_dft_c2r_1d", "plan_dft_r2c", "plan_dft_c2r", "plan_many_dft", "plan_options", "planning_mode", "provider",
     "query_providers",
 ]

@@ -334,26 +334,26 @@ class Plan:
 
 
 class RealPlan(Plan):
-    """Batched one-dimensional real transform of even length n (B200 extension; the reference's
-    plan API is complex-to-complex only). kind "r2c": forward, n reals per line in, n/2 + 1
-    complex per line out. kind "c2r": backward, n/2 + 1 complex per line in (imaginary parts of
-    bins 0 and n/2 ignored, as numpy.fft.irfft does), n reals out. Out of place only; the
-    normalization option scales relative to n exactly as for a complex plan of length n.
+    """Batched real transform of rank 1-3 with an even last length n (B200 extension; the
+    reference's plan API is complex-to-complex only), in numpy's rfftn / irfftn layouts.
+    kind "r2c": forward, prod(shape) reals per transform in, prod(shape[:-1]) x (n/2 + 1)
+    complex out. kind "c2r": backward, the reverse (imaginary parts of bins 0 and n/2 of every
+    last-axis line ignored, as numpy.fft.irfftn does). Out of place only; the normalization
+    option scales relative to prod(shape) exactly as for a complex plan of that shape.
     Buffers are float32/float64 and complex64/complex128 tensors (or raw device pointers)."""
 
-    def __init__(self, scalar: str, n: int, batch_count: int, kind: str, options: plan_options | None = None,
+    def __init__(self, scalar: str, n, batch_count: int, kind: str, options: plan_options | None = None,
                  device: int | None = None):
         options = options or plan_options()
         if scalar not in ("float", "double"):
             raise SyclfftError(error_code.unsupported_precision, "syclfft supports float and double precision")
         if kind not in ("r2c", "c2r"):
             raise SyclfftError(error_code.invalid_argument, "real transform kind must be 'r2c' or 'c2r'")
-        n = int(n)
-        self._lengths = [n]
+        self._lengths = [int(v) for v in n] if isinstance(n, (list, tuple)) else [int(n)]
         self._batch = int(batch_count)
         self._elements = _checked_element_count(self._lengths, self._batch)
-        if n % 2:
-            raise SyclfftError(error_code.invalid_argument, "real transforms need an even length")
+        if self._lengths[-1] % 2:
+            raise SyclfftError(error_code.invalid_argument, "real transforms need an even last length")
         if options.placement != placement.out_of_place:
             raise SyclfftError(error_code.invalid_argument, "real transforms are out of place")
         self._kind = kind
@@ -400,9 +400,12 @@ class RealPlan(Plan):
 
     def _layout(self, name):
         """(dtype, elements) of the input or output buffer."""
-        n, b = self._lengths[0], self._batch
-        real = (self.real_dtype, n * b)
-        spec = (self.dtype, (n // 2 + 1) * b)
+        n, b = self._lengths[-1], self._batch
+        outer = 1
+        for v in self._lengths[:-1]:
+            outer *= v
+        real = (self.real_dtype, outer * n * b)
+        spec = (self.dtype, outer * (n // 2 + 1) * b)
         if self._kind == "r2c":
             return real if name == "input" else spec
         return spec if name == "input" else real
@@ -434,6 +437,18 @@ class RealPlan(Plan):
 def plan_dft_r2c_1d(scalar, n, batch_count=1, options=None, device=None) -> RealPlan:
     """Forward real-to-complex transform(s) of length n: n reals -> n/2 + 1 complex per line."""
     return RealPlan(scalar, n, batch_count, "r2c", options, device)
+
+
+def plan_dft_r2c(scalar, lengths, batch_count=1, options=None, device=None) -> RealPlan:
+    """Forward real-to-complex transform(s) of shape `lengths` (rank 1-3, even last length), as
+    numpy.fft.rfftn over the shape's axes."""
+    return RealPlan(scalar, list(lengths), batch_count, "r2c", options, device)
+
+
+def plan_dft_c2r(scalar, lengths, batch_count=1, options=None, device=None) -> RealPlan:
+    """Backward complex-to-real transform(s) to shape `lengths`, as numpy.fft.irfftn (times the
+    transform size unless a normalization option scales it)."""
+    return RealPlan(scalar, list(lengths), batch_count, "c2r", options, device)
 
 
 def plan_dft_c2r_1d(scalar, n, batch_count=1, options=None, device=None) -> RealPlan:

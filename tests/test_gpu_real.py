@@ -229,3 +229,42 @@ def test_misaligned_real_buffers_are_rejected(torch, sf):
         p.execute(x.data_ptr() + 4, out)   # a real array starting at an odd float
     assert e.value.code == sf.error_code.execution_failed
     assert "aligned" in str(e.value)
+
+
+MULTI = [([8, 64], 3, False, 0), ([16, 12, 10], 2, True, 3), ([32, 8192], 2, False, 1),
+         ([64, 512], 4, True, 2), ([5, 6, 4], 1, False, 0), ([30, 1000], 3, False, 3)]
+
+
+@pytest.mark.parametrize("shape,batch,dbl,norm", MULTI, ids=str)
+def test_multidimensional_real_transforms(torch, sf, shape, batch, dbl, norm):
+    """rfftn / irfftn over 2D and 3D shapes (last axis fused or two-pass, outer axes on the
+    strided complex kernels) against numpy in FP64, then the C2R of the R2C result."""
+    total = math.prod(shape)
+    axes = tuple(range(1, len(shape) + 1))
+    spec_shape = shape[:-1] + [shape[-1] // 2 + 1]
+    scalar = "double" if dbl else "float"
+    opts = sf.plan_options(normalization=sf.normalization(norm))
+    f = sf.plan_dft_r2c(scalar, shape, batch, opts)
+    b = sf.plan_dft_c2r(scalar, shape, batch, opts)
+    d = f.describe()
+    assert d["shape"] == shape and "outer" in d
+    rng = np.random.default_rng(total + batch)
+    x = rng.uniform(-1, 1, [batch] + shape).astype(np.float64 if dbl else np.float32)
+    xt = torch.from_numpy(x).cuda()
+    spec = torch.empty(batch * math.prod(spec_shape), dtype=f.dtype, device="cuda")
+    back = torch.empty_like(xt)
+    b.execute(spec, back, dependencies=[f.execute(xt, spec)]).synchronize()
+    sf_ = scale_of(norm, -1, total)
+    sb_ = scale_of(norm, 1, total)
+    ref = np.fft.rfftn(x.astype(np.float64), axes=axes) * sf_
+    tol_ = (1e-12 if dbl else 1e-5) * max(1.0, math.log2(total))
+    assert rel_l2(spec.cpu().numpy(), ref.reshape(-1)) <= tol_
+    want = x.astype(np.float64) * total * sf_ * sb_
+    assert rel_l2(back.cpu().numpy(), want.reshape(-1)) <= 2 * tol_
+    # C2R of an arbitrary spectrum (imaginary parts at bins 0 and n/2 ignored) against irfftn
+    s = (rng.uniform(-1, 1, [batch] + spec_shape) + 1j * rng.uniform(-1, 1, [batch] + spec_shape))
+    s = s.astype(np.complex128 if dbl else np.complex64)
+    out = torch.empty_like(xt)
+    b.execute(torch.from_numpy(s).cuda(), out).synchronize()
+    ref_b = np.fft.irfftn(s.astype(np.complex128), s=shape, axes=axes) * total * sb_
+    assert rel_l2(out.cpu().numpy(), ref_b.reshape(-1)) <= tol_

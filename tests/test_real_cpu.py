@@ -119,3 +119,15 @@ def test_fused_real_catalog_matches_the_line_kernels():
         for r in radices:
             prod *= r
         assert prod == h and maxt % tpl == 0 and maxt // tpl >= 1
+
+
+def test_multidimensional_real_plan_argument_checks():
+    with pytest.raises(sf.SyclfftError) as e:
+        sf.plan_dft_r2c("float", [4, 7])            # odd last length
+    assert e.value.code == sf.error_code.invalid_argument
+    with pytest.raises(sf.SyclfftError) as e:
+        sf.plan_dft_c2r("double", [2, 2, 2, 2])     # rank 4
+    assert e.value.code == sf.error_code.invalid_argument
+    with pytest.raises(sf.SyclfftError) as e:
+        sf.plan_dft_r2c("float", [0, 8])
+    assert e.value.code == sf.error_code.invalid_argument

@@ -155,10 +155,12 @@ private:
 };
 
 // B200 extension, no counterpart in the reference (its v0.1 scope is complex-to-complex):
-// batched one-dimensional real transforms of even length n, out of place. r2c (forward): n
-// reals per transform in, n/2 + 1 complex out. c2r (backward): n/2 + 1 complex in (the
-// imaginary parts of bins 0 and n/2 are ignored), n reals out. plan_options::normalization
-// scales relative to n as for a complex plan of length n; placement must be out_of_place.
+// batched real transforms of rank 1-3 with an even last length n, out of place, in numpy's
+// rfftn / irfftn layouts. r2c (forward): prod(shape) reals per transform in,
+// prod(shape[0..rank-2]) x (n/2 + 1) complex out. c2r (backward): the reverse (the imaginary
+// parts of bins 0 and n/2 of every last-axis line are ignored). plan_options::normalization
+// scales relative to prod(shape) as for a complex plan of that shape; placement must be
+// out_of_place.
 template <class Scalar>
 class SYCLFFT_B200_CXX_EXPORT real_plan {
     static_assert(std::is_same_v<Scalar, float> || std::is_same_v<Scalar, double>,
@@ -179,11 +181,14 @@ public:
     // c2r plans (invalid_argument on an r2c plan)
     event execute(const complex_type* input, Scalar* output, const std::vector<event>& dependencies = {});
 
-    [[nodiscard]] std::size_t length() const noexcept;
+    [[nodiscard]] std::size_t length() const noexcept;  // the last (real) length n
+    [[nodiscard]] std::vector<std::size_t> shape() const;
     [[nodiscard]] std::size_t batch_count() const noexcept;
     [[nodiscard]] real_kind kind() const noexcept;
 
     real_plan(queue q, std::size_t n, std::size_t batch_count, real_kind kind, plan_options options);
+    real_plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, real_kind kind,
+              plan_options options);
 
 private:
     class impl;
@@ -219,6 +224,18 @@ real_plan<Scalar> plan_dft_r2c_1d(queue q, std::size_t n, std::size_t batch_coun
 template <class Scalar>
 real_plan<Scalar> plan_dft_c2r_1d(queue q, std::size_t n, std::size_t batch_count = 1, plan_options options = {}) {
     return real_plan<Scalar>(q, n, batch_count, real_kind::c2r, options);
+}
+
+template <class Scalar>
+real_plan<Scalar> plan_dft_r2c(queue q, const std::vector<std::size_t>& lengths, std::size_t batch_count = 1,
+                               plan_options options = {}) {
+    return real_plan<Scalar>(q, lengths, batch_count, real_kind::r2c, options);
+}
+
+template <class Scalar>
+real_plan<Scalar> plan_dft_c2r(queue q, const std::vector<std::size_t>& lengths, std::size_t batch_count = 1,
+                               plan_options options = {}) {
+    return real_plan<Scalar>(q, lengths, batch_count, real_kind::c2r, options);
 }
 
 template <class Scalar>

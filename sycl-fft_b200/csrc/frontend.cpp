@@ -436,10 +436,11 @@ template class plan<double>;
 template <class Scalar>
 class real_plan<Scalar>::impl {
 public:
-    impl(queue q, std::size_t n, std::size_t batch, real_kind kind, plan_options opts)
-        : queue_(q), n_(n), batch_count_(batch), kind_(kind), options_(opts) {
-        (void)detail::checked_element_count({n_}, batch_count_);
-        if (n_ % 2) throw exception(error_code::invalid_argument, "real transforms need an even length");
+    impl(queue q, std::vector<std::size_t> lengths, std::size_t batch, real_kind kind, plan_options opts)
+        : queue_(q), lengths_(std::move(lengths)), batch_count_(batch), kind_(kind), options_(opts) {
+        (void)detail::checked_element_count(lengths_, batch_count_);
+        n_ = lengths_.back();
+        if (n_ % 2) throw exception(error_code::invalid_argument, "real transforms need an even last length");
         if (options_.placement != placement::out_of_place)
             throw exception(error_code::invalid_argument, "real transforms are out of place");
         if (kind_ != real_kind::r2c && kind_ != real_kind::c2r)
@@ -465,8 +466,8 @@ public:
         config.abi_version = SYCLFFT_B200_PROVIDER_ABI_VERSION;
         config.scalar = std::is_same_v<Scalar, double> ? SYCLFFT_B200_SCALAR_DOUBLE : SYCLFFT_B200_SCALAR_FLOAT;
         config.direction = kind_ == real_kind::r2c ? -1 : 1;
-        config.rank = 1;
-        config.lengths[0] = n_;
+        config.rank = static_cast<uint32_t>(lengths_.size());
+        for (std::size_t i = 0; i < lengths_.size(); ++i) config.lengths[i] = lengths_[i];
         config.batch_count = batch_count_;
         config.in_place = 0;
         config.normalization = static_cast<uint32_t>(options_.normalization);
@@ -513,6 +514,7 @@ public:
     }
 
     queue queue_;
+    std::vector<std::size_t> lengths_;
     std::size_t n_{};
     std::size_t batch_count_{};
     real_kind kind_{real_kind::r2c};
@@ -525,7 +527,11 @@ public:
 
 template <class Scalar>
 real_plan<Scalar>::real_plan(queue q, std::size_t n, std::size_t batch_count, real_kind kind, plan_options options)
-    : impl_(std::make_unique<impl>(q, n, batch_count, kind, options)) {}
+    : impl_(std::make_unique<impl>(q, std::vector<std::size_t>{n}, batch_count, kind, options)) {}
+template <class Scalar>
+real_plan<Scalar>::real_plan(queue q, std::vector<std::size_t> lengths, std::size_t batch_count, real_kind kind,
+                             plan_options options)
+    : impl_(std::make_unique<impl>(q, std::move(lengths), batch_count, kind, options)) {}
 template <class Scalar>
 real_plan<Scalar>::real_plan(real_plan&&) noexcept = default;
 template <class Scalar>
@@ -546,6 +552,10 @@ event real_plan<Scalar>::execute(const complex_type* input, Scalar* output, cons
 template <class Scalar>
 std::size_t real_plan<Scalar>::length() const noexcept {
     return impl_ ? impl_->n_ : 0;
+}
+template <class Scalar>
+std::vector<std::size_t> real_plan<Scalar>::shape() const {
+    return impl_ ? impl_->lengths_ : std::vector<std::size_t>{};
 }
 template <class Scalar>
 std::size_t real_plan<Scalar>::batch_count() const noexcept {

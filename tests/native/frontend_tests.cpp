@@ -323,6 +323,31 @@ try {
         check(std::sqrt(num / den) < 1e-5, "r2c plan mismatch");
         check(std::sqrt(rnum / rden) < 1e-5, "c2r round trip mismatch");
         expect_error(sf::error_code::invalid_argument, [&] { c2r.execute(x.get(), spec.get()); });
+        // 2D: shape {6, 16}, 2 transforms; spectrum {6, 9} against the direct 2D DFT
+        const std::size_t a = 6, m = 16, hm = m / 2 + 1, nb = 2;
+        std::vector<double> real2(a * m * nb);
+        std::vector<std::complex<double>> cplx2(a * m * nb);
+        for (std::size_t i = 0; i < real2.size(); ++i) {
+            real2[i] = static_cast<double>((i * 5 + 2) % 13) / 6.0 - 1.0;
+            cplx2[i] = {real2[i], 0.0};
+        }
+        const auto full2 = reference_many(cplx2, {a, m}, nb, sf::direction::forward);
+        device_buffer<double> x2(real2.size());
+        device_buffer<std::complex<double>> s2(a * hm * nb);
+        x2.write(real2);
+        auto r2c2 = sf::plan_dft_r2c<double>(sf::queue{}, {a, m}, nb);
+        check(r2c2.shape() == std::vector<std::size_t>{a, m} && r2c2.length() == m, "2D real plan shape");
+        r2c2.execute(x2.get(), s2.get()).wait_and_throw();
+        const auto got2 = s2.read();
+        double n2 = 0, d2 = 0;
+        for (std::size_t b = 0; b < nb; ++b)
+            for (std::size_t i = 0; i < a; ++i)
+                for (std::size_t k = 0; k < hm; ++k) {
+                    const auto e = full2[(b * a + i) * m + k];
+                    n2 += std::norm(got2[(b * a + i) * hm + k] - e);
+                    d2 += std::norm(e);
+                }
+        check(std::sqrt(n2 / d2) < 1e-12, "2D r2c plan mismatch");
         expect_error(sf::error_code::invalid_argument, [] { (void)sf::plan_dft_r2c_1d<double>(sf::queue{}, 7); });
     }
     {

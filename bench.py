@@ -10,7 +10,9 @@ uniform[-1, 1) from a seed, all device-resident (every plan's buffer exceeds the
     complex<double> N=65536 x batch 512     (512 MiB)
 value  = GFLOP/s over the step (5 N log2 N per transform), all ranks' work / max rank time.
 e2e    = the same metric through the public plan API with pinned HOST buffers: every step
-         copies the inputs host->device, runs the six executes and copies the results back.
+         runs, per plan, one streamed host-buffer call (syclfft_b200.execute_host: the batch
+         moves through the device in chunks -- copy in, forward, backward, copy out -- with the
+         two copy directions and the kernels overlapped) from a pinned input to a pinned output.
 roofline: the dominant kernel's algorithmic bytes (2 * elements * sizeof(complex) per
          launch) / its CUDA-event launch time, against the measured HBM copy bandwidth.
 cpu_baseline: the CPU restatement of the reference's portable provider (oracle/) on the
@@ -392,10 +394,7 @@ def run_ours(args):
 
         def e2e_step():
             for i, (_, _, _, _, f, b) in enumerate(plans):
-                bufs[i].copy_(host_in[i], non_blocking=True)
-                f.execute(bufs[i])
-                b.execute(bufs[i])
-                host_out[i].copy_(bufs[i], non_blocking=True)
+                sf.execute_host([f, b], host_in[i], host_out[i], stream=stream)
 
         for _ in range(2):
             e2e_step()
@@ -410,7 +409,9 @@ def run_ours(args):
         e2e_ms = max_over_ranks([s2.elapsed_time(e2)], world, dev)[0]
         e2e = {"value": step_flops(workload) * args.e2e_steps * world / (e2e_ms / 1e3) / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d, "steps": args.e2e_steps,
-               "ms_per_step": e2e_ms / args.e2e_steps}
+               "ms_per_step": e2e_ms / args.e2e_steps,
+               "api": "syclfft_b200.execute_host([forward plan, backward plan], pinned in, pinned out) per plan",
+               "pcie_gbs_per_direction": round(h2d / (e2e_ms / args.e2e_steps / 1e3) / 1e9, 1)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu and not args.only and not args.plan and args.batch_div == 1:
@@ -576,7 +577,7 @@ def run_config(args):
 
 
 def run_table(args):
-    """Every configuration's rows on one GPU, one JSON line (the source of BASELINE.md):
+    """Every configuration's rows on one GPU, one JSON line (the per-configuration table):
     P  the provider's plain per-plan execute (estimate planning), device-resident, CUDA events;
     A  autotuned plans (planning_mode::measure) replayed from a captured CUDA graph;
     C  cuFFT through torch.fft as a black box (informational);
@@ -883,7 +884,7 @@ def main():
     ap.add_argument("--split", action="store_true",
                     help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
-    ap.add_argument("--table", action="store_true", help="every configuration's rows (BASELINE.md)")
+    ap.add_argument("--table", action="store_true", help="every configuration's rows (plain, autotuned, cuFFT via torch, CPU)")
     ap.add_argument("--table-rows", default="", help="with --table: only the rows whose name starts with this")
     ap.add_argument("--config", type=int, choices=[3, 4], default=0,
                     help="run a secondary configuration instead (3: Bluestein primes, 4: 3D/2D)")

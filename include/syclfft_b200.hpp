@@ -98,7 +98,10 @@ struct queue {
     CUstream_st* stream = nullptr;      // cudaStream_t; nullptr = legacy default stream
 };
 
-// Stand-in for sycl::event: completion of one execution.
+// Stand-in for sycl::event: completion of one execution. wait_and_throw() also reports a
+// failed device wait of that execution (a bounded wait in one of the plan's kernels gave up,
+// so its output is incomplete) as error_code::execution_failed, the code the reference gives
+// a failed provider execution (src/sycl/sycl.cpp:671-676); each failure is reported once.
 class SYCLFFT_B200_CXX_EXPORT event {
 public:
     event() = default;
@@ -106,9 +109,15 @@ public:
     [[nodiscard]] bool valid() const noexcept { return static_cast<bool>(ev_); }
     [[nodiscard]] CUevent_st* native() const noexcept { return ev_ ? ev_.get() : nullptr; }
     static event record(CUstream_st* stream);
+    // An event whose wait_and_throw() also reads and clears the status word of the provider
+    // plan `plan` through `take_status`; `owner` keeps that plan alive as long as the event.
+    static event record(CUstream_st* stream, std::shared_ptr<void> owner, void* plan, int (*take_status)(void*));
 
 private:
     std::shared_ptr<CUevent_st> ev_;
+    std::shared_ptr<void> owner_;
+    void* plan_ = nullptr;
+    int (*take_status_)(void*) = nullptr;
 };
 
 template <class Scalar>

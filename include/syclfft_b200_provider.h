@@ -157,9 +157,49 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_batch(void *plan, const void *in, v
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void *plan, const void *in, void *out, uint64_t batch,
                                                 int32_t direction, int32_t normalization, void *stream, char *err,
                                                 size_t cap);
-/* Device status word of the plan: 0 = healthy; 1 = a kernel's bounded wait on an
- * asynchronous copy gave up (the execution's output is incomplete). Synchronous. -1 on error. */
+/* Status word of the plan's device work (no reference counterpart; the reference reports a
+ * provider failure as a non-empty error buffer, turned into execution_failed by
+ * src/sycl/sycl.cpp:671-676): 0 = healthy; 1 / 2 / 3 = a bounded wait in one of the plan's
+ * kernels gave up (on a bulk copy, a tensor-core product or a tile copy), so the output of
+ * that execution is incomplete. The word lives in page-locked host memory that the kernels
+ * store to; read it once the execution has completed (event or stream synchronisation).
+ * Reading does not synchronise the device. -1 for a null plan. */
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void *plan);
+/* Like plan_status, and resets the word to 0: the front ends call it when an execution's
+ * event completes and raise execution_failed for a non-zero value, once per failure. */
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_take_status(void *plan);
+/* Failure-detection testing (no reference counterpart): the bounded waits in this plan's
+ * kernels give up after `polls` polls -- 0 gives up at once, so every such wait of the next
+ * execution fails and is reported in the status word; polls < 0 restores the default (2^26
+ * polls, about a second). The environment variable SYCLFFT_B200_WAIT_POLLS, when set to a
+ * number >= 0, is the limit of plans created while it is set. A copy or tensor-core product still in flight when a wait gives up
+ * is waited for (bounded) before the block exits, so nothing writes its shared or tensor
+ * memory afterwards. Returns 0, or -1 for a null plan. */
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_set_wait_limit(void *plan, int64_t polls);
+
+/* ---- Page-locked host buffers (the reference accepts host USM in execute,
+ *      src/sycl/sycl.cpp:72-85; here such buffers are streamed through the device). ----
+ *
+ * Runs `count` stages -- each a complex plan of contiguous layout, with a direction
+ * (0 = the plan's, -1 / +1) and a normalization (-1 = the plan's, else SYCLFFT_B200_NORM_*) --
+ * one after the other on `batch` transforms (0 = the first plan's batch count) read from the
+ * page-locked host buffer `in` and written to the page-locked host buffer `out` (in == out
+ * allowed). All stages have the same precision, transform size and device, and at least
+ * `batch` transforms. The batch is cut into chunks (SYCLFFT_B200_HOST_CHUNK_MB, 32 by
+ * default) that pass through device staging slots: copy in on an internal stream, the
+ * stages on `stream`, copy out on another internal stream, so both copy directions and the
+ * kernels overlap. Stream-ordered: the copies start after earlier work on `stream`, and
+ * `stream` completes after the last copy out. Not capturable in a CUDA graph (refused).
+ * Returns 0, or writes err and returns non-zero. Pageable (not page-locked) host memory is
+ * refused. */
+typedef struct syclfft_b200_host_stage_v1 {
+    void *plan;
+    int32_t direction;
+    int32_t normalization;
+} syclfft_b200_host_stage_v1;
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_host(const syclfft_b200_host_stage_v1 *stages, uint32_t count,
+                                                  const void *in, void *out, uint64_t batch, void *stream, char *err,
+                                                  size_t cap);
 
 /* ---- Grouped execution (no reference counterpart): the serving path's batched launch. ----
  *
@@ -197,12 +237,14 @@ SYCLFFT_B200_EXPORT void syclfft_b200_group_destroy(void *group);
  *
  * Batched 1-D complex<float> C2C of power-of-two length n in [2^15, 2^20] over `batch`
  * contiguous lines, n * batch <= 4194304 (4 Mi) elements; larger sizes are rejected with
- * an error message. in == out (in place) is allowed. direction -1 / +1,
+ * an error message. in == out (in place) is allowed; both must be 8-byte aligned (a
+ * misaligned pointer is refused before anything is launched). direction -1 / +1,
  * normalization SYCLFFT_B200_NORM_*. Enqueued on `stream` (cudaStream_t, NULL = legacy
  * default stream); returns 0, or writes err and returns non-zero.
  * All calls share the arrays: calls that overlap on the GPU race and must be ordered by
  * the caller. The first call on a device looks up the arrays' device addresses and
- * should come before any stream capture. */
+ * should come before any stream capture (made during a capture it is refused, and a
+ * later call retries). */
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void *in, void *out, uint64_t n, uint64_t batch,
                                                              int32_t direction, uint32_t normalization,
                                                              void *stream, char *err, size_t cap);

@@ -1,6 +1,8 @@
 // Shared-memory barrier, bulk-copy and proxy-fence helpers (inline PTX) used by the
 // copy-engine-pipelined and tensor-core kernels. Every wait on an mbarrier in this
-// project is a bounded poll of mbar_try_wait (kSpinLimit polls).
+// project is a bounded poll of mbar_try_wait: at most the plan's wait limit (kSpinLimit
+// polls by default), and kSpinLimit for the drain of a copy still in flight after a wait
+// gave up.
 #pragma once
 
 #include <cstdint>
@@ -43,4 +45,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 constexpr long long kSpinLimit = 1ll << 26;
+
+// Bounded wait for phase `parity` of `bar`: true once it completed, false after `polls`
+// polls (0 polls gives up at once).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, long long polls) {
+    for (long long spin = 0; spin < polls; ++spin)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Records a bounded wait that gave up in the plan's status word. The word lives in
+// page-locked host memory mapped into the device, so this is a plain system-scope store
+// (no atomic over the bus); the host reads it once the launch has completed.
+__device__ __forceinline__ void report_status(int* status, int code) {
+    if (!status) return;
+    *reinterpret_cast<volatile int*>(status) = code;
+    __threadfence_system();
+}
 }  // namespace sfb

@@ -89,14 +89,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t parity = static_cast<uint32_t>(it >> 1) & 1u;
         __syncthreads();  // buf[1-b] (the previous line's row scratch) is no longer read
         if (line + clusters < P.lines) load(b ^ 1, line + clusters);
-        bool ok = false;
-        for (long long spin = 0; spin < kSpinLimit; ++spin) {
-            if (mbar_try_wait(bars + b, parity)) {
-                ok = true;
-                break;
-            }
-        }
-        if (__syncthreads_or(!ok) && tid == 0 && P.status) atomicExch(P.status, 1);
+        const bool ok = mbar_wait_bounded(bars + b, parity, kSpinLimit);
+        if (__syncthreads_or(!ok) && tid == 0) report_status(P.status, 1);
         C* const slab = buffer(smem, b);
 
         // 1. column FFTs over n1 (column w = tid % 16, n2 = 16p + w), twiddled into Y

@@ -73,6 +73,8 @@ enum : int {
     kFeatRealPost = 512,  // R2C: the spectrum Z goes to shared memory, then X[k] for k = 0..N from
                           // the pairs (Z[k], Z[N-k]), N+1 bins per line stored
     kFeatRealPre = 1024,  // C2R: the first stage forms Z[k] from the bins (X[k], X[N-k]) on load
+    kFeatLoadCG = 2048,   // first-stage global loads bypass L1 (ld.global.cg): data another CTA of
+                          // the same launch wrote (the fused four-step's L2-resident ring)
 };
 
 // X[k] = 1/2 [(Z[k] + conj Z[N-k]) - i W_2N^k (Z[k] - conj Z[N-k])] * scale; a = Z[k], c = Z[N-k]
@@ -180,7 +182,10 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 if (X.line_ok) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
-                        C a = MODEC ? X.gin[(int64_t)(j + r * NR) * X.in_ks] : X.gin[j + r * NR];
+                        const C* src = MODEC ? X.gin + (int64_t)(j + r * NR) * X.in_ks : X.gin + (j + r * NR);
+                        C a;
+                        if constexpr (FEAT & kFeatLoadCG) a = __ldcg(src);
+                        else a = *src;
                         if (X.conj_in) a.y = -a.y;
                         v[i * R + r] = a;
                     }

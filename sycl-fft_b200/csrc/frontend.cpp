@@ -99,14 +99,39 @@ using syclfft_b200_create_ex_fn = void* (*)(const syclfft_b200_plan_config_v1*, 
 using syclfft_b200_create_real_fn = void* (*)(const syclfft_b200_plan_config_v1*, int32_t, uint32_t, char*, size_t);
 using syclfft_b200_create_strided_fn = void* (*)(const syclfft_b200_plan_config_v1*, const syclfft_b200_layout_v1*,
                                                  uint32_t, char*, size_t);
+using syclfft_b200_take_status_fn = int (*)(void*);
+using syclfft_b200_execute_host_fn = int (*)(const syclfft_b200_host_stage_v1*, uint32_t, const void*, void*, uint64_t,
+                                             void*, char*, size_t);
 
 struct loaded_provider {
     const syclfft_b200_provider_v1* api{};
     std::shared_ptr<void> module;
     syclfft_b200_create_ex_fn create_ex{};            // optional extensions: split precision,
     syclfft_b200_create_real_fn create_real{};        // real transforms,
-    syclfft_b200_create_strided_fn create_strided{};  // strided layouts
+    syclfft_b200_create_strided_fn create_strided{};  // strided layouts,
+    syclfft_b200_take_status_fn take_status{};        // device-wait failures,
+    syclfft_b200_execute_host_fn execute_host{};      // page-locked host buffers
 };
+
+// Owner of a provider plan: destroys it (keeping the module loaded until then) when the last
+// front-end object referring to it -- the plan or one of its events -- is gone.
+std::shared_ptr<void> own_plan(const loaded_provider& m, void* handle) {
+    auto api = m.api;
+    auto module = m.module;
+    return std::shared_ptr<void>(handle, [api, module](void* h) {
+        if (h) api->destroy(h);
+    });
+}
+
+// Where a pointer lives: 1 = device (or managed), 2 = page-locked host memory.
+int memory_kind(const void* pointer) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, pointer) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return attr.type == cudaMemoryTypeHost ? 2 : 1;
+}
 
 // provider_loader.cpp:178-232: first module in the search path that exports the entry
 // point wins; a wrong ABI version is a plugin_error.
@@ -136,7 +161,9 @@ loaded_provider load_b200_provider() {
         auto create_real = reinterpret_cast<syclfft_b200_create_real_fn>(dlsym(raw, "syclfft_b200_create_real"));
         auto create_strided =
             reinterpret_cast<syclfft_b200_create_strided_fn>(dlsym(raw, "syclfft_b200_create_strided"));
-        return {api, std::move(module), create_ex, create_real, create_strided};
+        auto take_status = reinterpret_cast<syclfft_b200_take_status_fn>(dlsym(raw, "syclfft_b200_plan_take_status"));
+        auto execute_host = reinterpret_cast<syclfft_b200_execute_host_fn>(dlsym(raw, "syclfft_b200_execute_host"));
+        return {api, std::move(module), create_ex, create_real, create_strided, take_status, execute_host};
     }
     throw exception(error_code::provider_unavailable, "Unable to load provider 'syclfft_provider_b200': " + errors);
 }
@@ -203,6 +230,21 @@ void event::wait_and_throw() const {
     if (!ev_) return;
     const cudaError_t e = cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(ev_.get()));
     if (e != cudaSuccess) throw exception(error_code::execution_failed, cudaGetErrorString(e));
+    if (take_status_ && plan_) {
+        const int code = take_status_(plan_);
+        if (code > 0)
+            throw exception(error_code::execution_failed, "a bounded wait in a B200 kernel gave up (status " +
+                                                              std::to_string(code) +
+                                                              "); the output of this execution is incomplete");
+    }
+}
+
+event event::record(CUstream_st* stream, std::shared_ptr<void> owner, void* plan, int (*take_status)(void*)) {
+    event out = record(stream);
+    out.owner_ = std::move(owner);
+    out.plan_ = plan;
+    out.take_status_ = take_status;
+    return out;
 }
 
 event event::record(CUstream_st* stream) {
@@ -264,6 +306,7 @@ public:
         config.normalization = static_cast<uint32_t>(options_.normalization);
         config.measure = options_.planning == planning_mode::measure ? 1 : 0;
         config.device = queue_.device;
+        strided_ = layout != nullptr;
         if (lay) {
             if (!module_.create_strided)
                 throw exception(error_code::provider_unavailable, "B200 provider module lacks syclfft_b200_create_strided");
@@ -281,6 +324,7 @@ public:
         if (!handle_) {
             throw exception(error_code::planning_failed, error[0] ? error.data() : "B200 plan creation failed");
         }
+        owner_ = detail::own_plan(module_, handle_);
     }
 
     ~impl() {
@@ -288,7 +332,6 @@ public:
             if (last_event_) last_event_->wait_and_throw();
         } catch (...) {
         }
-        if (handle_) module_.api->destroy(handle_);
     }
 
     void validate_pointer(const void* pointer, const char* name) const {
@@ -315,10 +358,19 @@ public:
         if (last_event_ && last_event_->valid())
             cudaStreamWaitEvent(stream, reinterpret_cast<cudaEvent_t>(last_event_->native()), 0);
         std::array<char, 1024> error{};
-        const int rc = module_.api->execute(handle_, input, output, queue_.stream, error.data(), error.size());
+        // page-locked host memory on both sides (host USM): streamed through the device in
+        // overlapped chunks; otherwise the kernels address the buffers directly
+        const bool host = !strided_ && detail::memory_kind(input) == 2 && detail::memory_kind(output) == 2;
+        int rc = 0;
+        if (host && module_.execute_host) {
+            syclfft_b200_host_stage_v1 stage{handle_, 0, -1};
+            rc = module_.execute_host(&stage, 1, input, output, 0, queue_.stream, error.data(), error.size());
+        } else {
+            rc = module_.api->execute(handle_, input, output, queue_.stream, error.data(), error.size());
+        }
         if (rc != 0 || error[0])
             throw exception(error_code::execution_failed, error[0] ? error.data() : "B200 execution failed");
-        event done = event::record(queue_.stream);
+        event done = event::record(queue_.stream, owner_, handle_, module_.take_status);
         last_event_ = done;
         return done;
     }
@@ -331,6 +383,8 @@ public:
     plan_options options_{};
     detail::loaded_provider module_;
     void* handle_{};
+    std::shared_ptr<void> owner_;  // destroys handle_ after the plan and its events are gone
+    bool strided_ = false;
     std::optional<event> last_event_;
     std::mutex mutex_;
 };
@@ -479,6 +533,7 @@ public:
                                       flags, error.data(), error.size());
         if (!handle_)
             throw exception(error_code::planning_failed, error[0] ? error.data() : "B200 plan creation failed");
+        owner_ = detail::own_plan(module_, handle_);
     }
 
     ~impl() {
@@ -486,7 +541,6 @@ public:
             if (last_event_) last_event_->wait_and_throw();
         } catch (...) {
         }
-        if (handle_) module_.api->destroy(handle_);
     }
 
     event execute(const void* input, void* output, const std::vector<event>& dependencies, real_kind called) {
@@ -508,7 +562,7 @@ public:
         const int rc = module_.api->execute(handle_, input, output, queue_.stream, error.data(), error.size());
         if (rc != 0 || error[0])
             throw exception(error_code::execution_failed, error[0] ? error.data() : "B200 execution failed");
-        event done = event::record(queue_.stream);
+        event done = event::record(queue_.stream, owner_, handle_, module_.take_status);
         last_event_ = done;
         return done;
     }
@@ -521,6 +575,7 @@ public:
     plan_options options_{};
     detail::loaded_provider module_;
     void* handle_{};
+    std::shared_ptr<void> owner_;  // destroys handle_ after the plan and its events are gone
     std::optional<event> last_event_;
     std::mutex mutex_;
 };

@@ -18,10 +18,12 @@
 // pass overwrites every scratch element the row pass reads, so nothing has to start at
 // zero. Calls that overlap on the GPU (different streams, no ordering between them) race
 // on the arrays. The first call on a device looks up the arrays' device addresses
-// (cudaGetSymbolAddress, with that device current); make that first call before any
-// stream capture.
+// (cudaGetSymbolAddress, with that device current) and the device's shared-memory limit;
+// make that first call before any stream capture (a first call made while the stream is
+// capturing is refused with an error, and a later call retries the lookup).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -43,10 +45,47 @@ static __device__ __align__(256) float2 g_noalloc_tables[kNoAllocMaxTable];
 struct DeviceArrays {
     float2* scratch = nullptr;
     float2* tables = nullptr;
-    cudaError_t status = cudaSuccess;
+    int smem_optin = 0;  // cudaDevAttrMaxSharedMemoryPerBlockOptin
+    bool ready = false;
 };
 DeviceArrays g_arrays[kMaxDevices];
-std::once_flag g_once[kMaxDevices];
+std::mutex g_arrays_mu[kMaxDevices];
+
+// Device addresses of the two arrays and the shared-memory limit of the current device
+// `dev`, looked up on the first successful call and kept; a failed lookup is not kept, so
+// a later call tries again.
+cudaError_t device_arrays(int dev, cudaStream_t st, DeviceArrays* out, std::string* why) {
+    std::lock_guard<std::mutex> lock(g_arrays_mu[dev]);
+    DeviceArrays& a = g_arrays[dev];
+    if (!a.ready) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        cudaError_t e = cudaStreamIsCapturing(st, &cap);
+        if (e != cudaSuccess) {
+            *why = "cudaStreamIsCapturing";
+            return e;
+        }
+        if (cap != cudaStreamCaptureStatusNone) {
+            *why = "the first no-allocation call on a device must not be made while its stream is capturing";
+            return cudaErrorStreamCaptureUnsupported;
+        }
+        DeviceArrays t;
+        e = cudaGetSymbolAddress(reinterpret_cast<void**>(&t.scratch), g_noalloc_scratch);
+        if (e == cudaSuccess) e = cudaGetSymbolAddress(reinterpret_cast<void**>(&t.tables), g_noalloc_tables);
+        if (e != cudaSuccess) {
+            *why = "cudaGetSymbolAddress";
+            return e;
+        }
+        e = cudaDeviceGetAttribute(&t.smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess) {
+            *why = "cudaDeviceGetAttribute";
+            return e;
+        }
+        t.ready = true;
+        a = t;
+    }
+    *out = a;
+    return cudaSuccess;
+}
 
 // exp(-2 pi i num / den) in double, stored as float.
 __device__ float2 cis_neg_f(long long num, long long den) {
@@ -128,6 +167,12 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
         set_error(err, cap, "input and output must be non-null device pointers");
         return 1;
     }
+    // The kernels move whole float2 elements: an address off an 8-byte boundary would fault
+    // on the device and leave the caller's context unusable, so it is refused here.
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % sizeof(float2)) {
+        set_error(err, cap, "input and output must be aligned to 8 bytes (one complex<float>)");
+        return 1;
+    }
     if (direction != -1 && direction != 1) {
         set_error(err, cap, "Invalid FFT direction");
         return 1;
@@ -140,7 +185,11 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
         set_error(err, cap, "FFT length and batch count must be non-zero");
         return 1;
     }
-    if (n > static_cast<uint64_t>(kNoAllocMaxElements) || batch > static_cast<uint64_t>(kNoAllocMaxElements) / n) {
+    if (n < (1u << 15) || n > (1u << 20) || (n & (n - 1))) {
+        set_error(err, cap, "no-allocation FFT supports power-of-two lengths 2^15 .. 2^20, got " + std::to_string(n));
+        return 1;
+    }
+    if (batch > static_cast<uint64_t>(kNoAllocMaxElements) / n) {
         set_error(err, cap, "no-allocation FFT is limited to " + std::to_string(kNoAllocMaxElements) +
                                 " complex<float> elements per call (n * batch)");
         return 1;
@@ -157,29 +206,39 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
             er = r;
         }
     }
-    if (!ec || !er || n < (1u << 15) || n > (1u << 20)) {
-        set_error(err, cap, "no-allocation FFT supports power-of-two lengths 2^15 .. 2^20, got " + std::to_string(n));
+    if (!ec || !er) {
+        set_error(err, cap, "no-allocation FFT has no kernel split for length " + std::to_string(n));
         return 1;
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (e != cudaSuccess) {
         set_error(err, cap, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
         return 1;
     }
-    // Once per device, with that device current: device addresses of the two arrays.
-    std::call_once(g_once[dev], [dev] {
-        DeviceArrays& a = g_arrays[dev];
-        a.status = cudaGetSymbolAddress(reinterpret_cast<void**>(&a.scratch), g_noalloc_scratch);
-        if (a.status == cudaSuccess)
-            a.status = cudaGetSymbolAddress(reinterpret_cast<void**>(&a.tables), g_noalloc_tables);
-    });
-    const DeviceArrays& arr = g_arrays[dev];
-    if (arr.status != cudaSuccess || !arr.scratch || !arr.tables) {
-        set_error(err, cap, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(arr.status));
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error(err, cap, "no-allocation FFT supports device ordinals below " + std::to_string(kMaxDevices) +
+                                ", got " + std::to_string(dev));
+        return 1;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DeviceArrays arr;
+    std::string why;
+    e = device_arrays(dev, st, &arr, &why);
+    if (e != cudaSuccess) {
+        set_error(err, cap, why + ": " + cudaGetErrorString(e));
         return 1;
     }
     const int n1 = ec->n, n2 = er->n;
+    const size_t smem_cols = static_cast<size_t>(ec->w) * n1 * sizeof(float2);
+    const size_t smem_rows = static_cast<size_t>(er->w) * pitch_k(n2) * sizeof(float2);
+    if (smem_cols > static_cast<size_t>(arr.smem_optin) || smem_rows > static_cast<size_t>(arr.smem_optin)) {
+        set_error(err, cap, "no-allocation FFT of length " + std::to_string(n) + " needs " +
+                                std::to_string(smem_cols > smem_rows ? smem_cols : smem_rows) +
+                                " bytes of shared memory per block; this device allows " +
+                                std::to_string(arr.smem_optin));
+        return 1;
+    }
     TableJob job{};
     job.n1 = n1;
     job.n2 = n2;
@@ -202,7 +261,6 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
         set_error(err, cap, "no-allocation FFT twiddle table overflow");
         return 1;
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     noalloc_fill_tables<<<(total + 255) / 256, 256, 0, st>>>(job, arr.tables);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -225,8 +283,7 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
     a.tw4_hi = arr.tables + job.off_hi;
     a.tw4_lo = arr.tables + job.off_lo;
     a.tw4_shift = shift;
-    e = launch_fixed(ec->id, false, true, a, ec->w * ec->tpl, static_cast<size_t>(ec->w) * n1 * sizeof(float2),
-                     B * a.col_tiles, in, arr.scratch, st);
+    e = launch_fixed(ec->id, false, true, a, ec->w * ec->tpl, smem_cols, B * a.col_tiles, in, arr.scratch, st);
     if (e != cudaSuccess) {
         set_error(err, cap, std::string("column pass: ") + cudaGetErrorString(e));
         return 1;
@@ -243,8 +300,7 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_noalloc_c2c_f32(const void* in, voi
     b.scale = scale;
     b.rows = n1;
     b.line = N;
-    e = launch_fixed(er->id, false, false, b, er->w * er->tpl,
-                     static_cast<size_t>(er->w) * pitch_k(n2) * sizeof(float2), b.col_tiles, arr.scratch, out, st);
+    e = launch_fixed(er->id, false, false, b, er->w * er->tpl, smem_rows, b.col_tiles, arr.scratch, out, st);
     if (e != cudaSuccess) {
         set_error(err, cap, std::string("row pass: ") + cudaGetErrorString(e));
         return 1;

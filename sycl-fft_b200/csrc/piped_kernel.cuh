@@ -10,8 +10,10 @@
 // engine is told to fetch the following line into the copy buffer, so that load hides
 // behind the remaining stages, and the last stage's stores drain during the next line.
 //
-// Waits on the copy are bounded: after kSpinLimit polls the CTA records a timeout in the
-// plan's status word and stops (all threads agree through a barrier first).
+// Waits on the copy are bounded: after P.wait_polls polls the CTA records a timeout in the
+// plan's status word, lets the copy it gave up on land (bounded again by kSpinLimit, so no
+// copy into its shared memory outlives it) and stops (all threads agree through a barrier
+// first).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -29,6 +31,7 @@ struct PipedParams {
     int conj_in = 0, conj_out = 0;
     double scale = 1.0;
     int* status = nullptr;  // set to 1 if a copy wait timed out
+    long long wait_polls = kSpinLimit;  // polls before a copy wait gives up
 };
 
 constexpr int kCopyChunks = 4;
@@ -89,16 +92,16 @@ __global__ void __launch_bounds__(MAXT, 1)
 
     uint32_t parity = 0;
     for (int64_t line = blockIdx.x; line < P.lines; line += gridDim.x) {
-        bool ok = false;
-        for (long long spin = 0; spin < kSpinLimit; ++spin) {
-            if (mbar_try_wait(bar, parity)) {
-                ok = true;
-                break;
-            }
-        }
+        const bool ok = mbar_wait_bounded(bar, parity, P.wait_polls);
         if (__syncthreads_or(!ok)) {
-            if (t == 0 && P.status) atomicExch(P.status, 1);
-            return;  // the only copy in flight is the one that never completed
+            if (t == 0) {
+                report_status(P.status, 1);
+                // the only copy in flight is the one given up on: let it land before the
+                // shared memory is released
+                mbar_wait_bounded(bar, parity, kSpinLimit);
+            }
+            __syncthreads();
+            return;
         }
         parity ^= 1u;
         X.gout = out + line * P.out_pitch;

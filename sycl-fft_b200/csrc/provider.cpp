@@ -33,6 +33,7 @@
 #include "layout_launch.hpp"
 #include "cluster_pipe.hpp"
 #include "bluestein_launch.hpp"
+#include "fused4_launch.hpp"
 #include "planner.hpp"
 
 namespace sfb {
@@ -81,6 +82,9 @@ struct BoundPass {
     PipedParams pp;    // used when spec.piped_id >= 0 and the buffers are 16-byte aligned
     TcParams tp;       // used when spec.tc_id >= 0
     ClusterPipeParams kp;  // used when spec.cluster_pipe and the buffers are 16-byte aligned
+    // four-step column pass whose row pass (the next pass) can run with it in one fused launch
+    // (fused4_kernel.cuh), or nullptr
+    const Fused4Entry* fused4 = nullptr;
 };
 
 TcParams to_tc(const PassParams& p, const void* tw, int* status) {
@@ -181,12 +185,54 @@ cudaStream_t memory_stream(int device) {
     return s;
 }
 
+// Status words of plans: 4-byte slots of page-locked host memory mapped into every device
+// (the kernels store to them directly; the host reads them after an execution completed,
+// without a device synchronisation). Blocks are never freed (cudaFreeHost would synchronize
+// the device); slots return to the pool in stream order after a plan's last execution.
+class StatusPool {
+public:
+    int* acquire() {
+        std::lock_guard<std::mutex> lock(mu_);
+        if (free_.empty()) {
+            constexpr int kBlock = 1024;
+            void* block = nullptr;
+            check(cudaHostAlloc(&block, kBlock * sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable),
+                  "cudaHostAlloc(status words)");
+            int* words = static_cast<int*>(block);
+            for (int i = kBlock - 1; i >= 0; --i) free_.push_back(words + i);
+        }
+        int* w = free_.back();
+        free_.pop_back();
+        __atomic_store_n(w, 0, __ATOMIC_SEQ_CST);
+        return w;
+    }
+    void release(int* w) {
+        std::lock_guard<std::mutex> lock(mu_);
+        free_.push_back(w);
+    }
+
+private:
+    std::mutex mu_;
+    std::vector<int*> free_;
+};
+
+StatusPool& status_pool() {
+    static StatusPool* pool = new StatusPool;  // outlives host callbacks still queued at exit
+    return *pool;
+}
+
+void release_status_word(void* w) { status_pool().release(static_cast<int*>(w)); }
+
 struct DevicePlan {
     PlanSpec spec;
     int device = 0;
     void* table_mem = nullptr;
     void* scratch = nullptr;
-    int* status = nullptr;  // device word: non-zero after a bounded wait in a kernel timed out
+    // Status word (StatusPool): non-zero after a bounded wait in one of the plan's kernels gave
+    // up. Plans built over other plans (real, strided) point at a child's word.
+    int* status = nullptr;
+    bool owns_status = false;
+    long long wait_polls = kSpinLimit;  // polls before a bounded wait in the plan's kernels gives up
     int sms = 148;
     std::vector<BoundPass> passes;
     cudaEvent_t done = nullptr;
@@ -234,6 +280,8 @@ struct DevicePlan {
             if (real_tw) cudaFreeAsync(real_tw, ms);
             if (pack_buf) cudaFreeAsync(pack_buf, ms);
             if (md_buf) cudaFreeAsync(md_buf, ms);
+            if (owns_status && cudaLaunchHostFunc(ms, release_status_word, status) == cudaSuccess)
+                owns_status = false;
         } else {
             if (done) cudaEventSynchronize(done);
             if (scratch) cudaFree(scratch);
@@ -243,6 +291,7 @@ struct DevicePlan {
             if (pack_buf) cudaFree(pack_buf);
             if (md_buf) cudaFree(md_buf);
         }
+        if (owns_status) status_pool().release(status);
         if (done) cudaEventDestroy(done);
         if (ready) cudaEventDestroy(ready);
         if (prev != device) cudaSetDevice(prev);
@@ -380,9 +429,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         offsets[i] = total;
         total += (plan->spec.table_sizes[i] * cs + 255) / 256 * 256;
     }
-    const size_t status_off = total;
-    total += 256;  // status word(s), zero-initialised with the tables
-    std::vector<unsigned char> blob(total, 0);
+    std::vector<unsigned char> blob(std::max<size_t>(total, 256), 0);
     for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
         if (req.dbl) pack_table<double>(plan->spec.tables[i], blob, offsets[i]);
         else pack_table<float>(plan->spec.tables[i], blob, offsets[i]);
@@ -390,7 +437,14 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
     cudaStream_t ms = memory_stream(device);
     check(cudaMallocAsync(&plan->table_mem, blob.size(), ms), "cudaMallocAsync(tables)");
     check(cudaMemcpyAsync(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(tables)");
-    plan->status = reinterpret_cast<int*>(static_cast<unsigned char*>(plan->table_mem) + status_off);
+    plan->status = status_pool().acquire();
+    plan->owns_status = true;
+    // failure-detection testing: SYCLFFT_B200_WAIT_POLLS sets the wait limit of new plans
+    if (const char* v = std::getenv("SYCLFFT_B200_WAIT_POLLS")) {
+        char* end = nullptr;
+        const long long polls = std::strtoll(v, &end, 10);
+        if (end != v && polls >= 0) plan->wait_polls = polls;
+    }
     check(cudaDeviceGetAttribute(&plan->sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
     plan->stream_scratch = (flags & SYCLFFT_B200_CREATE_STREAM_SCRATCH) != 0;
     if (plan->spec.scratch_elements && !plan->stream_scratch) {
@@ -457,6 +511,17 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         bp.pp = to_piped(bp.p, plan->status);
         bp.tp = to_tc(bp.p, tab(ps.tables.tc_tw), plan->status);
         plan->passes.push_back(bp);
+    }
+    // four-step column + row passes of a contiguous axis with a fused kernel: one launch, the
+    // intermediate in an L2-resident ring (SYCLFFT_B200_FUSED4=0 keeps the two launches)
+    const char* f4 = std::getenv("SYCLFFT_B200_FUSED4");
+    const bool fused_ok = !(f4 && f4[0] == '0') && !req.no_fixed;
+    for (size_t i = 0; fused_ok && i + 1 < plan->passes.size(); ++i) {
+        const PassSpec& a = plan->passes[i].spec_ref();
+        const PassSpec& b = plan->passes[i + 1].spec_ref();
+        if (a.kind == "fourstep_cols" && b.kind == "fourstep_rows" && a.fixed_id >= 0 && b.fixed_id >= 0 &&
+            a.p.mode == kModeC && b.p.mode == kModeK && a.dst == Buf::Scratch && b.src == Buf::Scratch)
+            plan->passes[i].fused4 = find_fused4(req.dbl, a.fixed_id, b.fixed_id);
     }
     return plan.release();
 }
@@ -914,6 +979,7 @@ bool launch_tma(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cud
     q.conj_out = f.conj_out;
     q.scale = f.scale;
     q.status = plan->status;
+    q.wait_polls = plan->wait_polls;
     const cudaError_t e = launch_tma_cols(bp.spec_ref().fixed_id, src, dst, p.n_outer, q, stream);
     if (e == cudaErrorInvalidValue) return false;
     check(e, "FFT TMA column pass launch");
@@ -954,6 +1020,11 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
 void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stream, uint64_t batch,
                   int direction, int normalization) {
     if (!plan || !in || !out) throw std::invalid_argument("invalid B200 execution argument");
+    // The kernels move whole float2 / double2 elements; a misaligned address would fault
+    // on the device (a sticky error for the whole context), so it is refused here.
+    if (!plan->real_kind &&
+        (reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % (plan->spec.req.dbl ? 16 : 8))
+        throw std::invalid_argument("buffers must be aligned to the complex element size");
     if (plan->real_kind) {
         execute_real(plan, in, out, stream, batch, direction, normalization);
         return;
@@ -1002,9 +1073,32 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
         if (b == Buf::Output) return out;
         return scratch;
     };
-    for (size_t i = 0; i < plan->passes.size(); ++i) {
+    const size_t np = plan->passes.size();
+    for (size_t i = 0; i < np; ++i) {
         BoundPass bp = rescale(plan->passes[i], batch, planned);
-        if (flip || set_scale) apply_override(bp, i == 0, i + 1 == plan->passes.size(), flip, scale, set_scale);
+        bp.pp.wait_polls = plan->wait_polls;
+        bp.tp.wait_polls = plan->wait_polls;
+        if (flip || set_scale) apply_override(bp, i == 0, i + 1 == np, flip, scale, set_scale);
+        if (bp.fused4 && i + 1 < np && bp.p.n_outer >= 3) {
+            BoundPass bq = rescale(plan->passes[i + 1], batch, planned);
+            if (flip || set_scale) apply_override(bq, false, i + 2 == np, flip, scale, set_scale);
+            Fused4Params f;
+            f.lines = bp.p.n_outer;
+            f.tw1 = bp.fp.tw;
+            f.tw2 = bq.fp.tw;
+            f.tw4_hi = bp.fp.tw4_hi;
+            f.tw4_lo = bp.fp.tw4_lo;
+            f.tw4_shift = bp.fp.tw4_shift;
+            f.conj_in = bp.fp.conj_in;
+            f.conj_out = bq.fp.conj_out;
+            f.scale = bq.fp.scale;
+            f.wait_polls = plan->wait_polls;
+            f.status = plan->status;
+            check(launch_fused4(*bp.fused4, f, buf(bp.spec_ref().src), buf(bq.spec_ref().dst), scratch, stream),
+                  "FFT fused four-step launch");
+            ++i;
+            continue;
+        }
         launch_bound_pass(plan, bp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream);
     }
     // Under capture the record becomes a node of the graph, so destroying the plan still
@@ -1012,6 +1106,148 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     check(capturing ? cudaEventRecordWithFlags(plan->done, stream, cudaEventRecordExternal)
                     : cudaEventRecord(plan->done, stream),
           "cudaEventRecord");
+}
+
+// ---------------------------------------------------------------- host buffers
+// Transforms of page-locked host buffers (syclfft_b200_execute_host). The batch is cut into
+// chunks that flow through device staging slots in a three-stage pipeline: copy in on one
+// stream, the stages' transforms on the caller's stream, copy out on another. The two PCIe
+// directions and the kernels then overlap, so a chunked call costs about the slower copy
+// direction plus one chunk, not the sum of both copies and the kernels.
+constexpr int kHostSlots = 4;
+
+struct HostStaging {
+    std::mutex mu;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    unsigned char* mem = nullptr;  // kHostSlots x 2 buffers of slot_bytes
+    size_t slot_bytes = 0;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t loaded[kHostSlots] = {}, computed[kHostSlots] = {}, freed[kHostSlots] = {};
+    bool pending[kHostSlots] = {};  // freed[i] guards a copy-out still to be waited for
+    unsigned next = 0;              // slot of the next chunk (rotates across calls)
+};
+
+HostStaging& host_staging(int device) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<HostStaging>> all;
+    std::lock_guard<std::mutex> lock(mu);
+    auto& h = all[device];
+    if (!h) {
+        auto fresh = std::make_unique<HostStaging>();
+        check(cudaStreamCreateWithFlags(&fresh->h2d, cudaStreamNonBlocking), "cudaStreamCreate(copy in)");
+        check(cudaStreamCreateWithFlags(&fresh->d2h, cudaStreamNonBlocking), "cudaStreamCreate(copy out)");
+        check(cudaEventCreateWithFlags(&fresh->start, cudaEventDisableTiming), "cudaEventCreate");
+        for (int i = 0; i < kHostSlots; ++i) {
+            check(cudaEventCreateWithFlags(&fresh->loaded[i], cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&fresh->computed[i], cudaEventDisableTiming), "cudaEventCreate");
+            check(cudaEventCreateWithFlags(&fresh->freed[i], cudaEventDisableTiming), "cudaEventCreate");
+        }
+        h = std::move(fresh);
+    }
+    return *h;
+}
+
+size_t host_chunk_bytes() {
+    static const size_t bytes = [] {
+        const char* v = std::getenv("SYCLFFT_B200_HOST_CHUNK_MB");
+        const long mb = v ? std::strtol(v, nullptr, 10) : 0;
+        return static_cast<size_t>(mb > 0 ? mb : 32) << 20;
+    }();
+    return bytes;
+}
+
+bool is_host_memory(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+void execute_host(const syclfft_b200_host_stage_v1* stages, uint32_t count, const void* in, void* out, uint64_t batch,
+                  cudaStream_t stream) {
+    if (!stages || count == 0) throw std::invalid_argument("at least one stage is needed");
+    if (!in || !out) throw std::invalid_argument("input and output must be non-null");
+    auto* first = static_cast<DevicePlan*>(stages[0].plan);
+    if (!first) throw std::invalid_argument("invalid B200 execution argument");
+    const bool dbl = first->spec.req.dbl;
+    const uint64_t line = first->spec.transform_size;
+    if (batch == 0) batch = first->spec.req.batch;
+    for (uint32_t i = 0; i < count; ++i) {
+        auto* p = static_cast<DevicePlan*>(stages[i].plan);
+        if (!p) throw std::invalid_argument("invalid B200 execution argument");
+        if (p->real_kind || p->strided)
+            throw std::invalid_argument("host-buffer execution takes complex plans of contiguous layout");
+        if (p->spec.req.dbl != dbl || p->spec.transform_size != line || p->device != first->device)
+            throw std::invalid_argument("host-buffer stages need one precision, transform size and device");
+        if (batch > p->spec.req.batch) throw std::invalid_argument("batch exceeds the plan's batch count");
+        if (stages[i].direction != 0 && stages[i].direction != -1 && stages[i].direction != 1)
+            throw std::invalid_argument("Invalid FFT direction");
+        if (stages[i].normalization > 3) throw std::invalid_argument("Invalid normalization");
+    }
+    const size_t cs = dbl ? 16 : 8;
+    if ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) % cs)
+        throw std::invalid_argument("buffers must be aligned to the complex element size");
+    if (!is_host_memory(in) || !is_host_memory(out))
+        throw std::invalid_argument("host buffers must be page-locked (cudaHostAlloc / cudaHostRegister)");
+    DeviceGuard guard(first->device);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
+    if (cap != cudaStreamCaptureStatusNone)
+        throw std::invalid_argument("host-buffer execution cannot be captured in a CUDA graph");
+
+    const size_t line_bytes = static_cast<size_t>(line) * cs;
+    const uint64_t chunk_lines = std::max<uint64_t>(1, host_chunk_bytes() / line_bytes);
+    const size_t need = static_cast<size_t>(std::min<uint64_t>(chunk_lines, batch)) * line_bytes;
+    HostStaging& hs = host_staging(first->device);
+    std::lock_guard<std::mutex> lock(hs.mu);
+    if (hs.slot_bytes < need) {
+        // every earlier chunk's copy-out is done before the staging memory is replaced
+        check(cudaStreamSynchronize(hs.d2h), "staging");
+        if (hs.mem) check(cudaFree(hs.mem), "cudaFree(staging)");
+        hs.mem = nullptr;
+        hs.slot_bytes = 0;
+        for (bool& b : hs.pending) b = false;
+        check(cudaMalloc(&hs.mem, need * 2 * kHostSlots), "cudaMalloc(staging)");
+        hs.slot_bytes = need;
+    }
+    // the copies start after the caller's earlier work on `stream`
+    check(cudaEventRecord(hs.start, stream), "cudaEventRecord");
+    check(cudaStreamWaitEvent(hs.h2d, hs.start, 0), "cudaStreamWaitEvent");
+    const auto* src = static_cast<const unsigned char*>(in);
+    auto* dst = static_cast<unsigned char*>(out);
+    int last = -1;
+    for (uint64_t l0 = 0; l0 < batch; l0 += chunk_lines) {
+        const uint64_t nl = std::min<uint64_t>(chunk_lines, batch - l0);
+        const size_t bytes = static_cast<size_t>(nl) * line_bytes;
+        const int slot = static_cast<int>(hs.next++ % kHostSlots);
+        unsigned char* a = hs.mem + static_cast<size_t>(slot) * 2 * hs.slot_bytes;
+        unsigned char* b = a + hs.slot_bytes;
+        if (hs.pending[slot]) check(cudaStreamWaitEvent(hs.h2d, hs.freed[slot], 0), "cudaStreamWaitEvent");
+        check(cudaMemcpyAsync(a, src + l0 * line_bytes, bytes, cudaMemcpyHostToDevice, hs.h2d), "copy in");
+        check(cudaEventRecord(hs.loaded[slot], hs.h2d), "cudaEventRecord");
+        check(cudaStreamWaitEvent(stream, hs.loaded[slot], 0), "cudaStreamWaitEvent");
+        unsigned char* cur = a;
+        for (uint32_t i = 0; i < count; ++i) {
+            auto* p = static_cast<DevicePlan*>(stages[i].plan);
+            if (p->spec.req.in_place) {
+                execute_plan(p, cur, cur, stream, nl, stages[i].direction, stages[i].normalization);
+            } else {
+                unsigned char* other = cur == a ? b : a;
+                execute_plan(p, cur, other, stream, nl, stages[i].direction, stages[i].normalization);
+                cur = other;
+            }
+        }
+        check(cudaEventRecord(hs.computed[slot], stream), "cudaEventRecord");
+        check(cudaStreamWaitEvent(hs.d2h, hs.computed[slot], 0), "cudaStreamWaitEvent");
+        check(cudaMemcpyAsync(dst + l0 * line_bytes, cur, bytes, cudaMemcpyDeviceToHost, hs.d2h), "copy out");
+        check(cudaEventRecord(hs.freed[slot], hs.d2h), "cudaEventRecord");
+        hs.pending[slot] = true;
+        last = slot;
+    }
+    // the caller's stream completes after the last copy-out (copy-outs run in order)
+    if (last >= 0) check(cudaStreamWaitEvent(stream, hs.freed[last], 0), "cudaStreamWaitEvent");
 }
 
 // ---------------------------------------------------------------- autotuner
@@ -1256,24 +1492,39 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
             "},\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
     } else {
         s = sfb::describe_plan(p->spec);
+        int fused = 0;
+        for (size_t i = 0; i + 1 < p->passes.size(); ++i) fused += p->passes[i].fused4 ? 1 : 0;
+        if (fused && !s.empty() && s.back() == '}')
+            s = s.substr(0, s.size() - 1) + ",\"fused_fourstep\":" + std::to_string(fused) + "}";
     }
     if (s.size() + 1 > cap) return -1;
     std::memcpy(buf, s.c_str(), s.size() + 1);
     return static_cast<int>(s.size());
 }
 
+namespace sfb {
+namespace {
+// Kernel launches of one execute of a complex plan (a fused four-step runs two passes in one).
+int pass_launches(const DevicePlan* p) {
+    int n = static_cast<int>(p->passes.size());
+    for (size_t i = 0; i + 1 < p->passes.size(); ++i) n -= p->passes[i].fused4 ? 1 : 0;
+    return n;
+}
+}  // namespace
+}  // namespace sfb
+
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void* plan) {
     const auto* p = static_cast<const sfb::DevicePlan*>(plan);
-    if (p && p->real_md) {
+    if (!p) return -1;
+    if (p->real_md) {
         const sfb::DevicePlan* last = p->inner.get();
-        return (last->real_fused ? 1 : static_cast<int>(last->inner->passes.size()) + 1) +
-               static_cast<int>(p->outer->passes.size());
+        return (last->real_fused ? 1 : sfb::pass_launches(last->inner.get()) + 1) + sfb::pass_launches(p->outer.get());
     }
-    if (p && p->real_kind) return p->real_fused ? 1 : static_cast<int>(p->inner->passes.size()) + 1;
-    if (p && p->strided)
-        return static_cast<int>(p->inner->passes.size()) +
+    if (p->real_kind) return p->real_fused ? 1 : sfb::pass_launches(p->inner.get()) + 1;
+    if (p->strided)
+        return sfb::pass_launches(p->inner.get()) +
                (p->interleaved ? 0 : (p->in_contig ? 0 : 1) + (p->out_contig ? 0 : 1));
-    return p ? static_cast<int>(p->passes.size()) : -1;
+    return sfb::pass_launches(p);
 }
 
 SYCLFFT_B200_EXPORT const char* syclfft_b200_version(void) { return "syclfft-b200 0.1"; }
@@ -1339,14 +1590,62 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void* plan, const void* in, void
     }
 }
 
-SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void* plan) {
-    const auto* p = static_cast<const sfb::DevicePlan*>(plan);
-    if (!p || !p->status) return -1;
+namespace sfb {
+namespace {
+// Every plan of a plan tree (a real or strided plan holds its complex plans in inner / outer).
+template <class F>
+void for_each_plan(DevicePlan* p, F&& f) {
+    if (!p) return;
+    f(p);
+    for_each_plan(p->inner.get(), f);
+    for_each_plan(p->outer.get(), f);
+}
+
+// First non-zero status word of the tree; with `clear`, every word is reset to 0.
+int read_status(DevicePlan* p, bool clear) {
     int value = 0;
-    int prev = 0;
-    cudaGetDevice(&prev);
-    if (prev != p->device) cudaSetDevice(p->device);
-    const cudaError_t e = cudaMemcpy(&value, p->status, sizeof(int), cudaMemcpyDeviceToHost);
-    if (prev != p->device) cudaSetDevice(prev);
-    return e == cudaSuccess ? value : -1;
+    for_each_plan(p, [&](DevicePlan* q) {
+        if (!q->status) return;
+        const int v = clear ? __atomic_exchange_n(q->status, 0, __ATOMIC_SEQ_CST)
+                            : __atomic_load_n(q->status, __ATOMIC_SEQ_CST);
+        if (!value) value = v;
+    });
+    return value;
+}
+}  // namespace
+}  // namespace sfb
+
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_host(const syclfft_b200_host_stage_v1* stages, uint32_t count,
+                                                  const void* in, void* out, uint64_t batch, void* stream, char* err,
+                                                  size_t cap) {
+    try {
+        sfb::execute_host(stages, count, in, out, batch, static_cast<cudaStream_t>(stream));
+        return 0;
+    } catch (const std::exception& e) {
+        sfb::set_error(err, cap, e.what());
+        return 1;
+    }
+}
+
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void* plan) {
+    auto* p = const_cast<sfb::DevicePlan*>(static_cast<const sfb::DevicePlan*>(plan));
+    if (!p || !p->status) return -1;
+    return sfb::read_status(p, false);
+}
+
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_take_status(void* plan) {
+    auto* p = static_cast<sfb::DevicePlan*>(plan);
+    if (!p || !p->status) return -1;
+    return sfb::read_status(p, true);
+}
+
+SYCLFFT_B200_EXPORT int syclfft_b200_plan_set_wait_limit(void* plan, int64_t polls) {
+    auto* p = static_cast<sfb::DevicePlan*>(plan);
+    if (!p) return -1;
+    const long long v = polls < 0 ? sfb::kSpinLimit : static_cast<long long>(polls);
+    sfb::for_each_plan(p, [&](sfb::DevicePlan* q) {
+        std::lock_guard<std::mutex> lock(q->mu);
+        q->wait_polls = v;
+    });
+    return 0;
 }

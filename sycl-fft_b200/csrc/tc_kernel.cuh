@@ -23,9 +23,9 @@
 // mbarrier, reads its row back from tensor memory (tcgen05.ld, the thread's own lane) and
 // stores the outputs (exchange buffer, or HBM for the last stage).
 //
-// Waits on the MMA mbarrier are bounded: after kSpinLimit polls the CTA records a timeout
-// in the plan's status word, waits (bounded again) for the commit, frees its tensor memory
-// and returns.
+// Waits on the MMA mbarrier are bounded: after P.wait_polls polls the CTA records a timeout
+// in the plan's status word, waits (bounded again, kSpinLimit polls) for the commit, frees
+// its tensor memory and returns.
 #pragma once
 
 #include <cstdint>
@@ -48,6 +48,7 @@ struct TcParams {
     // hi[a] = W_N^(64a) for a < ceil(N/64), then lo[b] = W_N^b for b < 64.
     const void* tw = nullptr;
     int* status = nullptr;     // set to 2 if an MMA wait timed out
+    long long wait_polls = kSpinLimit;  // polls before an MMA wait gives up
 };
 
 // Byte offset of element kk of row `row` in the canonical K-major no-swizzle layout: 8-row x
@@ -300,13 +301,7 @@ __global__ void __launch_bounds__(TcShape<R, S, L, G>::THREADS, 1)
             // One thread polls the MMA barrier; the others wait in the named barrier.
             bool done = true;
             if (t == 0) {
-                done = false;
-                for (long long spin = 0; spin < kSpinLimit; ++spin) {
-                    if (mbar_try_wait(bar, phase)) {
-                        done = true;
-                        break;
-                    }
-                }
+                done = mbar_wait_bounded(bar, phase, P.wait_polls);
                 tc_fence_before();
             }
             if (group_sync_or(bar_id, ROWS, !done)) {
@@ -346,10 +341,9 @@ __global__ void __launch_bounds__(TcShape<R, S, L, G>::THREADS, 1)
     }
     cp_async_wait_all();  // no copy into shared memory outlives the CTA
     if (stuck && t == 0) {
-        if (P.status) atomicExch(P.status, 2);
+        report_status(P.status, 2);
         // let the outstanding MMAs finish (bounded) before their tensor memory is released
-        for (long long spin = 0; spin < kSpinLimit; ++spin)
-            if (mbar_try_wait(bar, phase)) break;
+        mbar_wait_bounded(bar, phase, kSpinLimit);
     }
     tc_fence_before();
     __syncthreads();

@@ -9,8 +9,8 @@
 // column-mode layout of the size-specialised stages (element (a, w) at a * W + w), so the
 // first stage reads it in place and the last stage stores to HBM with the twiddle fused.
 //
-// Waits are bounded: after kSpinLimit polls the CTA records a timeout in the status word,
-// waits (bounded again) for its other copy in flight and returns.
+// Waits are bounded: after P.wait_polls polls the CTA records a timeout in the status word,
+// waits (bounded again, kSpinLimit polls) for its copies in flight and returns.
 #pragma once
 
 #include <cuda.h>
@@ -34,6 +34,7 @@ struct TmaColParams {
     int conj_in = 0, conj_out = 0;
     double scale = 1.0;
     int* status = nullptr;  // set to 3 if a tile wait timed out
+    long long wait_polls = kSpinLimit;  // polls before a tile wait gives up
 };
 
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* bar) {
@@ -90,20 +91,14 @@ __global__ void __launch_bounds__(W * TPL)
         const int b = NBUF > 1 ? (it & 1) : 0;
         const int64_t next = tile + gridDim.x;
         if (NBUF > 1 && tid == 0 && next < P.tiles) issue(next, b ^ 1);  // the other buffer was released below
-        bool ok = false;
-        for (long long spin = 0; spin < kSpinLimit; ++spin) {
-            if (mbar_try_wait(&bar[b], phase[b])) {
-                ok = true;
-                break;
-            }
-        }
+        const bool ok = mbar_wait_bounded(&bar[b], phase[b], P.wait_polls);
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
-                if (P.status) atomicExch(P.status, 3);
-                // the prefetch of the other buffer may still be in flight: wait for it (bounded)
-                if (NBUF > 1 && next < P.tiles)
-                    for (long long spin = 0; spin < kSpinLimit; ++spin)
-                        if (mbar_try_wait(&bar[b ^ 1], phase[b ^ 1])) break;
+                report_status(P.status, 3);
+                // the tile given up on and the prefetch of the other buffer may still be in
+                // flight: let them land (bounded) before the shared memory is released
+                mbar_wait_bounded(&bar[b], phase[b], kSpinLimit);
+                if (NBUF > 1 && next < P.tiles) mbar_wait_bounded(&bar[b ^ 1], phase[b ^ 1], kSpinLimit);
             }
             __syncthreads();
             return;

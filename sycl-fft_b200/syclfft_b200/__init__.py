@@ -15,6 +15,7 @@ from .api import (  # noqa: F401
     data_layout,
     direction,
     error_code,
+    execute_host,
     normalization,
     placement,
     plan_dft_1d,
@@ -33,7 +34,7 @@ from .api import (  # noqa: F401
 from . import _provider  # noqa: F401
 
 __all__ = [
-    "Plan", "RealPlan", "SyclfftError", "data_layout", "direction", "error_code", "normalization", "placement", "plan_dft_1d",
+    "Plan", "RealPlan", "SyclfftError", "data_layout", "direction", "error_code", "execute_host", "normalization", "placement", "plan_dft_1d",
     "plan_dft_2d", "plan_dft_3d", "plan_dft_r2c_1d", "plan_dft_c2r_1d", "plan_dft_r2c", "plan_dft_c2r", "plan_many_dft", "plan_options", "planning_mode", "provider",
     "query_providers",
 ]

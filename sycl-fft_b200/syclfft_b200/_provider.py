@@ -68,6 +68,14 @@ class GroupItemV1(ctypes.Structure):
     ]
 
 
+class HostStageV1(ctypes.Structure):
+    _fields_ = [
+        ("plan", ctypes.c_void_p),
+        ("direction", ctypes.c_int32),
+        ("normalization", ctypes.c_int32),
+    ]
+
+
 class ProviderV1(ctypes.Structure):
     _fields_ = [
         ("abi_version", ctypes.c_uint32),
@@ -87,6 +95,9 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_plan_launches",
     "syclfft_b200_version",
     "syclfft_b200_plan_status",
+    "syclfft_b200_plan_take_status",
+    "syclfft_b200_plan_set_wait_limit",
+    "syclfft_b200_execute_host",
     "syclfft_b200_create_ex",
     "syclfft_b200_execute_batch",
     "syclfft_b200_execute_ex",
@@ -131,6 +142,14 @@ def load(path: str | None = None):
                                             ctypes.c_size_t]
     lib.syclfft_b200_plan_status.restype = ctypes.c_int
     lib.syclfft_b200_plan_status.argtypes = [ctypes.c_void_p]
+    lib.syclfft_b200_plan_take_status.restype = ctypes.c_int
+    lib.syclfft_b200_plan_take_status.argtypes = [ctypes.c_void_p]
+    lib.syclfft_b200_plan_set_wait_limit.restype = ctypes.c_int
+    lib.syclfft_b200_plan_set_wait_limit.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+    lib.syclfft_b200_execute_host.restype = ctypes.c_int
+    lib.syclfft_b200_execute_host.argtypes = [ctypes.POINTER(HostStageV1), ctypes.c_uint32, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_char_p,
+                                              ctypes.c_size_t]
     lib.syclfft_b200_group_supports.restype = ctypes.c_int
     lib.syclfft_b200_group_supports.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
     lib.syclfft_b200_group_create.restype = ctypes.c_void_p

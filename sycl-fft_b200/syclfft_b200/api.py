@@ -143,6 +143,107 @@ def _torch():
     return torch
 
 
+_EVENT_CLS = None
+
+
+def _event_class():
+    """ExecutionEvent: the torch.cuda.Event an execute returns (the stand-in for sycl::event),
+    which also reports a failed device wait. A bounded wait in a plan's kernel that gave up
+    leaves that execution's output incomplete and sets the plan's status word; the reference
+    reports a failed provider execution as error_code::execution_failed (src/sycl/sycl.cpp:
+    671-676), and so do synchronize() and wait_and_throw() here, once per failure."""
+    global _EVENT_CLS
+    if _EVENT_CLS is None:
+        torch = _torch()
+
+        class ExecutionEvent(torch.cuda.Event):
+            def __new__(cls, lib=None, handles=()):
+                self = super().__new__(cls)
+                self._lib = lib
+                self._handles = handles
+                return self
+
+            def synchronize(self):
+                super().synchronize()
+                self._check()
+
+            def wait_and_throw(self):
+                self.synchronize()
+
+            def _check(self):
+                for h in self._handles:
+                    code = self._lib.syclfft_b200_plan_take_status(h)
+                    if code > 0:
+                        raise SyclfftError(error_code.execution_failed,
+                                           f"a bounded wait in a B200 kernel gave up (status {code}); the output of "
+                                           "this execution is incomplete")
+
+        _EVENT_CLS = ExecutionEvent
+    return _EVENT_CLS
+
+
+def _host_tensor(t):
+    """True for a page-locked (pinned) CPU tensor: host USM in the reference's terms."""
+    torch = _torch()
+    return isinstance(t, torch.Tensor) and not t.is_cuda
+
+
+def execute_host(stages, input, output=None, batch=None, stream=None):
+    """Run `stages` -- (plan, direction or None, normalization or None) tuples, or plans -- one
+    after the other on transforms held in page-locked host tensors (B200 extension over the
+    reference's host-USM execute, sycl.cpp:72-85). The batch streams through the device in
+    chunks: copy in, the stages, copy out, on overlapping streams. `output` defaults to
+    `input` (in place). Returns the completion event (an ExecutionEvent)."""
+    torch = _torch()
+    items = []
+    for st in stages:
+        plan, d, n = (st, None, None) if isinstance(st, Plan) else (tuple(st) + (None, None))[:3]
+        if not getattr(plan, "_handle", None):
+            raise SyclfftError(error_code.invalid_state, "Cannot execute a moved-from plan")
+        items.append((plan, 0 if d is None else int(d), -1 if n is None else int(n)))
+    if not items:
+        raise SyclfftError(error_code.invalid_argument, "at least one stage is needed")
+    first = items[0][0]
+    output = input if output is None else output
+    for t, name in ((input, "input"), (output, "output")):
+        if not isinstance(t, torch.Tensor) or t.is_cuda:
+            raise SyclfftError(error_code.invalid_pointer, f"{name} must be a page-locked host tensor")
+        if not t.is_pinned():
+            raise SyclfftError(error_code.invalid_pointer,
+                               f"{name} is pageable host memory; host buffers must be page-locked (pin_memory)")
+        if t.dtype != first.dtype:
+            raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {first.dtype}")
+    b = first._batch if batch is None else int(batch)
+    need = b * (first._elements // first._batch)
+    for t, name in ((input, "input"), (output, "output")):
+        if not t.is_contiguous() or t.numel() < need:
+            raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {need} elements")
+    arr = (_provider.HostStageV1 * len(items))()
+    for i, (plan, d, n) in enumerate(items):
+        arr[i].plan, arr[i].direction, arr[i].normalization = plan._handle, d, n
+    s = stream or torch.cuda.current_stream(first._device)
+    locks = sorted({id(p): p for p, _, _ in items}.values(), key=id)
+    for p in locks:
+        p._lock.acquire()
+    try:
+        for p in locks:
+            if p._last_event is not None:
+                s.wait_event(p._last_event)
+        err = ctypes.create_string_buffer(_provider.ERR_CAP)
+        rc = first._lib.syclfft_b200_execute_host(arr, len(items), input.data_ptr(), output.data_ptr(), b,
+                                                  s.cuda_stream, err, _provider.ERR_CAP)
+        if rc != 0 or err.value:
+            raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
+        ev = _event_class()(first._lib, tuple(p._handle for p in locks))
+        ev.record(s)
+        for p in locks:
+            p._last_event = ev
+        return ev
+    finally:
+        for p in locks:
+            p._lock.release()
+
+
 def _checked_element_count(lengths, batch):
     if len(lengths) == 0 or len(lengths) > 3:
         raise SyclfftError(error_code.invalid_argument, "FFT rank must be between 1 and 3")
@@ -220,6 +321,7 @@ class Plan:
         self._handle = h
         self._lock = threading.Lock()
         self._last_event = None
+        self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
 
     # -- properties (syclfft.hpp:62-66) --
     def shape(self):
@@ -264,9 +366,11 @@ class Plan:
             if t == 0:
                 raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
             return t
-        if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        if isinstance(t, torch.Tensor) and not t.is_cuda and t.is_pinned():
+            pass  # page-locked host memory is device-accessible (read over the bus)
+        elif not isinstance(t, torch.Tensor) or not t.is_cuda:
             raise SyclfftError(error_code.invalid_pointer, f"{name} is not a device allocation in the plan context")
-        if t.device.index != self._device:
+        elif t.device.index != self._device:
             raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
         if t.dtype != self.dtype:
             raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {self.dtype}")
@@ -276,35 +380,53 @@ class Plan:
         return t.data_ptr()
 
     def execute(self, a, b=None, dependencies=None, stream=None):
-        """execute(inout[, deps]) for in-place plans, execute(input, output[, deps]) otherwise."""
+        """execute(inout[, deps]) for in-place plans, execute(input, output[, deps]) otherwise.
+
+        Buffers are CUDA tensors or raw device pointers; page-locked host tensors on both sides
+        (host USM, which the reference's execute accepts, sycl.cpp:72-85) stream through the
+        device in overlapped chunks (execute_host); a page-locked host tensor on one side only
+        is read or written by the kernels directly over the bus. Returns an ExecutionEvent."""
         if not getattr(self, "_handle", None):
             raise SyclfftError(error_code.invalid_state, "Cannot execute a moved-from plan")
         one_pointer = b is None
-        inp = self._pointer(a, "input")
-        out = inp if one_pointer else self._pointer(b, "output")
         pl = self._options.placement
         if pl == placement.in_place and not one_pointer:
             raise SyclfftError(error_code.invalid_argument, "In-place plan must be executed with execute(inout)")
         if pl == placement.out_of_place and one_pointer:
             raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires input and output arguments")
+        if _host_tensor(a) and (one_pointer or _host_tensor(b)) and not isinstance(self, RealPlan) \
+                and self._extent["input"] == self._elements and self._extent["output"] == self._elements:
+            if pl == placement.out_of_place and a.data_ptr() == b.data_ptr():
+                raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires distinct allocations")
+            torch = _torch()
+            s = stream or torch.cuda.current_stream(self._device)
+            for dep in dependencies or ():
+                s.wait_event(dep)
+            return execute_host([self], a, a if one_pointer else b, stream=s)
+        inp = self._pointer(a, "input")
+        out = inp if one_pointer else self._pointer(b, "output")
         if pl == placement.out_of_place and inp == out:
             raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires distinct allocations")
         torch = _torch()
         s = stream or torch.cuda.current_stream(self._device)
         with self._lock:
-            with torch.cuda.stream(s):
+            if s == torch.cuda.current_stream(self._device):
                 capturing = torch.cuda.is_current_stream_capturing()
+            else:
+                with torch.cuda.stream(s):
+                    capturing = torch.cuda.is_current_stream_capturing()
             for dep in dependencies or ():
                 s.wait_event(dep)
             if self._last_event is not None and not capturing:
                 # A graph cannot depend on work outside its capture; captured launches run
                 # only at replay, which the caller orders against earlier executes.
                 s.wait_event(self._last_event)
-            err = ctypes.create_string_buffer(_provider.ERR_CAP)
+            err = self._err
+            err[0] = b"\0"
             rc = self._api.execute(self._handle, inp, out, s.cuda_stream, err, _provider.ERR_CAP)
             if rc != 0 or err.value:
                 raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
-            ev = torch.cuda.Event()
+            ev = _event_class()(self._lib, (self._handle,))
             ev.record(s)
             # an event recorded inside a capture belongs to the graph: ordering of replays
             # against later executes is the caller's, as for any captured work
@@ -315,7 +437,10 @@ class Plan:
         h = getattr(self, "_handle", None)
         if h:
             if self._last_event is not None:
-                self._last_event.synchronize()
+                try:
+                    self._last_event.synchronize()
+                except SyclfftError:
+                    pass  # a failed wait was already reported or is moot once the plan goes
             self._api.destroy(h)
             self._handle = None
 
@@ -389,6 +514,7 @@ class RealPlan(Plan):
         self._handle = h
         self._lock = threading.Lock()
         self._last_event = None
+        self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
 
     @property
     def kind(self):

@@ -181,6 +181,8 @@ class Server:
         self.err = ctypes.create_string_buffer(ERR)
         self.plan_bytes = 0
         self.plans_created = 0
+        self.evictions = 0
+        self.max_waiting = 0
         self.pending = {}   # plan key -> future of a plan being created ahead of use
         self.pool = None
         self._gen = None
@@ -224,6 +226,7 @@ class Server:
             _, (oh, ob, oev) = self.plans.popitem(last=False)
             self.plan_bytes -= ob
             self.retired.append((oh, oev))
+            self.evictions += 1
         self._reap()
         return h
 
@@ -317,11 +320,23 @@ class Server:
             raise RuntimeError(self.err.value.decode())
 
     # ---------------------------------------------------------------- loops
+    def _keep(self, r: Request, keep_results):
+        """What a run keeps of a finished request's output before its buffer is reused: all of
+        it on the host (keep_results True) or what a callable returns for it."""
+        if callable(keep_results):
+            r.result = keep_results(r)
+        elif keep_results:
+            r.result = r.out.cpu()
+
     def run(self, requests, mode="served", keep_results=False):
         """Serve `requests` (sorted by arrival); returns statistics. mode 'served' (continuous
         batching), 'plain' (one request at a time on resident plans) or 'plan_per_request'
-        (one request at a time, each with its own plan created and destroyed around it)."""
+        (one request at a time, each with its own plan created and destroyed around it).
+        keep_results: False, True (every output copied to the host into r.result) or a
+        callable f(request) -> r.result, called once the output is complete."""
         torch = self.torch
+        self.evictions = 0
+        self.max_waiting = 0
         reqs = sorted(requests, key=lambda r: r.arrival)
         for r in reqs:
             r.nbytes = 2 * r.elements * (16 if r.double else 8)
@@ -363,8 +378,7 @@ class Server:
                 ev.synchronize()
                 self.api.destroy(h)
                 r.t_done = start.elapsed_time(ev) / 1e3
-                if keep_results:
-                    r.result = r.out.cpu()
+                self._keep(r, keep_results)
                 self._release(r)
         elif mode == "plain":
             s = self.streams[0]
@@ -380,8 +394,7 @@ class Server:
                 h[2] = ev
                 ev.synchronize()
                 r.t_done = start.elapsed_time(ev) / 1e3
-                if keep_results:
-                    r.result = r.out.cpu()
+                self._keep(r, keep_results)
                 self._release(r)
         else:
             self._serve(reqs, t0, start, keep_results)
@@ -398,7 +411,7 @@ class Server:
             "p50_ms": 1e3 * lat_sorted[len(lat) // 2], "p99_ms": 1e3 * lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))],
             "mean_ms": 1e3 * statistics.mean(lat), "plans_resident": len(self.plans),
             "plans_created": self.plans_created, "groups": len(self.groups),
-            "plan_bytes": self.plan_bytes,
+            "plan_bytes": self.plan_bytes, "plan_evictions": self.evictions, "max_waiting": self.max_waiting,
         }
 
     def _serve(self, reqs, t0, start, keep_results):
@@ -423,6 +436,7 @@ class Server:
                 waiting.append(reqs[nxt])
                 self._prefetch(reqs[nxt])  # start its plan while it waits for admission
                 nxt += 1
+            self.max_waiting = max(self.max_waiting, len(waiting))
             # admission by HBM budget: FIFO, while the request's buffers fit in the arena
             bins = {}
             while waiting:
@@ -459,8 +473,7 @@ class Server:
                     t = start.elapsed_time(ev) / 1e3
                     for r in rs:
                         r.t_done = t
-                        if keep_results:
-                            r.result = r.out.cpu()
+                        self._keep(r, keep_results)
                         self._release(r)
                     completed += len(rs)
                     progressed = True

@@ -5,6 +5,7 @@
 // tests/test_frontend.py. Exit status 0 = every check passed.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -431,6 +432,61 @@ try {
     });
     expect_error(sf::error_code::invalid_argument,
                  [] { (void)sf::plan_many_dft<float>(sf::queue{}, {2, 2, 2, 2}, 1, sf::direction::forward); });
+    {
+        // Page-locked host buffers (host USM, which the reference's execute accepts,
+        // sycl.cpp:72-85) stream through the device in chunks: same values as the device path.
+        const std::size_t n = 4096, batch = 2100, count = n * batch;  // more than one 32 MiB chunk
+        std::complex<float>*hin = nullptr, *hout = nullptr;
+        check(cudaHostAlloc(reinterpret_cast<void**>(&hin), count * sizeof(std::complex<float>), 0) == cudaSuccess,
+              "cudaHostAlloc");
+        check(cudaHostAlloc(reinterpret_cast<void**>(&hout), count * sizeof(std::complex<float>), 0) == cudaSuccess,
+              "cudaHostAlloc");
+        std::vector<std::complex<float>> source(count);
+        for (std::size_t i = 0; i < count; ++i)
+            source[i] = {static_cast<float>((i * 5 + 1) % 9) / 4.f, static_cast<float>((i * 3 + 2) % 7) / 5.f};
+        std::copy(source.begin(), source.end(), hin);
+        device_buffer<std::complex<float>> din(count), dout(count);
+        din.write(source);
+        auto fft = sf::plan_many_dft<float>(sf::queue{}, {n}, batch, sf::direction::forward,
+                                            make_plan_options(sf::placement::out_of_place, sf::normalization::forward));
+        fft.execute(din.get(), dout.get()).wait_and_throw();
+        fft.execute(hin, hout).wait_and_throw();
+        const auto expected = dout.read();
+        auto close = [&](const std::complex<float>* got) {
+            for (std::size_t i = 0; i < count; ++i)
+                if (std::abs(got[i] - expected[i]) > 1e-6f * (1.f + std::abs(expected[i]))) return false;
+            return true;
+        };
+        check(close(hout), "host-buffer execute differs");
+        auto inplace = sf::plan_many_dft<float>(sf::queue{}, {n}, batch, sf::direction::forward,
+                                                make_plan_options(sf::placement::in_place, sf::normalization::forward));
+        inplace.execute(hin).wait_and_throw();
+        check(close(hin), "in-place host-buffer execute differs");
+        cudaFreeHost(hin);
+        cudaFreeHost(hout);
+    }
+    {
+        // A bounded device wait that gives up surfaces as execution_failed on wait_and_throw
+        // (the reference's code for a failed provider execution, sycl.cpp:671-676). The
+        // 13440-point plan runs the copy-pipelined kernel; SYCLFFT_B200_WAIT_POLLS=0 makes its
+        // copy waits give up at once (the copies still land before the blocks exit).
+        const std::size_t n = 13440, batch = 16, count = n * batch;
+        device_buffer<std::complex<float>> input(count), output(count);
+        std::vector<std::complex<float>> source(count, {1.f, 0.f});
+        input.write(source);
+        setenv("SYCLFFT_B200_WAIT_POLLS", "0", 1);
+        auto impatient = sf::plan_many_dft<float>(sf::queue{}, {n}, batch, sf::direction::forward);
+        unsetenv("SYCLFFT_B200_WAIT_POLLS");
+        auto failed = impatient.execute(input.get(), output.get());
+        expect_error(sf::error_code::execution_failed, [&] { failed.wait_and_throw(); });
+        failed.wait_and_throw();  // reported once
+        auto healthy = sf::plan_many_dft<float>(sf::queue{}, {n}, batch, sf::direction::forward);
+        healthy.execute(input.get(), output.get()).wait_and_throw();
+        const auto actual = output.read();
+        for (std::size_t b = 0; b < batch; ++b)
+            check(std::abs(actual[b * n].real() - float(n)) < 1e-2f && std::abs(actual[b * n + 1]) < 1e-2f,
+                  "transform after a reported timeout is wrong");
+    }
     std::cout << "front-end tests passed\n";
     return 0;
 } catch (const std::exception& ex) {

@@ -164,6 +164,22 @@ def test_parity_vs_oracle_and_fp64(sf, torch, oracle_mod, shape, batch, dbl, gau
         assert e_or <= max(tol, 2 * e_or64), f"vs oracle {e_or:.3e} (oracle vs FP64 {e_or64:.3e})"
 
 
+def test_config1_exact_case_vs_oracle(sf, torch, oracle_mod):
+    """The CPU-baseline workload exactly: complex<float> N=1024, batch 1, forward, out of place,
+    normalization none, re/im ~ U[-1, 1) from a seed; against the oracle and FP64."""
+    n = 1024
+    x = uniform_complex(n, 1, np.complex64)
+    out, p = run(sf, torch, x, [n], 1, -1, 0, False, in_place=False)
+    assert p.batch_count() == 1
+    ref64 = fp64_fft(x, [n], 1, -1)
+    ora = oracle_mod.OraclePlan([n], 1, -1, 0, False).execute(x)
+    tol = spec_tol(n, False)
+    assert rel_l2(out, ref64) <= tol
+    assert rel_l2(out, ora) <= max(tol, 2 * rel_l2(ora, ref64))
+    # the reference's element-wise bound (sycl_tests.cpp:242, float 4e-4) holds as well
+    assert np.all(np.abs(out - ora) <= 4e-4 * (1 + np.abs(ora)))
+
+
 GENERIC = [([4096], 16, False), ([13440], 2, False), ([256, 64], 2, True), ([64, 48, 40], 1, False),
            ([2048], 8, True), ([128, 256], 2, False), ([65536], 4, True)]
 

@@ -124,6 +124,55 @@ def test_serving_alone_vs_mix(torch):
         srv.close()
 
 
+def test_serving_alone_vs_mix_full_stream_shape(torch):
+    """The serving configuration's request mix at its real shape: lengths up to 2^20 (powers of
+    two, 7-smooth, primes up to 65537), batches up to 512, 20% complex<double>, random
+    direction and normalization, Poisson arrivals at 50k/s; an admission budget small enough
+    that requests wait for memory, and a plan budget small enough that resident plans are
+    evicted. Every result must be the same served alone and in the mix: the L2 norm of each
+    output and 2048 sampled elements (fixed positions per request) within the float/double
+    tolerance, and a handful of outputs against an FP64 FFT in full."""
+    from syclfft_b200 import serving
+    reqs = serving.make_request_stream(count=600, rate=50000.0, seed=23)
+    assert max(r.lengths[0] for r in reqs) > 1 << 17 and max(r.batch for r in reqs) > 256
+    assert any(r.double for r in reqs) and any(r.lengths[0] > 60000 and not serving._smooth7(r.lengths[0])
+                                               for r in reqs)
+    largest = max(2 * r.elements * (16 if r.double else 8) for r in reqs)
+    full = {r.rid for r in sorted(reqs, key=lambda r: r.elements)[::60]}  # ten, small to large
+
+    def keep(r):
+        out = r.out.view(-1)
+        g = torch.Generator(device=out.device).manual_seed(r.rid)
+        idx = torch.randint(0, out.numel(), (2048,), device=out.device, generator=g)
+        norm = float(torch.linalg.vector_norm(out.to(torch.complex128)))
+        return norm, out[idx].cpu(), (out.cpu() if r.rid in full else None)
+
+    srv = serving.Server(budget_bytes=max(1.05 * largest, 6e9), streams=4, plan_budget_bytes=256e6)
+    try:
+        mixed = srv.run(reqs, mode="served", keep_results=keep)
+        results = {r.rid: r.result for r in reqs}
+        alone = srv.run(reqs, mode="plain", keep_results=keep)
+    finally:
+        srv.close()
+    assert mixed["max_waiting"] > 0, mixed      # admission had to wait for memory
+    assert mixed["plan_evictions"] > 0, mixed   # resident plans were evicted
+    for r in reqs:
+        n = r.lengths[0]
+        tol = spec_tol(n, r.double)
+        (na, sa, fa), (nb, sb, fb) = results[r.rid], r.result
+        assert abs(na - nb) <= tol * max(nb, 1e-30), (r, na, nb)
+        assert rel_l2(sa.numpy(), sb.numpy()) <= tol, r
+    for r in reqs:
+        if r.rid not in full:
+            continue
+        x = serving.synthetic_input(r).cpu().numpy()
+        n = r.lengths[0]
+        ref = fp64_fft(x, [n], r.batch, r.direction, norm_scale(r.normalization, r.direction, n))
+        assert rel_l2(results[r.rid][2].numpy(), ref) <= spec_tol(n, r.double), r
+    for st in (mixed, alone):
+        assert st["requests"] == len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
+
+
 def test_cuda_graph_capture_and_replay(torch):
     """Plan executes and grouped launches are capturable in a CUDA graph; replays with new
     input data give the same results as direct execution."""

@@ -54,8 +54,7 @@ def noalloc(torch, x, out, n, batch, direction, norm):
     return rc, err.value.decode()
 
 
-def test_noalloc_matches_plan_entry_point_twice(torch):
-    cases = [(65536, 8, -1, 3), (1 << 20, 2, 1, 2)]  # two calls in a row, different length and direction
+def check_against_plan(torch, cases):
     for n, batch, direction, norm in cases:
         g = torch.Generator(device="cuda").manual_seed(n + batch)
         x = torch.complex(torch.rand(n * batch, device="cuda", generator=g) * 2 - 1,
@@ -72,9 +71,22 @@ def test_noalloc_matches_plan_entry_point_twice(torch):
         # also against an FP64 FFT of the same input
         xs = x.view(batch, n)[:2].cpu().numpy().astype(np.complex128)
         f = np.fft.fft(xs, axis=1) if direction == -1 else np.fft.ifft(xs, axis=1) * n
-        scale = {3: 1 / math.sqrt(n), 2: (1 / n if direction == 1 else 1.0)}[norm]
+        scale = {0: 1.0, 1: (1 / n if direction == -1 else 1.0), 2: (1 / n if direction == 1 else 1.0),
+                 3: 1 / math.sqrt(n)}[norm]
         got = out.view(batch, n)[:2].cpu().numpy()
         assert np.linalg.norm(got - f * scale) / np.linalg.norm(f * scale) <= tol
+
+
+def test_noalloc_matches_plan_entry_point_twice(torch):
+    # two calls in a row, different length and direction
+    check_against_plan(torch, [(65536, 8, -1, 3), (1 << 20, 2, 1, 2)])
+
+
+@pytest.mark.parametrize("case", [(1 << 15, 1, 1, 0), (1 << 20, 4, -1, 1), (1 << 17, 3, 1, 2)])
+def test_noalloc_boundary_cases(torch, case):
+    # the shortest length (128 x 256 split), a batch exactly at the 4 Mi element limit, an odd
+    # batch; every normalization in one direction or the other
+    check_against_plan(torch, [case])
 
 
 def test_noalloc_in_place_and_limits(torch):
@@ -90,3 +102,13 @@ def test_noalloc_in_place_and_limits(torch):
     assert rc != 0 and "limited" in msg
     rc, msg = noalloc(torch, big, big, 3 * 4096, 1, -1, 0)
     assert rc != 0 and "power-of-two" in msg
+    # a view 4 bytes into a buffer: refused on the host before anything is launched
+    raw = torch.zeros(2 * n + 2, dtype=torch.float32, device="cuda")
+    base = raw.data_ptr()
+    err = ctypes.create_string_buffer(1024)
+    from syclfft_b200 import _provider
+    rc = _provider.load().syclfft_b200_execute_noalloc_c2c_f32(base + 4, base + 4, n, 1, -1, 0,
+                                                               torch.cuda.current_stream().cuda_stream, err, 1024)
+    assert rc != 0 and "aligned" in err.value.decode()
+    torch.cuda.synchronize()
+    assert int(torch.count_nonzero(raw)) == 0

@@ -25,4 +25,18 @@ const Fused4Entry* find_fused4(bool dbl, int col_id, int row_id);
 cudaError_t launch_fused4(const Fused4Entry& e, Fused4Params& p, const void* in, void* out, void* scratch,
                           cudaStream_t stream);
 
+struct FusedBlueEntry {
+    int id, dbl, n1, w1, colf_id, n2, w2, rows_id, coli_id, threads;
+    int64_t smem;
+};
+
+// The fused Bluestein kernel for the three size-specialised Bluestein passes colf_id, rows_id,
+// coli_id (bluestein_catalog.h), or nullptr.
+const FusedBlueEntry* find_fusedblue(bool dbl, int colf_id, int rows_id, int coli_id);
+
+// Launches entry `e` over `p.lines` lines (ring and lag chosen as for launch_fused4; the ring
+// holds M-point slots of `scratch`, which must hold `lines` of them, lines >= 4).
+cudaError_t launch_fusedblue(const FusedBlueEntry& e, FusedBlueParams& p, const void* in, void* out, void* scratch,
+                             cudaStream_t stream);
+
 }  // namespace sfb

@@ -54,17 +54,17 @@ struct Fused4Launcher {
         if (e != cudaSuccess) return e;
         const int64_t grid = int64_t(sms) * per_sm;
         int lag = 0, ring = 0;
-        if (!fused4_geometry(grid, TILES, p.lines, kFused4MaxRing, &lag, &ring)) return cudaErrorInvalidValue;
+        if (!fused_geometry(grid, TILES, p.lines, 2, kFused4MaxRing, &lag, &ring)) return cudaErrorInvalidValue;
         p.lag = lag;
         p.ring = ring;
         const int64_t tickets = p.lines * TILES;
-        if (tickets >= int64_t(UINT_MAX) - grid) return cudaErrorInvalidValue;
+        if (tickets >= int64_t(INT_MAX)) return cudaErrorInvalidValue;
         auto* ctrl = reinterpret_cast<unsigned*>(static_cast<C*>(scratch) + int64_t(ring) * L);
         e = cudaMemsetAsync(ctrl, 0, kFused4CtrlWords * sizeof(unsigned), stream);
         if (e != cudaSuccess) return e;
-        const int64_t blocks = grid < tickets ? grid : tickets;
+        // one block per tile; the resident blocks (grid) only set the lag
         fft_fused4_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>
-            <<<static_cast<unsigned>(blocks), THREADS, static_cast<size_t>(smem()), stream>>>(
+            <<<static_cast<unsigned>(tickets), THREADS, static_cast<size_t>(smem()), stream>>>(
                 p, static_cast<const C*>(in), static_cast<C*>(out), static_cast<C*>(scratch), ctrl);
         return cudaGetLastError();
     }
@@ -82,7 +82,94 @@ const Fused4Entry kEntries[] = {
 #undef SFB_X
 };
 
+template <class T, int N1, int TPL1, int W1, int N2, int TPL2, int W2, int THREADS, int MINB, class RC, class RR>
+struct FusedBlueLauncher {
+    static constexpr int64_t smem() {
+        constexpr int64_t a = int64_t(N1) * W1;
+        constexpr int64_t b = int64_t(W2) * kpitch<T, N2>();
+        return (a > b ? a : b) * int64_t(sizeof(cplx<T>));
+    }
+    static cudaError_t resident(int* per_sm) {
+        static std::atomic<int> known[kMaxDevices];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        int k = known[dev].load();
+        if (k <= 0) {
+            auto kernel = fft_fusedblue_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>;
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem()));
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, THREADS, static_cast<size_t>(smem()));
+            if (e != cudaSuccess) return e;
+            if (k <= 0) return cudaErrorInvalidConfiguration;
+            known[dev].store(k);
+        }
+        *per_sm = k;
+        return cudaSuccess;
+    }
+    static cudaError_t run(FusedBlueParams& p, const void* in, void* out, void* scratch, cudaStream_t stream) {
+        using C = cplx<T>;
+        constexpr int64_t M = int64_t(N1) * N2;
+        constexpr int TILES = 2 * (N2 / W1) + N1 / W2;  // tickets per line
+        int per_sm = 0;
+        cudaError_t e = resident(&per_sm);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0;
+        e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        const int64_t grid = int64_t(sms) * per_sm;
+        int lag = 0, ring = 0;
+        if (!fused_geometry(grid, TILES, p.lines, 3, kFused4MaxRing, &lag, &ring)) return cudaErrorInvalidValue;
+        p.lag = lag;
+        p.ring = ring;
+        const int64_t tickets = p.lines * TILES;
+        if (tickets >= int64_t(INT_MAX)) return cudaErrorInvalidValue;
+        auto* ctrl = reinterpret_cast<unsigned*>(static_cast<C*>(scratch) + int64_t(ring) * M);
+        e = cudaMemsetAsync(ctrl, 0, kFused4CtrlWords * sizeof(unsigned), stream);
+        if (e != cudaSuccess) return e;
+        // one block per tile; the resident blocks (grid) only set the lag
+        fft_fusedblue_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>
+            <<<static_cast<unsigned>(tickets), THREADS, static_cast<size_t>(smem()), stream>>>(
+                p, static_cast<const C*>(in), static_cast<C*>(out), static_cast<C*>(scratch), ctrl);
+        return cudaGetLastError();
+    }
+};
+
+#define SFB_FUSEDBLUE_TYPE(ID, DBL, N1, TPL1, W1, CF, N2, TPL2, W2, RW, CI, THREADS, MINB, RC, RR)              \
+    FusedBlueLauncher<std::conditional_t<(DBL) != 0, double, float>, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, \
+                      SFB_RADICES RC, SFB_RADICES RR>
+
+const FusedBlueEntry kBlueEntries[] = {
+#define SFB_X(ID, DBL, N1, TPL1, W1, CF, N2, TPL2, W2, RW, CI, THREADS, MINB, RC, RR) \
+    {ID, DBL, N1, W1, CF, N2, W2, RW, CI, THREADS,                                    \
+     SFB_FUSEDBLUE_TYPE(ID, DBL, N1, TPL1, W1, CF, N2, TPL2, W2, RW, CI, THREADS, MINB, RC, RR)::smem()},
+    SFB_FUSEDBLUE_CATALOG(SFB_X)
+#undef SFB_X
+};
+
 }  // namespace
+
+const FusedBlueEntry* find_fusedblue(bool dbl, int colf_id, int rows_id, int coli_id) {
+    for (const auto& e : kBlueEntries)
+        if (e.dbl == (dbl ? 1 : 0) && e.colf_id == colf_id && e.rows_id == rows_id && e.coli_id == coli_id) return &e;
+    return nullptr;
+}
+
+cudaError_t launch_fusedblue(const FusedBlueEntry& entry, FusedBlueParams& p, const void* in, void* out,
+                             void* scratch, cudaStream_t stream) {
+    switch (entry.id) {
+#define SFB_X(ID, DBL, N1, TPL1, W1, CF, N2, TPL2, W2, RW, CI, THREADS, MINB, RC, RR)                             \
+    case ID:                                                                                                    \
+        return SFB_FUSEDBLUE_TYPE(ID, DBL, N1, TPL1, W1, CF, N2, TPL2, W2, RW, CI, THREADS, MINB, RC, RR)::run( \
+            p, in, out, scratch, stream);
+        SFB_FUSEDBLUE_CATALOG(SFB_X)
+#undef SFB_X
+        default:
+            return cudaErrorInvalidDeviceFunction;
+    }
+}
 
 const Fused4Entry* find_fused4(bool dbl, int col_id, int row_id) {
     for (const auto& e : kEntries)

@@ -85,6 +85,9 @@ struct BoundPass {
     // four-step column pass whose row pass (the next pass) can run with it in one fused launch
     // (fused4_kernel.cuh), or nullptr
     const Fused4Entry* fused4 = nullptr;
+    // Bluestein forward column pass whose row and inverse column passes (the next two) can run
+    // with it in one fused launch, or nullptr
+    const FusedBlueEntry* fusedblue = nullptr;
 };
 
 TcParams to_tc(const PassParams& p, const void* tw, int* status) {
@@ -237,6 +240,7 @@ struct DevicePlan {
     std::vector<BoundPass> passes;
     cudaEvent_t done = nullptr;
     cudaEvent_t ready = nullptr;  // tables complete (recorded on the memory stream at creation)
+    bool ready_done = false;      // `ready` has completed: executes need not wait for it
     bool stream_scratch = false;  // scratch comes from the executing stream's arena
     std::mutex mu;
     // Real transforms (syclfft_b200_create_real): a complex plan of half the length, with the
@@ -522,6 +526,12 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         if (a.kind == "fourstep_cols" && b.kind == "fourstep_rows" && a.fixed_id >= 0 && b.fixed_id >= 0 &&
             a.p.mode == kModeC && b.p.mode == kModeK && a.dst == Buf::Scratch && b.src == Buf::Scratch)
             plan->passes[i].fused4 = find_fused4(req.dbl, a.fixed_id, b.fixed_id);
+        if (i + 2 < plan->passes.size() && a.kind == "bluestein_cols_fwd" && b.kind == "bluestein_rows_conv") {
+            const PassSpec& c = plan->passes[i + 2].spec_ref();
+            if (c.kind == "bluestein_cols_inv" && a.blue_id >= 0 && b.blue_id >= 0 && c.blue_id >= 0 &&
+                a.dst == Buf::Scratch && b.src == Buf::Scratch && b.dst == Buf::Scratch && c.src == Buf::Scratch)
+                plan->passes[i].fusedblue = find_fusedblue(req.dbl, a.blue_id, b.blue_id, c.blue_id);
+        }
     }
     return plan.release();
 }
@@ -1044,9 +1054,15 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     check(cudaStreamIsCapturing(stream, &cap), "cudaStreamIsCapturing");
     const bool capturing = cap != cudaStreamCaptureStatusNone;
-    if (plan->ready) {
+    if (plan->ready && !plan->ready_done) {
         if (!capturing) {
-            check(cudaStreamWaitEvent(stream, plan->ready, 0), "cudaStreamWaitEvent");
+            // no event query during a capture: it would invalidate the capture
+            if (cudaEventQuery(plan->ready) == cudaSuccess) {
+                plan->ready_done = true;  // the tables are complete: no further waits
+            } else {
+                cudaGetLastError();  // cudaErrorNotReady is not an error here
+                check(cudaStreamWaitEvent(stream, plan->ready, 0), "cudaStreamWaitEvent");
+            }
         } else {
             // A graph cannot depend on work outside its capture: finish the plan's tables on
             // the host now (relaxed mode lets this thread synchronize while a capture is open),
@@ -1097,6 +1113,25 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
             check(launch_fused4(*bp.fused4, f, buf(bp.spec_ref().src), buf(bq.spec_ref().dst), scratch, stream),
                   "FFT fused four-step launch");
             ++i;
+            continue;
+        }
+        if (bp.fusedblue && i + 2 < np && bp.p.n_outer >= 4) {
+            BoundPass bq = rescale(plan->passes[i + 1], batch, planned);
+            BoundPass br = rescale(plan->passes[i + 2], batch, planned);
+            if (flip || set_scale) {
+                apply_override(bq, false, false, flip, scale, set_scale);
+                apply_override(br, false, i + 3 == np, flip, scale, set_scale);
+            }
+            FusedBlueParams f;
+            f.lines = bp.p.n_outer;
+            f.wait_polls = plan->wait_polls;
+            f.status = plan->status;
+            f.a = bp.fp;
+            f.b = bq.fp;
+            f.c = br.fp;
+            check(launch_fusedblue(*bp.fusedblue, f, buf(bp.spec_ref().src), buf(br.spec_ref().dst), scratch, stream),
+                  "FFT fused Bluestein launch");
+            i += 2;
             continue;
         }
         launch_bound_pass(plan, bp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream);
@@ -1492,10 +1527,13 @@ SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void* plan, char* buf, 
             "},\"inner\":" + sfb::describe_plan(p->inner->spec) + "}";
     } else {
         s = sfb::describe_plan(p->spec);
-        int fused = 0;
+        int fused = 0, fusedblue = 0;
         for (size_t i = 0; i + 1 < p->passes.size(); ++i) fused += p->passes[i].fused4 ? 1 : 0;
+        for (size_t i = 0; i + 2 < p->passes.size(); ++i) fusedblue += p->passes[i].fusedblue ? 1 : 0;
         if (fused && !s.empty() && s.back() == '}')
             s = s.substr(0, s.size() - 1) + ",\"fused_fourstep\":" + std::to_string(fused) + "}";
+        if (fusedblue && !s.empty() && s.back() == '}')
+            s = s.substr(0, s.size() - 1) + ",\"fused_bluestein\":" + std::to_string(fusedblue) + "}";
     }
     if (s.size() + 1 > cap) return -1;
     std::memcpy(buf, s.c_str(), s.size() + 1);
@@ -1508,6 +1546,7 @@ namespace {
 int pass_launches(const DevicePlan* p) {
     int n = static_cast<int>(p->passes.size());
     for (size_t i = 0; i + 1 < p->passes.size(); ++i) n -= p->passes[i].fused4 ? 1 : 0;
+    for (size_t i = 0; i + 2 < p->passes.size(); ++i) n -= p->passes[i].fusedblue ? 2 : 0;
     return n;
 }
 }  // namespace

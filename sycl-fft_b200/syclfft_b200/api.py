@@ -238,6 +238,7 @@ def execute_host(stages, input, output=None, batch=None, stream=None):
         ev.record(s)
         for p in locks:
             p._last_event = ev
+            p._last_stream = s.cuda_stream
         return ev
     finally:
         for p in locks:
@@ -321,6 +322,7 @@ class Plan:
         self._handle = h
         self._lock = threading.Lock()
         self._last_event = None
+        self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
 
     # -- properties (syclfft.hpp:62-66) --
@@ -417,9 +419,10 @@ class Plan:
                     capturing = torch.cuda.is_current_stream_capturing()
             for dep in dependencies or ():
                 s.wait_event(dep)
-            if self._last_event is not None and not capturing:
+            if self._last_event is not None and not capturing and self._last_stream != s.cuda_stream:
                 # A graph cannot depend on work outside its capture; captured launches run
-                # only at replay, which the caller orders against earlier executes.
+                # only at replay, which the caller orders against earlier executes. On the
+                # stream of the previous execute, stream order already serialises them.
                 s.wait_event(self._last_event)
             err = self._err
             err[0] = b"\0"
@@ -431,6 +434,7 @@ class Plan:
             # an event recorded inside a capture belongs to the graph: ordering of replays
             # against later executes is the caller's, as for any captured work
             self._last_event = None if capturing else ev
+            self._last_stream = None if capturing else s.cuda_stream
             return ev
 
     def close(self):
@@ -514,6 +518,7 @@ class RealPlan(Plan):
         self._handle = h
         self._lock = threading.Lock()
         self._last_event = None
+        self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
 
     @property

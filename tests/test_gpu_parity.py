@@ -377,3 +377,35 @@ def test_pipelined_cluster_kernel(sf, torch, in_place, monkeypatch):
         assert len(passes) == 1 and passes[0]["cluster_pipe"] == 1, passes
         ref = fp64_fft(x, [n], batch, d, norm_scale(norm, d, n))
         assert rel_l2(out, ref) <= spec_tol(n, True)
+
+
+@pytest.mark.parametrize("shape,batch,dbl", [([65536], 8, False), ([65536], 6, True), ([65537], 6, False),
+                                             ([65537], 5, True), ([4099], 6, True), ([24, 65536], 1, False)],
+                         ids=lambda v: str(v))
+def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, batch, dbl):
+    """The fused launches (four-step columns + rows, Bluestein forward columns + rows + inverse
+    columns, with the intermediate in an L2-resident ring) against the same plan's separate
+    passes (SYCLFFT_B200_FUSED4=0) and FP64, both directions through execute_ex, with every
+    normalization."""
+    import ctypes
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 31 + n, dt)
+    xi = torch.from_numpy(x).cuda()
+    outs = {}
+    for fused in ("1", "0"):
+        monkeypatch.setenv("SYCLFFT_B200_FUSED4", fused)
+        p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)
+        desc = p.describe()
+        assert bool(desc.get("fused_fourstep") or desc.get("fused_bluestein")) == (fused == "1"), desc
+        for d, nm in ((-1, 0), (1, 2), (-1, 3)):
+            out = torch.empty_like(xi)
+            rc = p._lib.syclfft_b200_execute_ex(p._handle, xi.data_ptr(), out.data_ptr(), 0, d, nm,
+                                                torch.cuda.current_stream().cuda_stream, p._err, 1024)
+            assert rc == 0, p._err.value
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            assert rel_l2(got, fp64_fft(x, shape, batch, d, norm_scale(nm, d, n))) <= spec_tol(n, dbl), (fused, d, nm)
+            outs[(fused, d, nm)] = got
+    for d, nm in ((-1, 0), (1, 2), (-1, 3)):
+        assert rel_l2(outs[("1", d, nm)], outs[("0", d, nm)]) <= spec_tol(n, dbl)

@@ -11,9 +11,10 @@
 
 #define SFB_FUSED4_CATALOG(X)                                                   \
     X(0, 1, 256, 32, 8, 49, 256, 32, 8, 57, 256, 4, (8, 8, 4), (8, 8, 4))       \
-    X(1, 0, 256, 16, 16, 44, 256, 16, 16, 53, 256, 4, (16, 16), (16, 16))
+    X(1, 0, 256, 16, 16, 44, 256, 16, 16, 53, 256, 4, (16, 16), (16, 16))         \
+    X(2, 0, 112, 8, 24, 61, 120, 8, 16, 62, 192, 5, (16, 7), (8, 15))
 
-#define SFB_FUSED4_COUNT 2
+#define SFB_FUSED4_COUNT 3
 
 // Fused Bluestein kernels (fft_fusedblue_kernel): the three size-specialised Bluestein passes of
 // a convolution of length M = N1 * N2 (forward columns COLF_ID, rows ROWS_ID, inverse columns

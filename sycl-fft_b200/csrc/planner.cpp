@@ -2,6 +2,7 @@
 
 #include "cluster_catalog.h"
 #include "fixed_catalog.h"
+#include "fused4_catalog.h"
 #include "piped_catalog.h"
 #include "tc_catalog.h"
 #include "bluestein_catalog.h"
@@ -335,9 +336,21 @@ struct Builder {
         if (req.no_fixed) return;
         PassParams& p = ps.p;
         const FixedEntry* e = find_fixed(req.dbl, p.mode, p.n, feat);
-        if (!e || e->nstages != p.fft1.nstages) return;
-        for (int i = 0; i < e->nstages; ++i)
-            if (e->radices[i] != p.fft1.radix[i]) return;
+        if (!e) return;
+        // the entry's own radix sequence (it may use butterflies the runtime-parameterised
+        // kernel does not have, such as the prime-factor radix 15)
+        if (e->nstages != p.fft1.nstages || !std::equal(e->radices, e->radices + e->nstages, p.fft1.radix)) {
+            StageSeq q;
+            q.nstages = e->nstages;
+            int ns = 1;
+            for (int i = 0; i < e->nstages; ++i) {
+                q.radix[i] = e->radices[i];
+                q.ns[i] = ns;
+                ns *= e->radices[i];
+            }
+            if (ns != p.n) return;
+            p.fft1 = q;
+        }
         const int threads = round_up(e->w * e->tpl, 32);
         if (threads > e->maxt) return;
         if (feat == kFixedTw4) {
@@ -660,12 +673,31 @@ struct Builder {
         return true;
     }
 
+    // A four-step split of L whose column and row passes have size-specialised kernels that a
+    // fused four-step kernel (fused4_catalog.h) runs together.
+    bool fused_split(int64_t L, int64_t& n1, int64_t& n2) {
+        for (int64_t a = 2; a * 2 <= L; ++a) {
+            if (L % a) continue;
+            const int64_t b = L / a;
+            const FixedEntry* c = find_fixed(req.dbl, kModeC, static_cast<int>(a), kFixedTw4);
+            const FixedEntry* r = find_fixed(req.dbl, kModeK, static_cast<int>(b), kFixedTStore);
+            if (c && r && has_fused4(req.dbl, c->id, r->id)) {
+                n1 = a;
+                n2 = b;
+                return true;
+            }
+        }
+        return false;
+    }
+
     void axis(int ax, int64_t L, int64_t s, int64_t O, Buf& cur) {
         const bool bwd = req.direction == 1;
         const int64_t E = static_cast<int64_t>(plan.elements);
+        int64_t f1 = 0, f2 = 0;
+        const bool fused_instead = s == 1 && req.fused_single && !req.no_fixed && O >= 3 && fused_split(L, f1, f2);
         if (smooth7(static_cast<uint64_t>(L))) {
             const int mode = s == 1 ? kModeK : kModeC;
-            if (fits(L, mode)) {
+            if (fits(L, mode) && !fused_instead) {
                 PassSpec ps;
                 ps.kind = "single";
                 ps.axis = ax;
@@ -703,7 +735,12 @@ struct Builder {
                 }
             }
             int64_t n1, n2;
-            if (!split(L, n1, n2)) throw std::runtime_error("FFT length too large for this provider");
+            if (fused_instead) {
+                n1 = f1;
+                n2 = f2;
+            } else if (!split(L, n1, n2)) {
+                throw std::runtime_error("FFT length too large for this provider");
+            }
             plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(E));
             // column pass
             PassSpec a;
@@ -1220,6 +1257,18 @@ const TcEntry* find_tc(int n, bool cols) {
     for (const TcEntry& e : kTc)
         if (e.n == n && (e.cols != 0) == cols) return &e;
     return nullptr;
+}
+
+bool has_fused4(bool dbl, int col_id, int row_id) {
+    struct Pair { int dbl, col, row; };
+    static const Pair pairs[] = {
+#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR) {DBL, COL, ROW},
+        SFB_FUSED4_CATALOG(SFB_X)
+#undef SFB_X
+    };
+    for (const Pair& q : pairs)
+        if (q.dbl == (dbl ? 1 : 0) && q.col == col_id && q.row == row_id) return true;
+    return false;
 }
 
 const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {

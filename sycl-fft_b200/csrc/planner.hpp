@@ -83,6 +83,8 @@ struct FixedEntry {
     int nstages;
 };
 const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat);
+// A fused four-step kernel (fused4_catalog.h) runs these column and row entries together.
+bool has_fused4(bool dbl, int col_id, int row_id);
 
 // One entry of piped_catalog.h as seen by the host.
 struct PipedEntry {
@@ -125,6 +127,10 @@ struct PlanRequest {
     bool no_fixed = false;   // force the generic kernel (tests, tuning)
     bool no_cluster = false; // force the two-pass four-step for long lines
     bool no_piped = false;   // never use the copy-engine-pipelined kernels
+    // Lines that fit one block but have a fused four-step kernel (fused4_catalog.h) run as a
+    // four-step through it (column and row passes in one launch, L2-resident intermediate)
+    // instead of the single pass; needs at least 3 lines.
+    bool fused_single = false;
     bool use_tma = false;    // four-step column passes on the TMA-staged kernels (opt-in: measured
                              // level with the plain size-specialised kernel on B200)
     int cluster_p = 0;       // > 0: put long lines on the cluster kernel of this cluster size

@@ -388,6 +388,10 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags, 
     if (const char* k = std::getenv("SYCLFFT_B200_TMA")) req.use_tma = std::strcmp(k, "1") == 0;
     // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
     if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
+    if (const char* k = std::getenv("SYCLFFT_B200_FUSED4_SINGLE")) req.fused_single = std::strcmp(k, "1") == 0;
+    if (const char* k = std::getenv("SYCLFFT_B200_FUSED4")) {
+        if (std::strcmp(k, "0") == 0) req.fused_single = false;
+    }
     // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
     // =pipe: complex<double> 65536-point lines on the pipelined 16-CTA cluster kernel.
     if (const char* k = std::getenv("SYCLFFT_B200_CLUSTER")) {

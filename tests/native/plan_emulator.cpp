@@ -8,6 +8,7 @@
 // truncation. Used by tests/ to check plan decompositions (four-step, Bluestein,
 // strided axes) without a GPU. Never used by the product library.
 #include <complex>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -205,6 +206,9 @@ int run_request(int dbl, int dir, int norm, int in_place, unsigned rank, const u
         req.force_maxv = force_maxv;
         req.smem_limit = smem_limit;
         req.skip_axes = skip_axes;
+        // the provider's switch for fused four-step routing of lines that fit one block
+        const char* fs = std::getenv("SYCLFFT_B200_FUSED4_SINGLE");
+        req.fused_single = fs && std::strcmp(fs, "1") == 0;
         PlanSpec plan = make_plan(req);
         set_err(desc, desc_cap, describe_plan(plan));
         const int64_t E = static_cast<int64_t>(plan.elements);

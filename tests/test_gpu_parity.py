@@ -380,7 +380,8 @@ def test_pipelined_cluster_kernel(sf, torch, in_place, monkeypatch):
 
 
 @pytest.mark.parametrize("shape,batch,dbl", [([65536], 8, False), ([65536], 6, True), ([65537], 6, False),
-                                             ([65537], 5, True), ([4099], 6, True), ([24, 65536], 1, False)],
+                                             ([65537], 5, True), ([4099], 6, True), ([24, 65536], 1, False),
+                                             ([13440], 7, False)],
                          ids=lambda v: str(v))
 def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, batch, dbl):
     """The fused launches (four-step columns + rows, Bluestein forward columns + rows + inverse
@@ -393,6 +394,9 @@ def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, 
     x = uniform_complex(n * batch, 31 + n, dt)
     xi = torch.from_numpy(x).cuda()
     outs = {}
+    # 13440 fits one block: its fused four-step (112 x 120) is the opt-in alternative to the
+    # single pass (SYCLFFT_B200_FUSED4_SINGLE=1)
+    monkeypatch.setenv("SYCLFFT_B200_FUSED4_SINGLE", "1")
     for fused in ("1", "0"):
         monkeypatch.setenv("SYCLFFT_B200_FUSED4", fused)
         p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)

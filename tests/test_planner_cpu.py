@@ -110,3 +110,22 @@ def test_bluestein_on_catalog_kernels():
         out, _ = emulate(x, shape, 2, -1, norm=1, double=dbl)
         ref = np.fft.fft(x.reshape(2, n), axis=1).reshape(-1) / n
         assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+
+
+def test_fused_single_routes_13440_through_a_catalogued_split(monkeypatch):
+    """With SYCLFFT_B200_FUSED4_SINGLE=1 a length that fits one block but has a fused four-step
+    kernel (13440 = 112 x 120) is planned as that four-step, on the catalog's radix sequences
+    (16, 7) and (8, 15); the FP64 emulation of its passes is the DFT. Without it the single pass
+    stays."""
+    import numpy as np
+    import native_libs as nl
+    n, b = 13440, 3
+    x = np.random.default_rng(3).standard_normal(n * b) + 1j * np.random.default_rng(4).standard_normal(n * b)
+    out, desc = nl.emulate(x, [n], b, -1)
+    assert [p["kind"] for p in desc["passes"]] == ["single"]
+    monkeypatch.setenv("SYCLFFT_B200_FUSED4_SINGLE", "1")
+    out, desc = nl.emulate(x, [n], b, -1)
+    assert [(p["kind"], p["radices"]) for p in desc["passes"]] == [("fourstep_cols", [16, 7]),
+                                                                    ("fourstep_rows", [8, 15])]
+    ref = np.fft.fft(x.reshape(b, n), axis=1).reshape(-1)
+    assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-14

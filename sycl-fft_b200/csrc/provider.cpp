@@ -390,7 +390,9 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags, 
     if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
     if (const char* k = std::getenv("SYCLFFT_B200_FUSED4_SINGLE")) req.fused_single = std::strcmp(k, "1") == 0;
     if (const char* k = std::getenv("SYCLFFT_B200_FUSED4")) {
-        if (std::strcmp(k, "0") == 0) req.fused_single = false;
+        if (std::strcmp(k, "1") != 0) req.fused_single = false;
+    } else {
+        req.fused_single = false;  // the fused kernels are opt-in
     }
     // SYCLFFT_B200_CLUSTER=off: long lines take the two-pass four-step; =8 / =16: cluster size.
     // =pipe: complex<double> 65536-point lines on the pipelined 16-CTA cluster kernel.
@@ -520,10 +522,11 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         bp.tp = to_tc(bp.p, tab(ps.tables.tc_tw), plan->status);
         plan->passes.push_back(bp);
     }
-    // four-step column + row passes of a contiguous axis with a fused kernel: one launch, the
-    // intermediate in an L2-resident ring (SYCLFFT_B200_FUSED4=0 keeps the two launches)
+    // four-step column + row passes (and Bluestein's three passes) of a contiguous axis with a
+    // fused kernel: one launch, the intermediate in an L2-resident ring. Opt-in
+    // (SYCLFFT_B200_FUSED4=1): measured slower than the separate launches on B200.
     const char* f4 = std::getenv("SYCLFFT_B200_FUSED4");
-    const bool fused_ok = !(f4 && f4[0] == '0') && !req.no_fixed;
+    const bool fused_ok = f4 && f4[0] == '1' && !req.no_fixed;
     for (size_t i = 0; fused_ok && i + 1 < plan->passes.size(); ++i) {
         const PassSpec& a = plan->passes[i].spec_ref();
         const PassSpec& b = plan->passes[i + 1].spec_ref();

@@ -390,6 +390,11 @@ class Plan:
         is read or written by the kernels directly over the bus. Returns an ExecutionEvent."""
         if not getattr(self, "_handle", None):
             raise SyclfftError(error_code.invalid_state, "Cannot execute a moved-from plan")
+        # pointers are validated before the placement rules, as sycl.cpp:619-635 does
+        if a is None or (isinstance(a, int) and a == 0):
+            raise SyclfftError(error_code.invalid_pointer, "input must be non-null")
+        if isinstance(b, int) and b == 0:
+            raise SyclfftError(error_code.invalid_pointer, "output must be non-null")
         one_pointer = b is None
         pl = self._options.placement
         if pl == placement.in_place and not one_pointer:

@@ -41,14 +41,18 @@ WAITING = [([13440], 32, False, "piped"), ([256], 512, True, "tc"), ([65536], 16
 
 
 @pytest.mark.parametrize("shape,batch,split,kind", WAITING, ids=lambda v: str(v))
-def test_wait_that_gives_up_raises_execution_failed(sf, torch, shape, batch, split, kind):
+def test_wait_that_gives_up_raises_execution_failed(sf, torch, monkeypatch, shape, batch, split, kind):
+    monkeypatch.setenv("SYCLFFT_B200_FUSED4", "1")  # the fused kernels are opt-in
     n = int(np.prod(shape))
     x = uniform_complex(n * batch, 77 + n)
     xt = torch.from_numpy(x).cuda()
     out = torch.empty_like(xt)
     p = sf.plan_many_dft("float", shape, batch, sf.direction.forward, sf.plan_options(split_precision=split))
     desc = p.describe()
-    assert kind in [ps["kind"] for ps in desc["passes"]] or desc.get(kind), desc
+    runs = {"piped": any(ps["piped_id"] >= 0 for ps in desc["passes"]),
+            "tc": any(ps["tc_id"] >= 0 for ps in desc["passes"]),
+            "fused_fourstep": bool(desc.get("fused_fourstep"))}
+    assert runs[kind], desc
     lib = p._lib
     assert lib.syclfft_b200_plan_set_wait_limit(p._handle, 0) == 0
     ev = p.execute(xt, out)

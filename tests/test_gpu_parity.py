@@ -397,7 +397,7 @@ def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, 
     # 13440 fits one block: its fused four-step (112 x 120) is the opt-in alternative to the
     # single pass (SYCLFFT_B200_FUSED4_SINGLE=1)
     monkeypatch.setenv("SYCLFFT_B200_FUSED4_SINGLE", "1")
-    for fused in ("1", "0"):
+    for fused in ("1", "0"):  # opt-in fused launches, then the default separate passes
         monkeypatch.setenv("SYCLFFT_B200_FUSED4", fused)
         p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)
         desc = p.describe()

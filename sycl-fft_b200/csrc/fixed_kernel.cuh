@@ -75,7 +75,17 @@ enum : int {
     kFeatRealPre = 1024,  // C2R: the first stage forms Z[k] from the bins (X[k], X[N-k]) on load
     kFeatLoadCG = 2048,   // first-stage global loads bypass L1 (ld.global.cg): data another CTA of
                           // the same launch wrote (the fused four-step's L2-resident ring)
+    kFeatLoadCS = 4096,   // first-stage global loads and last-stage global stores marked
+    kFeatStoreCS = 8192,  // streaming (ld/st .cs, evicted first): data read or written once, so
+                          // it does not push an L2-resident ring out of the cache
 };
+
+template <int FEAT, class C>
+__device__ __forceinline__ C fixed_load(const C* p) {
+    if constexpr (FEAT & kFeatLoadCG) return __ldcg(p);
+    else if constexpr (FEAT & kFeatLoadCS) return __ldcs(p);
+    else return *p;
+}
 
 // X[k] = 1/2 [(Z[k] + conj Z[N-k]) - i W_2N^k (Z[k] - conj Z[N-k])] * scale; a = Z[k], c = Z[N-k]
 template <class C, class T>
@@ -154,7 +164,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                     const int g = k * X.g_k + X.sel;
                     C a = cmake<C>(T(0), T(0));
                     if (X.line_ok && g < X.in_len) {
-                        a = MODEC ? X.gin[(int64_t)k * X.in_ks] : X.gin[k];
+                        a = fixed_load<FEAT>(MODEC ? X.gin + (int64_t)k * X.in_ks : X.gin + k);
                         if (X.flip_in) a.y = -a.y;
                         a = cmul(a, __ldg(X.premul + g));
                         if (X.conj_in) a.y = -a.y;
@@ -183,9 +193,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const C* src = MODEC ? X.gin + (int64_t)(j + r * NR) * X.in_ks : X.gin + (j + r * NR);
-                        C a;
-                        if constexpr (FEAT & kFeatLoadCG) a = __ldcg(src);
-                        else a = *src;
+                        C a = fixed_load<FEAT>(src);
                         if (X.conj_in) a.y = -a.y;
                         v[i * R + r] = a;
                     }
@@ -262,8 +270,9 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                         if constexpr (FEAT & kFeatPostmul) {
                             if (X.flip_out) a.y = -a.y;
                         }
-                        if constexpr (MODEC) X.gout[(int64_t)k * X.out_ks] = a;
-                        else X.gout[k] = a;
+                        C* dst = MODEC ? X.gout + (int64_t)k * X.out_ks : X.gout + k;
+                        if constexpr (FEAT & kFeatStoreCS) __stcs(dst, a);
+                        else *dst = a;
                     }
                 }
             } else {

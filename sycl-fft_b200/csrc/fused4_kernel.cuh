@@ -116,7 +116,8 @@ __device__ __forceinline__ void fused_done(unsigned* ctrl, int ring, int phase, 
 
 template <class T, int N1, int TPL1, int W1, int... RC>
 __device__ __forceinline__ void fused4_cols(FixedCtx<T>& X, Radices<RC...>) {
-    fixed_stages<T, N1, TPL1, true, W1, kFeatTw4, 1, 0, true, RC...>(X);
+    // the input is read once: streaming loads keep the ring in L2
+    fixed_stages<T, N1, TPL1, true, W1, kFeatTw4 | kFeatLoadCS, 1, 0, true, RC...>(X);
 }
 
 template <class T, int N2, int TPL2, int W2, int... RR>
@@ -202,7 +203,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             const int k = idx / W2;
             const int ww = idx - k * W2;
             const C a = sm[ww * kpitch<T, N2>() + pidx<T>(k)];
-            dst[ww + int64_t(k) * N1] = cmake<C>(a.x * sc, a.y * sy);
+            __stcs(dst + ww + int64_t(k) * N1, cmake<C>(a.x * sc, a.y * sy));  // written once: streaming
         }
     }
 }
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             X.sm = sm + threadIdx.x % W1;
             X.gin = in + job.line * P.a.in_hi + X.sel;
             X.gout = buf + X.sel;
-            fusedblue_cols<T, N1, TPL1, W1, kFeatPremul | kFeatTw4>(X, RC{});
+            fusedblue_cols<T, N1, TPL1, W1, kFeatPremul | kFeatTw4 | kFeatLoadCS>(X, RC{});
         } else if (job.phase == 1) {
             const int w = threadIdx.x / TPL2;
             X.t = threadIdx.x - w * TPL2;
@@ -327,7 +328,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
             X.sm = sm + threadIdx.x % W1;
             X.gin = buf + X.sel;
             X.gout = out + job.line * P.c.out_hi + X.sel;
-            fusedblue_cols<T, N1, TPL1, W1, kFeatPostmul | kFeatLoadCG>(X, RC{});
+            fusedblue_cols<T, N1, TPL1, W1, kFeatPostmul | kFeatLoadCG | kFeatStoreCS>(X, RC{});
         }
         fused_done(ctrl, P.ring, job.phase, slot);
     }

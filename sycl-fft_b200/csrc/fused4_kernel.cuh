@@ -107,11 +107,17 @@ __device__ __forceinline__ bool fused_claim(const FusedSched& q, int ring, unsig
     return !__syncthreads_or(!ok);
 }
 
-// Counts a finished tile of `phase` for its ring slot once every thread's stores are visible.
+// Release-add at GPU scope: orders every access that happens before it (the block's, through
+// the barrier before it) ahead of the counter update that waiting blocks acquire.
+__device__ __forceinline__ void red_release_add(unsigned* word, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(word), "r"(v) : "memory");
+}
+
+// Counts a finished tile of `phase` for its ring slot once every thread's accesses are done:
+// the barrier orders them before thread 0's release (one fence per block, not per thread).
 __device__ __forceinline__ void fused_done(unsigned* ctrl, int ring, int phase, int slot) {
-    __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(ctrl + 2 + phase * ring + slot, 1u);
+    if (threadIdx.x == 0) red_release_add(ctrl + 2 + phase * ring + slot, 1u);
 }
 
 template <class T, int N1, int TPL1, int W1, int... RC>
@@ -190,10 +196,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
         X.in_ks = 1;
         X.out_ks = 1;
         fused4_rows<T, N2, TPL2, W2>(X, RR{});  // ends with a barrier: the ring slot is read
-        if (tid == 0) {
-            __threadfence();  // the block's ring reads are ordered before the count
-            atomicAdd(ctrl + 2 + P.ring + slot, 1u);
-        }
+        if (tid == 0) red_release_add(ctrl + 2 + P.ring + slot, 1u);  // the block's ring reads come first
         // transposed store: rows k1 = tile*W2 .. +W2-1 of the output line, element k1 + N1 * k2
         C* dst = out + line * L + int64_t(tile) * W2;
         const T sc = static_cast<T>(P.scale);
@@ -204,6 +207,114 @@ __global__ void __launch_bounds__(THREADS, MINB)
             const int ww = idx - k * W2;
             const C a = sm[ww * kpitch<T, N2>() + pidx<T>(k)];
             __stcs(dst + ww + int64_t(k) * N1, cmake<C>(a.x * sc, a.y * sy));  // written once: streaming
+        }
+    }
+}
+
+// Persistent form of the same four-step: grid = the resident blocks, each looping over tiles.
+// Thread 0 claims the block's next ticket as soon as the current tile starts, so the claim's
+// round trip to L2 overlaps the tile's work instead of preceding it (one-tile blocks pay a
+// claim, a dependency check and a counter update of latency per tile). A block then holds two
+// tickets at once; progress still holds: the smallest unfinished ticket is either some block's
+// current tile, whose dependencies are all finished, or some block's claimed-ahead ticket, whose
+// block's current tile is smaller and so finished.
+template <class T, int N1, int TPL1, int W1, int N2, int TPL2, int W2, int THREADS, int MINB, class RC, class RR>
+__global__ void __launch_bounds__(THREADS, MINB)
+    fft_fused4p_kernel(const __grid_constant__ Fused4Params P, const cplx<T>* in, cplx<T>* out, cplx<T>* ring,
+                       unsigned* ctrl) {
+    using C = cplx<T>;
+    constexpr int64_t L = int64_t(N1) * N2;
+    constexpr int TC = N2 / W1;
+    constexpr int TR = N1 / W2;
+    static_assert(N2 % W1 == 0 && N1 % W2 == 0, "tiles must cover a line exactly");
+    static_assert(W1 * TPL1 <= THREADS && W2 * TPL2 <= THREADS, "block too small");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* sm = reinterpret_cast<C*>(smem_raw);
+    __shared__ long long s_ticket;
+    const int tid = threadIdx.x;
+    FusedSched q;
+    q.lines = P.lines;
+    q.lag = P.lag;
+    q.phases = 2;
+    q.tiles[0] = TC;
+    q.tiles[1] = TR;
+    const int64_t total = fused_total(q);
+    long long next = 0;
+    if (tid == 0) s_ticket = atomicAdd(ctrl, 1u);
+    for (;;) {
+        __syncthreads();  // s_ticket is set; the previous tile is done with shared memory
+        const int64_t t = s_ticket;
+        if (t >= total) break;
+        if (tid == 0) next = atomicAdd(ctrl, 1u);  // claimed ahead: used after this tile
+        const FusedTile job = fused_decode(q, t);
+        const int64_t line = job.line;
+        const int tile = job.tile;
+        const int slot = static_cast<int>(line % P.ring);
+        const unsigned gen = static_cast<unsigned>(line / P.ring);
+        bool ok = true;
+        if (tid == 0) {
+            ok = job.phase == 0 ? (gen == 0 || wait_count(ctrl + 2 + P.ring + slot, unsigned(TR) * gen, P.wait_polls))
+                                : wait_count(ctrl + 2 + slot, unsigned(TC) * (gen + 1), P.wait_polls);
+            if (!ok) {
+                report_status(P.status, 4);
+                atomicExch(ctrl + 1, 1u);
+            }
+        }
+        if (__syncthreads_or(!ok)) break;
+        C* const buf = ring + slot * L;
+        FixedCtx<T> X;
+        X.scale = T(1);
+        X.conj_in = false;
+        X.conj_out = false;
+        if (job.phase == 0) {
+            const int w = tid % W1;
+            X.t = tid / W1;
+            X.active = X.t < TPL1;
+            const int c = tile * W1 + w;
+            X.line_ok = X.active;
+            X.sel = c;
+            X.twb = static_cast<const C*>(P.tw1);
+            X.tw4_hi = static_cast<const C*>(P.tw4_hi);
+            X.tw4_lo = static_cast<const C*>(P.tw4_lo);
+            X.tw4_shift = P.tw4_shift;
+            X.sm = sm + w;
+            X.gin = in + line * L + c;
+            X.gout = buf + c;
+            X.in_ks = N2;
+            X.out_ks = N2;
+            X.conj_in = P.conj_in != 0;
+            fused4_cols<T, N1, TPL1, W1>(X, RC{});
+            fused_done(ctrl, P.ring, 0, slot);
+        } else {
+            const int w = tid / TPL2;
+            X.t = tid - w * TPL2;
+            X.active = w < W2;
+            const int row = tile * W2 + w;
+            X.line_ok = X.active;
+            X.sel = 0;
+            X.twb = static_cast<const C*>(P.tw2);
+            X.sm = sm + w * kpitch<T, N2>();
+            X.gin = buf + static_cast<int64_t>(row) * N2;
+            X.gout = nullptr;
+            X.in_ks = 1;
+            X.out_ks = 1;
+            fused4_rows<T, N2, TPL2, W2>(X, RR{});
+            if (tid == 0) red_release_add(ctrl + 2 + P.ring + slot, 1u);
+            C* dst = out + line * L + int64_t(tile) * W2;
+            const T sc = static_cast<T>(P.scale);
+            const T sy = P.conj_out ? -sc : sc;
+#pragma unroll 4
+            for (int idx = tid; idx < W2 * N2; idx += THREADS) {
+                const int k = idx / W2;
+                const int ww = idx - k * W2;
+                const C a = sm[ww * kpitch<T, N2>() + pidx<T>(k)];
+                __stcs(dst + ww + int64_t(k) * N1, cmake<C>(a.x * sc, a.y * sy));
+            }
+        }
+        if (tid == 0) {
+            unsigned abort;
+            asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(abort) : "l"(ctrl + 1) : "memory");
+            s_ticket = abort ? total : next;
         }
     }
 }

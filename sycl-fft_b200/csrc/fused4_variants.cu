@@ -1,6 +1,8 @@
 // Instantiations of the fused four-step kernels listed in fused4_catalog.h and their launcher.
 #include <atomic>
 #include <climits>
+#include <cstdlib>
+#include <cstring>
 #include <type_traits>
 
 #include "fused4_catalog.h"
@@ -13,7 +15,8 @@ constexpr int kMaxDevices = 64;
 
 #define SFB_RADICES(...) Radices<__VA_ARGS__>
 
-template <class T, int N1, int TPL1, int W1, int N2, int TPL2, int W2, int THREADS, int MINB, class RC, class RR>
+template <class T, int N1, int TPL1, int W1, int N2, int TPL2, int W2, int THREADS, int MINB, int PERSIST, class RC,
+          class RR>
 struct Fused4Launcher {
     static constexpr int64_t smem() {
         constexpr int64_t a = int64_t(N1) * W1;
@@ -40,13 +43,44 @@ struct Fused4Launcher {
         *per_sm = k;
         return cudaSuccess;
     }
+    // persistent claim-ahead kernel or one tile per block: the catalog's choice, unless
+    // SYCLFFT_B200_FUSED4_MODE=tile|persistent says otherwise
+    static bool persistent() {
+        static const bool v = [] {
+            const char* m = std::getenv("SYCLFFT_B200_FUSED4_MODE");
+            if (m && std::strcmp(m, "tile") == 0) return false;
+            if (m && std::strcmp(m, "persistent") == 0) return true;
+            return PERSIST != 0;
+        }();
+        return v;
+    }
+    static cudaError_t resident_p(int* per_sm) {
+        static std::atomic<int> known[kMaxDevices];
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+        int k = known[dev].load();
+        if (k <= 0) {
+            auto kernel = fft_fused4p_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>;
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem()));
+            if (e != cudaSuccess) return e;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&k, kernel, THREADS, static_cast<size_t>(smem()));
+            if (e != cudaSuccess) return e;
+            if (k <= 0) return cudaErrorInvalidConfiguration;
+            known[dev].store(k);
+        }
+        *per_sm = k;
+        return cudaSuccess;
+    }
     static cudaError_t run(Fused4Params& p, const void* in, void* out, void* scratch, cudaStream_t stream) {
         using C = cplx<T>;
         constexpr int64_t L = int64_t(N1) * N2;
         constexpr int TILES = N2 / W1 + N1 / W2;  // tickets per line
         if (p.lines < 3) return cudaErrorInvalidValue;
+        const bool pers = persistent();
         int per_sm = 0;
-        cudaError_t e = resident(&per_sm);
+        cudaError_t e = pers ? resident_p(&per_sm) : resident(&per_sm);
         if (e != cudaSuccess) return e;
         int dev = 0, sms = 0;
         e = cudaGetDevice(&dev);
@@ -54,7 +88,9 @@ struct Fused4Launcher {
         if (e != cudaSuccess) return e;
         const int64_t grid = int64_t(sms) * per_sm;
         int lag = 0, ring = 0;
-        if (!fused_geometry(grid, TILES, p.lines, 2, kFused4MaxRing, &lag, &ring)) return cudaErrorInvalidValue;
+        // persistent blocks hold a claimed-ahead ticket too: twice the tiles in flight
+        if (!fused_geometry(pers ? 2 * grid : grid, TILES, p.lines, 2, kFused4MaxRing, &lag, &ring))
+            return cudaErrorInvalidValue;
         p.lag = lag;
         p.ring = ring;
         const int64_t tickets = p.lines * TILES;
@@ -62,6 +98,13 @@ struct Fused4Launcher {
         auto* ctrl = reinterpret_cast<unsigned*>(static_cast<C*>(scratch) + int64_t(ring) * L);
         e = cudaMemsetAsync(ctrl, 0, kFused4CtrlWords * sizeof(unsigned), stream);
         if (e != cudaSuccess) return e;
+        if (pers) {
+            const int64_t blocks = grid < tickets ? grid : tickets;
+            fft_fused4p_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>
+                <<<static_cast<unsigned>(blocks), THREADS, static_cast<size_t>(smem()), stream>>>(
+                    p, static_cast<const C*>(in), static_cast<C*>(out), static_cast<C*>(scratch), ctrl);
+            return cudaGetLastError();
+        }
         // one block per tile; the resident blocks (grid) only set the lag
         fft_fused4_kernel<T, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, RC, RR>
             <<<static_cast<unsigned>(tickets), THREADS, static_cast<size_t>(smem()), stream>>>(
@@ -70,14 +113,14 @@ struct Fused4Launcher {
     }
 };
 
-#define SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR)              \
-    Fused4Launcher<std::conditional_t<(DBL) != 0, double, float>, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, \
+#define SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR)              \
+    Fused4Launcher<std::conditional_t<(DBL) != 0, double, float>, N1, TPL1, W1, N2, TPL2, W2, THREADS, MINB, PERSIST, \
                    SFB_RADICES RC, SFB_RADICES RR>
 
 const Fused4Entry kEntries[] = {
-#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR) \
-    {ID, DBL, N1, W1, COL, N2, W2, ROW, THREADS,                                    \
-     SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR)::smem()},
+#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR) \
+    {ID, DBL, N1, W1, COL, N2, W2, ROW, THREADS,                                             \
+     SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR)::smem()},
     SFB_FUSED4_CATALOG(SFB_X)
 #undef SFB_X
 };
@@ -180,10 +223,10 @@ const Fused4Entry* find_fused4(bool dbl, int col_id, int row_id) {
 cudaError_t launch_fused4(const Fused4Entry& entry, Fused4Params& p, const void* in, void* out, void* scratch,
                           cudaStream_t stream) {
     switch (entry.id) {
-#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR) \
-    case ID:                                                                        \
-        return SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR)::run(p, in, out, \
-                                                                                                   scratch, stream);
+#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR)                  \
+    case ID:                                                                                                 \
+        return SFB_FUSED4_TYPE(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR)::run( \
+            p, in, out, scratch, stream);
         SFB_FUSED4_CATALOG(SFB_X)
 #undef SFB_X
         default:

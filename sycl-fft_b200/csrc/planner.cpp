@@ -1262,7 +1262,7 @@ const TcEntry* find_tc(int n, bool cols) {
 bool has_fused4(bool dbl, int col_id, int row_id) {
     struct Pair { int dbl, col, row; };
     static const Pair pairs[] = {
-#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, RC, RR) {DBL, COL, ROW},
+#define SFB_X(ID, DBL, N1, TPL1, W1, COL, N2, TPL2, W2, ROW, THREADS, MINB, PERSIST, RC, RR) {DBL, COL, ROW},
         SFB_FUSED4_CATALOG(SFB_X)
 #undef SFB_X
     };

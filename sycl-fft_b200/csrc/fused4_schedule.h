@@ -108,9 +108,12 @@ inline bool fused_geometry(int64_t blocks, int tiles_per_line, int64_t lines, in
     int64_t r = span * d + d + 2;
     const int64_t cap = lines - 1 < max_ring ? lines - 1 : max_ring;
     if (r > cap) {
-        // shrink the lag until the ring fits: ring = span * d + 1 at the least
+        // a smaller ring: split it evenly between the phases' lags and the gap before a slot is
+        // reused (phase 0 of line l waits for the last phase of line l - ring, claimed
+        // ring - span * d segments earlier), so neither wait is claimed right behind its target
         r = cap;
-        d = (r - 1) / span;
+        d = r / phases;
+        if (span * d >= r) d = (r - 1) / span;
     }
     if (d < 1) return false;
     *lag = static_cast<int>(d);

@@ -26,6 +26,9 @@ int f4_check(int64_t lines, int64_t blocks, int phases, const int* tiles, int ma
     *lag_out = lag;
     *ring_out = ring;
     if (!(lag >= 1 && int64_t(phases - 1) * lag < ring && ring <= lines - 1 && ring <= max_ring)) return 2;
+    // a slot's reuse is claimed at least as many segments after its last use as a phase lag
+    // minus one (an even split when the ring is capped)
+    if (lines > 2 * phases && ring - int64_t(phases - 1) * lag < lag - 1) return 11;
     if (int64_t(ring) * line_bytes + ctrl_bytes > lines * line_bytes) return 3;  // ring + control in scratch
     sfb::FusedSched q;
     q.lines = lines;

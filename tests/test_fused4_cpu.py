@@ -47,6 +47,15 @@ def test_schedule(lib, tiles, line_bytes, lines, blocks):
         assert 1 <= lag and (len(tiles) - 1) * lag < ring <= min(lines - 1, 64)
 
 
+def test_capped_ring_keeps_reuse_gap(lib):
+    """c64 65536 x 1024 on 1184 blocks in flight: the wanted ring (80 slots) exceeds the cap of
+    64, so lag and reuse gap share it instead of the lag taking all of it (a slot's next user
+    then waits right behind its last one)."""
+    rc, lag, ring, waits = check(lib, 1024, 1184, (16, 16), 65536 * 8)
+    assert rc == 0 and ring == 64 and lag == 32
+    assert waits < 0.25 * 1024 * 32  # not one wait per tile: the lag and the reuse gap share the ring
+
+
 def test_full_config_lag_leaves_few_waits(lib):
     """c128 65536 x 512 on 148 SMs x 4 blocks: the lag covers the tiles in flight."""
     rc, lag, ring, waits = check(lib, 512, 592, (32, 32), 65536 * 16)

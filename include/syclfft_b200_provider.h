@@ -225,6 +225,31 @@ SYCLFFT_B200_EXPORT int syclfft_b200_group_execute(void *group, const syclfft_b2
                                                    uint32_t count, void *stream, char *err, size_t cap);
 SYCLFFT_B200_EXPORT void syclfft_b200_group_destroy(void *group);
 
+/* ---- Radix-family execution (no reference counterpart): one launch for requests of
+ *      different lengths. ----
+ *
+ * A family is the power-of-two lengths whose single-pass kernels share one block shape:
+ * complex<float> 64 .. 4096 and complex<double> 64 .. 2048 (syclfft_b200_family_supports).
+ * One execute runs up to 256 requests per launch (more are split), each with its own length
+ * of the family, buffers, batch, direction and normalization; requests are tiles of one kernel
+ * launch that dispatches on each request's length. The request table is passed as kernel
+ * parameters, so executes are stream-ordered, need no device staging and can be captured in a
+ * CUDA graph. in == out is allowed per request; buffers aligned to the complex element. */
+typedef struct syclfft_b200_family_item_v1 {
+    const void *in;
+    void *out;
+    uint64_t n;              /* length: a power of two of the family */
+    uint64_t batch;          /* lines of length n */
+    int32_t direction;       /* -1 / +1 */
+    uint32_t normalization;  /* SYCLFFT_B200_NORM_* */
+} syclfft_b200_family_item_v1;
+
+SYCLFFT_B200_EXPORT int syclfft_b200_family_supports(uint32_t scalar, uint64_t n);
+SYCLFFT_B200_EXPORT void *syclfft_b200_family_create(uint32_t scalar, int32_t device, char *err, size_t cap);
+SYCLFFT_B200_EXPORT int syclfft_b200_family_execute(void *family, const syclfft_b200_family_item_v1 *items,
+                                                    uint32_t count, void *stream, char *err, size_t cap);
+SYCLFFT_B200_EXPORT void syclfft_b200_family_destroy(void *family);
+
 /* ---- Transform without device allocation (no counterpart in the reference). ----
  *
  * For callers that cannot allocate device memory at the point they need a transform:

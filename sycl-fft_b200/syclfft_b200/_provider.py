@@ -68,6 +68,17 @@ class GroupItemV1(ctypes.Structure):
     ]
 
 
+class FamilyItemV1(ctypes.Structure):
+    _fields_ = [
+        ("in_", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("n", ctypes.c_uint64),
+        ("batch", ctypes.c_uint64),
+        ("direction", ctypes.c_int32),
+        ("normalization", ctypes.c_uint32),
+    ]
+
+
 class HostStageV1(ctypes.Structure):
     _fields_ = [
         ("plan", ctypes.c_void_p),
@@ -106,6 +117,10 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_group_execute",
     "syclfft_b200_group_destroy",
     "syclfft_b200_execute_noalloc_c2c_f32",
+    "syclfft_b200_family_supports",
+    "syclfft_b200_family_create",
+    "syclfft_b200_family_execute",
+    "syclfft_b200_family_destroy",
     "syclfft_b200_create_real",
     "syclfft_b200_create_strided",
 )
@@ -158,6 +173,15 @@ def load(path: str | None = None):
     lib.syclfft_b200_group_execute.restype = ctypes.c_int
     lib.syclfft_b200_group_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(GroupItemV1), ctypes.c_uint32,
                                                ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_family_supports.restype = ctypes.c_int
+    lib.syclfft_b200_family_supports.argtypes = [ctypes.c_uint32, ctypes.c_uint64]
+    lib.syclfft_b200_family_create.restype = ctypes.c_void_p
+    lib.syclfft_b200_family_create.argtypes = [ctypes.c_uint32, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_family_execute.restype = ctypes.c_int
+    lib.syclfft_b200_family_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(FamilyItemV1), ctypes.c_uint32,
+                                                ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_family_destroy.restype = None
+    lib.syclfft_b200_family_destroy.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_group_destroy.restype = None
     lib.syclfft_b200_group_destroy.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_create_real.restype = ctypes.c_void_p

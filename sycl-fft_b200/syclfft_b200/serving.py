@@ -4,9 +4,11 @@ Requests of mixed lengths, batch counts, precisions, directions and normalizatio
 over time. The server keeps plans and their tables resident on the device, admits waiting
 requests while their buffers (and any new plan's scratch) fit an HBM budget, and launches
 everything admitted so far without waiting for earlier work: requests whose length has a
-size-specialised single-pass kernel are packed into one grouped launch per length family
-(syclfft_b200_group_execute), the others run on resident plans made for up to a
-any batch up to 512 (syclfft_b200_execute_ex), created ahead of admission by a worker
+size-specialised single-pass kernel are packed into one launch: power-of-two lengths up to
+4096 (float) / 2048 (double) of every admitted request into one radix-family launch
+(syclfft_b200_family_execute), other such lengths one grouped launch per length
+(syclfft_b200_group_execute); the others run on resident plans made for any batch up to
+512 (syclfft_b200_execute_ex), created ahead of admission by a worker
 thread while the request waits. Families are spread over several CUDA
 streams so independent work overlaps on the device. Latency is measured from a request's
 arrival to the CUDA event that completes it. For comparison, the plain mode executes one
@@ -178,6 +180,7 @@ class Server:
         self.plans = OrderedDict()
         self.retired = []   # (handle, event): released when the event has completed
         self.groups = {}    # (n, double) -> handle
+        self.families = {}  # double -> radix-family handle (power-of-two lengths of one launch)
         self.err = ctypes.create_string_buffer(ERR)
         self.plan_bytes = 0
         self.plans_created = 0
@@ -204,7 +207,7 @@ class Server:
 
     def _prefetch(self, r: Request):
         key = (r.lengths, r.double)
-        if key in self.plans or key in self.pending or self.pool is None or self.groupable(r):
+        if key in self.plans or key in self.pending or self.pool is None or self.groupable(r) or self.family_member(r):
             return
         self.pending[key] = self.pool.submit(self._create, r.lengths, r.double)
 
@@ -251,6 +254,20 @@ class Server:
             self.groups[key] = g
         return g
 
+    def _family(self, double):
+        f = self.families.get(double)
+        if f is None:
+            f = self.lib.syclfft_b200_family_create(2 if double else 1, self.dev, self.err, ERR)
+            if not f:
+                raise RuntimeError(self.err.value.decode())
+            self.families[double] = f
+        return f
+
+    def family_member(self, r: Request):
+        """Lengths served by the radix-family launch: several lengths in one kernel."""
+        return len(r.lengths) == 1 and bool(self.lib.syclfft_b200_family_supports(2 if r.double else 1,
+                                                                                  r.lengths[0]))
+
     def groupable(self, r: Request):
         return len(r.lengths) == 1 and bool(self.lib.syclfft_b200_group_supports(2 if r.double else 1, r.lengths[0]))
 
@@ -264,8 +281,11 @@ class Server:
             self.api.destroy(handle)
         for g in self.groups.values():
             self.lib.syclfft_b200_group_destroy(g)
+        for f in self.families.values():
+            self.lib.syclfft_b200_family_destroy(f)
         self.plans.clear()
         self.groups.clear()
+        self.families.clear()
         self.arena = None
         # hand the request buffers cached by torch back to the device for other pools
         self.torch.cuda.empty_cache()
@@ -304,6 +324,20 @@ class Server:
         if rc:
             raise RuntimeError(self.err.value.decode())
         return h
+
+    def _execute_family(self, double, reqs, stream):
+        f = self._family(double)
+        items = (_provider.FamilyItemV1 * len(reqs))()
+        for i, r in enumerate(reqs):
+            items[i].in_ = r.inp.data_ptr()
+            items[i].out = r.out.data_ptr()
+            items[i].n = r.lengths[0]
+            items[i].batch = r.batch
+            items[i].direction = r.direction
+            items[i].normalization = r.normalization
+        rc = self.lib.syclfft_b200_family_execute(f, items, len(reqs), stream.cuda_stream, self.err, ERR)
+        if rc:
+            raise RuntimeError(self.err.value.decode())
 
     def _execute_group(self, key, reqs, stream):
         n, double = key
@@ -410,7 +444,7 @@ class Server:
             "requests_per_s": len(reqs) / makespan,
             "p50_ms": 1e3 * lat_sorted[len(lat) // 2], "p99_ms": 1e3 * lat_sorted[min(len(lat) - 1, int(0.99 * len(lat)))],
             "mean_ms": 1e3 * statistics.mean(lat), "plans_resident": len(self.plans),
-            "plans_created": self.plans_created, "groups": len(self.groups),
+            "plans_created": self.plans_created, "groups": len(self.groups), "families": len(self.families),
             "plan_bytes": self.plan_bytes, "plan_evictions": self.evictions, "max_waiting": self.max_waiting,
         }
 
@@ -444,7 +478,12 @@ class Server:
                 if not self._reserve(r):
                     break
                 waiting.popleft()
-                key = ("g", r.lengths[0], r.double) if self.groupable(r) else ("p", r.lengths, r.double)
+                if self.family_member(r):
+                    key = ("f", r.double)
+                elif self.groupable(r):
+                    key = ("g", r.lengths[0], r.double)
+                else:
+                    key = ("p", r.lengths, r.double)
                 bins.setdefault(key, []).append(r)
             # launch everything admitted: one grouped launch per length family
             for key, rs in bins.items():
@@ -454,7 +493,9 @@ class Server:
                 with torch.cuda.stream(s):
                     for r in rs:
                         self._fill(r)
-                    if key[0] == "g":
+                    if key[0] == "f":
+                        self._execute_family(key[1], rs, s)
+                    elif key[0] == "g":
                         self._execute_group((key[1], key[2]), rs, s)
                     else:
                         for r in rs:

@@ -58,6 +58,59 @@ def test_grouped_launch_matches_fp64(torch):
     assert lib.syclfft_b200_group_supports(1, 1009) == 0
 
 
+def test_family_launch_matches_fp64(torch):
+    """Requests of every length of a radix family (powers of two up to 4096 float / 2048
+    double), with their own batches, directions and normalizations, some in place, in one
+    launch; again from a captured CUDA graph with new inputs."""
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    rng = np.random.default_rng(8)
+    for dbl, top in ((False, 4096), (True, 2048)):
+        sc = 2 if dbl else 1
+        assert lib.syclfft_b200_family_supports(sc, 64) and lib.syclfft_b200_family_supports(sc, top)
+        assert not lib.syclfft_b200_family_supports(sc, 2 * top) and not lib.syclfft_b200_family_supports(sc, 96)
+        fam = lib.syclfft_b200_family_create(sc, -1, err, 1024)
+        assert fam, err.value
+        dt = np.complex128 if dbl else np.complex64
+        reqs = []
+        n = 64
+        while n <= top:
+            for _ in range(2):
+                b = int(rng.integers(1, 70))
+                d = int(rng.choice([-1, 1]))
+                nm = int(rng.integers(0, 4))
+                xi = torch.from_numpy(uniform_complex(n * b, n + b, dt)).cuda()
+                xo = xi if len(reqs) % 3 == 0 else torch.empty_like(xi)
+                reqs.append((n, xi, xo, b, d, nm))
+            n *= 2
+        items = (_provider.FamilyItemV1 * len(reqs))()
+        for k, (n, xi, xo, b, d, nm) in enumerate(reqs):
+            items[k].in_, items[k].out, items[k].n, items[k].batch = xi.data_ptr(), xo.data_ptr(), n, b
+            items[k].direction, items[k].normalization = d, nm
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        inputs = [xi.clone() for _, xi, _, _, _, _ in reqs]
+        assert lib.syclfft_b200_family_execute(fam, items, len(reqs), s.cuda_stream, err, 1024) == 0, err.value
+        torch.cuda.synchronize()
+        for (n, xi, xo, b, d, nm), x in zip(reqs, inputs):
+            ref = fp64_fft(x.cpu().numpy(), [n], b, d, norm_scale(nm, d, n))
+            assert rel_l2(xo.cpu().numpy(), ref) <= spec_tol(n, dbl), (n, b, d, nm)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=s):
+            assert lib.syclfft_b200_family_execute(fam, items, len(reqs), s.cuda_stream, err, 1024) == 0
+        fresh = [x.clone().normal_() for x in inputs]
+        for (n, xi, xo, b, d, nm), x in zip(reqs, fresh):
+            xi.copy_(x)
+        graph.replay()
+        torch.cuda.synchronize()
+        for (n, xi, xo, b, d, nm), x in zip(reqs, fresh):
+            ref = fp64_fft(x.cpu().numpy(), [n], b, d, norm_scale(nm, d, n))
+            assert rel_l2(xo.cpu().numpy(), ref) <= spec_tol(n, dbl), (n, b, d, nm)
+        del graph
+        lib.syclfft_b200_family_destroy(fam)
+
+
 @pytest.mark.parametrize("shape,dbl", [([4096], False), ([65536], True), ([65537], False), ([1009], True),
                                        ([13440], False), ([24, 40], False), ([30000], True)], ids=str)
 def test_execute_smaller_batch(torch, shape, dbl):
@@ -119,7 +172,7 @@ def test_serving_alone_vs_mix(torch):
             assert rel_l2(results[r.rid].numpy(), ref) <= spec_tol(n, r.double)
         for st in (mixed, alone):
             assert st["requests"] == len(reqs) and st["p99_ms"] >= st["p50_ms"] > 0
-        assert mixed["groups"] >= 1
+        assert mixed["groups"] + mixed["families"] >= 1
     finally:
         srv.close()
 

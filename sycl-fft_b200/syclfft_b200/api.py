@@ -324,6 +324,7 @@ class Plan:
         self._last_event = None
         self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
+        self._execute = self._api.execute
 
     # -- properties (syclfft.hpp:62-66) --
     def shape(self):
@@ -368,14 +369,16 @@ class Plan:
             if t == 0:
                 raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
             return t
-        if isinstance(t, torch.Tensor) and not t.is_cuda and t.is_pinned():
-            pass  # page-locked host memory is device-accessible (read over the bus)
-        elif not isinstance(t, torch.Tensor) or not t.is_cuda:
+        if not isinstance(t, torch.Tensor):
             raise SyclfftError(error_code.invalid_pointer, f"{name} is not a device allocation in the plan context")
-        elif t.device.index != self._device:
-            raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
-        if t.dtype != self.dtype:
-            raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {self.dtype}")
+        if t.is_cuda:
+            if t.get_device() != self._device:
+                raise SyclfftError(error_code.invalid_pointer, f"{name} lives on another device than the plan")
+        elif not t.is_pinned():  # page-locked host memory is device-accessible (read over the bus)
+            raise SyclfftError(error_code.invalid_pointer, f"{name} is not a device allocation in the plan context")
+        dtype = torch.complex128 if self._double else torch.complex64
+        if t.dtype != dtype:
+            raise SyclfftError(error_code.invalid_argument, f"{name} has dtype {t.dtype}, plan needs {dtype}")
         need = self._extent[name]
         if not t.is_contiguous() or t.numel() < need:
             raise SyclfftError(error_code.invalid_argument, f"{name} must be contiguous with >= {need} elements")
@@ -415,31 +418,32 @@ class Plan:
         if pl == placement.out_of_place and inp == out:
             raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires distinct allocations")
         torch = _torch()
-        s = stream or torch.cuda.current_stream(self._device)
+        current = torch.cuda.current_stream(self._device)
+        s = stream or current
         with self._lock:
-            if s == torch.cuda.current_stream(self._device):
+            if s is current or s == current:
                 capturing = torch.cuda.is_current_stream_capturing()
             else:
                 with torch.cuda.stream(s):
                     capturing = torch.cuda.is_current_stream_capturing()
             for dep in dependencies or ():
                 s.wait_event(dep)
-            if self._last_event is not None and not capturing and self._last_stream != s.cuda_stream:
+            handle = s.cuda_stream
+            if self._last_event is not None and not capturing and self._last_stream != handle:
                 # A graph cannot depend on work outside its capture; captured launches run
                 # only at replay, which the caller orders against earlier executes. On the
                 # stream of the previous execute, stream order already serialises them.
                 s.wait_event(self._last_event)
             err = self._err
-            err[0] = b"\0"
-            rc = self._api.execute(self._handle, inp, out, s.cuda_stream, err, _provider.ERR_CAP)
-            if rc != 0 or err.value:
+            # the provider writes the error buffer only on failure (a non-zero return)
+            if self._execute(self._handle, inp, out, handle, err, _provider.ERR_CAP) != 0:
                 raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
-            ev = _event_class()(self._lib, (self._handle,))
+            ev = (_EVENT_CLS or _event_class())(self._lib, (self._handle,))
             ev.record(s)
             # an event recorded inside a capture belongs to the graph: ordering of replays
             # against later executes is the caller's, as for any captured work
             self._last_event = None if capturing else ev
-            self._last_stream = None if capturing else s.cuda_stream
+            self._last_stream = None if capturing else handle
             return ev
 
     def close(self):
@@ -525,6 +529,7 @@ class RealPlan(Plan):
         self._last_event = None
         self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
+        self._execute = self._api.execute
 
     @property
     def kind(self):

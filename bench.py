@@ -855,9 +855,9 @@ def run_serve(args):
            "config": {"workload": "serving_stream", "requests": len(reqs), "arrival_rate_per_s": args.rate,
                       "lengths": "1/3 pow2 2^6..2^20, 1/3 7-smooth, 1/3 primes 257..65537",
                       "batch": "log-uniform 1..512", "precision": "80% c64 / 20% c128",
-                      "hbm_budget_gb": args.budget_gb}}
+                      "hbm_budget_gb": args.budget_gb, "plan_workers": args.plan_workers}}
     for mode in ("served", "plain", "plan_per_request"):
-        srv = serving.Server(budget_bytes=args.budget_gb * 1e9, streams=4)
+        srv = serving.Server(budget_bytes=args.budget_gb * 1e9, streams=4, plan_workers=args.plan_workers)
         try:
             st = srv.run([serving.Request(**{k: getattr(r, k) for k in ("rid", "lengths", "batch", "double",
                                                                          "direction", "normalization", "seed",
@@ -901,6 +901,7 @@ def main():
     ap.add_argument("--requests", type=int, default=20000)
     ap.add_argument("--rate", type=float, default=50000.0)
     ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--plan-workers", type=int, default=2, help="--serve: threads creating plans ahead of admission")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

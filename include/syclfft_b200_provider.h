@@ -90,6 +90,9 @@ SYCLFFT_B200_EXPORT const syclfft_b200_provider_v1 *syclfft_b200_get_provider_v1
 /* JSON description of the plan's passes (kernel kind, FFT length, radices, tile
  * shape, bytes moved). Returns the string length, or -1 if it did not fit. */
 SYCLFFT_B200_EXPORT int syclfft_b200_describe_plan(const void *plan, char *buf, size_t cap);
+/* Device memory the plan holds: its tables (twiddles, chirps, chirp spectra) and any scratch
+ * it owns (plans made with SYCLFFT_B200_CREATE_STREAM_SCRATCH own none). 0 for a null plan. */
+SYCLFFT_B200_EXPORT uint64_t syclfft_b200_plan_device_bytes(const void *plan);
 /* Number of kernel launches one execute performs. */
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_launches(const void *plan);
 /* Library version string. */

@@ -230,6 +230,7 @@ struct DevicePlan {
     PlanSpec spec;
     int device = 0;
     void* table_mem = nullptr;
+    size_t table_bytes = 0;  // size of table_mem
     void* scratch = nullptr;
     // Status word (StatusPool): non-zero after a bounded wait in one of the plan's kernels gave
     // up. Plans built over other plans (real, strided) point at a child's word.
@@ -446,6 +447,7 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
     }
     cudaStream_t ms = memory_stream(device);
     check(cudaMallocAsync(&plan->table_mem, blob.size(), ms), "cudaMallocAsync(tables)");
+    plan->table_bytes = blob.size();
     check(cudaMemcpyAsync(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(tables)");
     plan->status = status_pool().acquire();
     plan->owns_status = true;
@@ -1671,6 +1673,18 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_host(const syclfft_b200_host_stage_
         sfb::set_error(err, cap, e.what());
         return 1;
     }
+}
+
+SYCLFFT_B200_EXPORT uint64_t syclfft_b200_plan_device_bytes(const void* plan) {
+    auto* p = const_cast<sfb::DevicePlan*>(static_cast<const sfb::DevicePlan*>(plan));
+    if (!p) return 0;
+    uint64_t bytes = 0;
+    sfb::for_each_plan(p, [&](sfb::DevicePlan* q) {
+        const size_t cs = q->spec.req.dbl ? 16 : 8;
+        bytes += q->table_bytes;
+        if (q->scratch) bytes += q->spec.scratch_elements * cs;
+    });
+    return bytes;
 }
 
 SYCLFFT_B200_EXPORT int syclfft_b200_plan_status(const void* plan) {

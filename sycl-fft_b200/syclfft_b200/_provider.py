@@ -106,6 +106,7 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_plan_launches",
     "syclfft_b200_version",
     "syclfft_b200_plan_status",
+    "syclfft_b200_plan_device_bytes",
     "syclfft_b200_plan_take_status",
     "syclfft_b200_plan_set_wait_limit",
     "syclfft_b200_execute_host",
@@ -155,6 +156,8 @@ def load(path: str | None = None):
     lib.syclfft_b200_execute_ex.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_char_p,
                                             ctypes.c_size_t]
+    lib.syclfft_b200_plan_device_bytes.restype = ctypes.c_uint64
+    lib.syclfft_b200_plan_device_bytes.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_plan_status.restype = ctypes.c_int
     lib.syclfft_b200_plan_status.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_plan_take_status.restype = ctypes.c_int

@@ -165,7 +165,7 @@ class Server:
     """`budget_bytes` bounds the request buffers in flight; `plan_budget_bytes` bounds the
     resident plans (least recently used plans are released once their last launch is done)."""
 
-    def __init__(self, device=None, budget_bytes=120e9, streams=4, plan_budget_bytes=16e9):
+    def __init__(self, device=None, budget_bytes=120e9, streams=4, plan_budget_bytes=16e9, plan_workers=2):
         import torch
         from collections import OrderedDict
         self.torch = torch
@@ -173,6 +173,7 @@ class Server:
         self.lib = _provider.load()
         self.api = _provider.provider(self.lib)
         self.budget = float(budget_bytes)
+        self.plan_workers = int(plan_workers)  # threads creating plans ahead of admission
         self.plan_budget = float(plan_budget_bytes)
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(streams)]
         # (lengths, double, batch class) -> [handle, bytes, last launch event]; both directions
@@ -219,8 +220,7 @@ class Server:
             return h
         fut = self.pending.pop(key, None)
         handle = fut.result() if fut is not None else self._create(r.lengths, r.double)
-        n = math.prod(r.lengths)
-        nbytes = 16 * n * (16 if r.double else 8)  # bound on the tables
+        nbytes = int(self.lib.syclfft_b200_plan_device_bytes(handle))  # the plan's tables
         h = [handle, nbytes, None]
         self.plans[key] = h
         self.plan_bytes += nbytes
@@ -450,7 +450,7 @@ class Server:
 
     def _serve(self, reqs, t0, start, keep_results):
         from concurrent.futures import ThreadPoolExecutor
-        self.pool = ThreadPoolExecutor(max_workers=2)
+        self.pool = ThreadPoolExecutor(max_workers=self.plan_workers)
         try:
             self._serve_loop(reqs, t0, start, keep_results)
         finally:

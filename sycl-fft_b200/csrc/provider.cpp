@@ -329,9 +329,72 @@ void* stream_arena(int device, cudaStream_t stream, size_t bytes, bool capturing
     return a.ptr;
 }
 
+// Page-locked staging buffers for plan-table uploads, per device. A copy from pageable memory
+// first waits for everything queued on the memory stream (other plans' chirp and spectrum
+// work), which serialised concurrent plan creations behind each other's device work; a copy
+// from page-locked memory is asynchronous. A buffer is reused once the event recorded after
+// its copy has completed; buffers are never freed (cudaFreeHost would synchronize the device).
+class UploadStaging {
+public:
+    struct Buffer {
+        unsigned char* data = nullptr;
+        size_t cap = 0;
+        cudaEvent_t copied = nullptr;
+        bool in_use = false;  // acquired and not yet released
+        bool pending = false; // a copy from it may still run
+    };
+    Buffer* acquire(size_t bytes) {
+        std::lock_guard<std::mutex> lock(mu_);
+        Buffer* pick = nullptr;
+        for (auto& b : buffers_) {
+            if (b->in_use || b->cap < bytes) continue;
+            if (b->pending) {
+                if (cudaEventQuery(b->copied) != cudaSuccess) {
+                    cudaGetLastError();  // not ready yet
+                    continue;
+                }
+                b->pending = false;
+            }
+            if (!pick || b->cap < pick->cap) pick = b.get();
+        }
+        if (!pick) {
+            auto b = std::make_unique<Buffer>();
+            b->cap = std::max<size_t>((bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1), size_t(1) << 20);
+            void* p = nullptr;
+            check(cudaHostAlloc(&p, b->cap, cudaHostAllocPortable), "cudaHostAlloc(table staging)");
+            b->data = static_cast<unsigned char*>(p);
+            check(cudaEventCreateWithFlags(&b->copied, cudaEventDisableTiming), "cudaEventCreate");
+            pick = b.get();
+            buffers_.push_back(std::move(b));
+        }
+        pick->in_use = true;
+        return pick;
+    }
+    // The copy from `b` was enqueued on `stream`: the buffer is free again once it completed.
+    void release(Buffer* b, cudaStream_t stream) {
+        std::lock_guard<std::mutex> lock(mu_);
+        b->pending = cudaEventRecord(b->copied, stream) == cudaSuccess;
+        if (!b->pending) cudaStreamSynchronize(stream);  // could not track it: wait instead
+        b->in_use = false;
+    }
+
+private:
+    std::mutex mu_;
+    std::vector<std::unique_ptr<Buffer>> buffers_;
+};
+
+UploadStaging& upload_staging(int device) {
+    static std::mutex mu;
+    static std::map<int, UploadStaging*> all;  // never destroyed: buffers outlive static teardown
+    std::lock_guard<std::mutex> lock(mu);
+    auto& s = all[device];
+    if (!s) s = new UploadStaging;
+    return *s;
+}
+
 template <class T>
-void pack_table(const std::vector<std::complex<double>>& t, std::vector<unsigned char>& blob, size_t off) {
-    T* dst = reinterpret_cast<T*>(blob.data() + off);
+void pack_table(const std::vector<std::complex<double>>& t, unsigned char* blob, size_t off) {
+    T* dst = reinterpret_cast<T*>(blob + off);
     for (size_t i = 0; i < t.size(); ++i) {
         dst[2 * i] = static_cast<T>(t[i].real());
         dst[2 * i + 1] = static_cast<T>(t[i].imag());
@@ -440,15 +503,20 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         offsets[i] = total;
         total += (plan->spec.table_sizes[i] * cs + 255) / 256 * 256;
     }
-    std::vector<unsigned char> blob(std::max<size_t>(total, 256), 0);
-    for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
-        if (req.dbl) pack_table<double>(plan->spec.tables[i], blob, offsets[i]);
-        else pack_table<float>(plan->spec.tables[i], blob, offsets[i]);
-    }
+    const size_t table_bytes = std::max<size_t>(total, 256);
     cudaStream_t ms = memory_stream(device);
-    check(cudaMallocAsync(&plan->table_mem, blob.size(), ms), "cudaMallocAsync(tables)");
-    plan->table_bytes = blob.size();
-    check(cudaMemcpyAsync(plan->table_mem, blob.data(), blob.size(), cudaMemcpyHostToDevice, ms), "cudaMemcpy(tables)");
+    UploadStaging& staging = upload_staging(device);
+    UploadStaging::Buffer* blob = staging.acquire(table_bytes);
+    std::memset(blob->data, 0, table_bytes);
+    for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
+        if (req.dbl) pack_table<double>(plan->spec.tables[i], blob->data, offsets[i]);
+        else pack_table<float>(plan->spec.tables[i], blob->data, offsets[i]);
+    }
+    cudaError_t up = cudaMallocAsync(&plan->table_mem, table_bytes, ms);
+    if (up == cudaSuccess) up = cudaMemcpyAsync(plan->table_mem, blob->data, table_bytes, cudaMemcpyHostToDevice, ms);
+    staging.release(blob, ms);
+    check(up, "plan table upload");
+    plan->table_bytes = table_bytes;
     plan->status = status_pool().acquire();
     plan->owns_status = true;
     // failure-detection testing: SYCLFFT_B200_WAIT_POLLS sets the wait limit of new plans

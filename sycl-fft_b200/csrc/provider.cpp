@@ -1398,9 +1398,8 @@ std::map<std::string, std::string>& tune_cache() {
     return cache;
 }
 
-float time_candidate(DevicePlan* plan, int64_t batch, void* a, void* b) {
-    cudaStream_t s = nullptr;
-    check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+// Device time of one execute of a candidate plan on the tuning stream `s` (best of 3 x 3).
+float time_candidate(DevicePlan* plan, int64_t batch, void* a, void* b, cudaStream_t s) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1422,7 +1421,6 @@ float time_candidate(DevicePlan* plan, int64_t batch, void* a, void* b) {
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    cudaStreamDestroy(s);
     return best;
 }
 
@@ -1468,13 +1466,21 @@ PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
     const uint64_t per = elements / req.batch;
     // time on at most ~256 MB per buffer: a sub-batch has the same per-line kernel behaviour
     const int64_t batch = static_cast<int64_t>(std::max<uint64_t>(1, std::min<uint64_t>(req.batch, (uint64_t(256) << 20) / (per * cs))));
+    // Everything runs on a private stream, stream-ordered (cudaMallocAsync, cudaFreeAsync): a
+    // tuning plan made inside a busy process waits for its own work, not for the device.
+    cudaStream_t ts = nullptr;
+    check(cudaStreamCreateWithFlags(&ts, cudaStreamNonBlocking), "cudaStreamCreate(autotune)");
     void *a = nullptr, *b = nullptr;
-    check(cudaMalloc(&a, batch * per * cs), "cudaMalloc(autotune)");
-    if (cudaMalloc(&b, batch * per * cs) != cudaSuccess) {
-        cudaFree(a);
-        throw std::runtime_error("cudaMalloc(autotune)");
+    cudaError_t ae = cudaMallocAsync(&a, batch * per * cs, ts);
+    if (ae == cudaSuccess) ae = cudaMallocAsync(&b, batch * per * cs, ts);
+    if (ae == cudaSuccess) ae = cudaMemsetAsync(a, 0, batch * per * cs, ts);
+    if (ae != cudaSuccess) {
+        if (a) cudaFreeAsync(a, ts);
+        if (b) cudaFreeAsync(b, ts);
+        cudaStreamSynchronize(ts);
+        cudaStreamDestroy(ts);
+        throw std::runtime_error(std::string("autotune buffers: ") + cudaGetErrorString(ae));
     }
-    cudaMemset(a, 0, batch * per * cs);
     std::ostringstream rep;
     rep << "{\"timed_batch\":" << batch << ",\"candidates\":{";
     std::string best_name = "default";
@@ -1499,7 +1505,7 @@ PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
         } catch (...) {
             continue;
         }
-        const float ms = time_candidate(p.get(), batch, a, b);
+        const float ms = time_candidate(p.get(), batch, a, b, ts);
         rep << (first ? "" : ",") << "\"" << k.name << "\":" << ms;
         first = false;
         if (ms < best) {
@@ -1507,9 +1513,10 @@ PlanRequest tune(const PlanRequest& req, int device, std::string* report) {
             best_name = k.name;
         }
     }
-    cudaDeviceSynchronize();
-    cudaFree(a);
-    cudaFree(b);
+    cudaFreeAsync(a, ts);
+    cudaFreeAsync(b, ts);
+    cudaStreamSynchronize(ts);
+    cudaStreamDestroy(ts);
     rep << "},\"choice\":\"" << best_name << "\"}";
     *report = rep.str();
     cache[key] = best_name;

@@ -157,10 +157,10 @@ def _event_class():
         torch = _torch()
 
         class ExecutionEvent(torch.cuda.Event):
-            def __new__(cls, lib=None, handles=()):
+            def __new__(cls, lib=None, plans=()):
                 self = super().__new__(cls)
                 self._lib = lib
-                self._handles = handles
+                self._plans = plans  # kept alive while the event is: their status words are read
                 return self
 
             def synchronize(self):
@@ -171,7 +171,10 @@ def _event_class():
                 self.synchronize()
 
             def _check(self):
-                for h in self._handles:
+                for p in self._plans:
+                    h = getattr(p, "_handle", None)
+                    if not h:
+                        continue  # closed or moved from: nothing left to report
                     code = self._lib.syclfft_b200_plan_take_status(h)
                     if code > 0:
                         raise SyclfftError(error_code.execution_failed,
@@ -234,7 +237,7 @@ def execute_host(stages, input, output=None, batch=None, stream=None):
                                                   s.cuda_stream, err, _provider.ERR_CAP)
         if rc != 0 or err.value:
             raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
-        ev = _event_class()(first._lib, tuple(p._handle for p in locks))
+        ev = _event_class()(first._lib, tuple(locks))
         ev.record(s)
         for p in locks:
             p._last_event = ev
@@ -438,7 +441,7 @@ class Plan:
             # the provider writes the error buffer only on failure (a non-zero return)
             if self._execute(self._handle, inp, out, handle, err, _provider.ERR_CAP) != 0:
                 raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
-            ev = (_EVENT_CLS or _event_class())(self._lib, (self._handle,))
+            ev = (_EVENT_CLS or _event_class())(self._lib, (self,))
             ev.record(s)
             # an event recorded inside a capture belongs to the graph: ordering of replays
             # against later executes is the caller's, as for any captured work

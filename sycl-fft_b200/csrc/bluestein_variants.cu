@@ -1,5 +1,6 @@
 // Instantiations of the size-specialised Bluestein pass kernels listed in
-// bluestein_catalog.h, one compile unit per SFB_BLUE_PART = 4 * double + kind.
+// bluestein_catalog.h, one compile unit per SFB_BLUE_PART = 8 * rader + 4 * double + kind
+// (rader: the Rader features of the same entries).
 #include <atomic>
 #include <climits>
 #include <type_traits>
@@ -19,9 +20,14 @@ constexpr int kMaxDevices = 64;
 
 // Features of each kind: fused single pass, forward column pass, row convolution pass,
 // inverse column pass.
-constexpr int kBlueFeat[4] = {kFeatPremul | kFeatConv | kFeatPostmul, kFeatPremul | kFeatTw4,
-                              kFeatConv | kFeatTw4 | kFeatTw4Conj, kFeatPostmul};
+constexpr int kBlueFeat[8] = {kFeatPremul | kFeatConv | kFeatPostmul, kFeatPremul | kFeatTw4,
+                              kFeatConv | kFeatTw4 | kFeatTw4Conj, kFeatPostmul,
+                              // Rader: gather, convolution with the bin-0 term, scatter
+                              kFeatGather | kFeatConv | kFeatScatter | kFeatRaderDC, kFeatGather | kFeatTw4,
+                              kFeatConv | kFeatTw4 | kFeatTw4Conj | kFeatRaderDC, kFeatScatter};
 constexpr bool kBlueModeC[4] = {false, true, false, true};
+
+constexpr int kRader = SFB_BLUE_PART / 8;
 
 template <bool ENABLED, class T, int KIND, int N, int TPL, int W, int MAXT, int... Rs>
 struct BlueLauncher {
@@ -34,7 +40,7 @@ template <class T, int KIND, int N, int TPL, int W, int MAXT, int... Rs>
 struct BlueLauncher<true, T, KIND, N, TPL, W, MAXT, Rs...> {
     static cudaError_t run(const FixedParams& p, int threads, size_t smem, int64_t grid, const void* in, void* out,
                            cudaStream_t stream) {
-        auto kernel = fft_fixed_kernel<T, N, TPL, kBlueModeC[KIND], W, kBlueFeat[KIND], MAXT, 64, Rs...>;
+        auto kernel = fft_fixed_kernel<T, N, TPL, kBlueModeC[KIND], W, kBlueFeat[kRader * 4 + KIND], MAXT, 64, Rs...>;
         static std::atomic<int> configured[kMaxDevices];
         int dev = 0;
         cudaError_t e = cudaGetDevice(&dev);
@@ -66,7 +72,7 @@ cudaError_t SFB_BLUE_CAT(launch_blue_p, SFB_BLUE_PART)(int id, const FixedParams
     switch (id) {
 #define SFB_X(ID, DBL, KIND, N, TPL, W, MAXT, ...)                                                            \
     case ID:                                                                                                  \
-        return BlueLauncher<((DBL) * 4 + (KIND)) == SFB_BLUE_PART, std::conditional_t<(DBL) != 0, double, float>, \
+        return BlueLauncher<((DBL) * 4 + (KIND)) == SFB_BLUE_PART % 8, std::conditional_t<(DBL) != 0, double, float>, \
                             KIND, N, TPL, W, MAXT, __VA_ARGS__>::run(p, threads, smem, grid, in, out, stream);
         SFB_BLUESTEIN_CATALOG(SFB_X)
 #undef SFB_X

@@ -6,9 +6,11 @@
 //
 // Plain passes use them (a whole line per CTA row, conjugation for inverse transforms and
 // the normalization scale fused into the store), the four-step column and row passes
-// (twiddle fused into the store, transposed store), and the Bluestein passes: a zero-padded
+// (twiddle fused into the store, transposed store), the Bluestein passes (a zero-padded
 // chirp pre-multiply on the first load, a spectrum multiply between two FFTs held in
-// shared memory, and a chirp post-multiply with truncation on the last store.
+// shared memory, and a chirp post-multiply with truncation on the last store) and the Rader
+// passes of prime lengths (a permuted gather on the first load, the same spectrum multiply
+// with the x[0] term, a permuted scatter on the last store).
 //   kModeK: lines are contiguous (line pitch `in_pitch`), threads walk elements;
 //   kModeC: lines are strided columns (element stride `in_ks`, columns contiguous),
 //           threads walk W adjacent columns so every access is a W-wide segment.
@@ -52,6 +54,22 @@ struct FixedParams {
     int pw_stride = 0;
     int conj_mid = 0;
     int flip_in = 0, flip_out = 0;
+    // Rader features (a prime length L whose convolution length M = L - 1 the catalog covers:
+    // with g a primitive root mod L, X[g^-q] = x[0] + sum_p x[g^p] W^(g^(p-q)), a cyclic
+    // convolution of length M). kFeatGather loads element g as x[perm_in[g]] from the start
+    // of the line (g < in_len); kFeatScatter stores element g to y[perm_out[g]] (g < out_len);
+    // kFeatRaderDC (the convolution pass): bin 0 of the first FFT is A0 = sum over the
+    // gathered line, so X[0] = x[0] + A0 is stored at y[0], and x[0] is added to bin 0 of the
+    // spectrum product, which adds it to every convolution output. dc_x / dc_y are the line
+    // starts of x and y for the three-pass row kernel (line o = row / rows), dc_scale and
+    // dc_flip_in / dc_flip_out the scale and direction flips of the outputs around it.
+    const int* perm_in = nullptr;
+    const int* perm_out = nullptr;
+    const void* dc_x = nullptr;
+    void* dc_y = nullptr;
+    int64_t dc_x_pitch = 0, dc_y_pitch = 0;
+    double dc_scale = 1.0;
+    int dc_flip_in = 0, dc_flip_out = 0;
 };
 
 // Features (bits): kFeatTw4 four-step twiddle on the last store, kFeatTStore transposed
@@ -78,6 +96,9 @@ enum : int {
     kFeatLoadCS = 4096,   // first-stage global loads and last-stage global stores marked
     kFeatStoreCS = 8192,  // streaming (ld/st .cs, evicted first): data read or written once, so
                           // it does not push an L2-resident ring out of the cache
+    kFeatGather = 16384,  // Rader: first-stage loads through perm_in
+    kFeatScatter = 32768, // Rader: last-stage stores through perm_out
+    kFeatRaderDC = 65536, // Rader: X[0] and the x[0] term at bin 0 of the convolution pass
 };
 
 template <int FEAT, class C>
@@ -124,6 +145,13 @@ struct FixedCtx {
     const C *premul, *postmul, *pw;  // pw: pointwise table of this line (kFeatConv)
     int g_k, in_len, out_len;
     bool conj_mid, flip_in, flip_out;
+    const int *perm_in, *perm_out;  // Rader permutations
+    const C* gline;                  // start of this thread's input line (kFeatGather)
+    C* gline_out;                    // start of its output line (kFeatScatter)
+    const C* rx;                     // x line and y line of the bin-0 term (kFeatRaderDC)
+    C* ry;
+    T dc_scale;
+    bool dc_flip_in, dc_flip_out;
 };
 
 template <class T> __host__ __device__ constexpr int pad_shift_c() { return sizeof(T) == 4 ? 4 : 3; }
@@ -167,6 +195,19 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                         a = fixed_load<FEAT>(MODEC ? X.gin + (int64_t)k * X.in_ks : X.gin + k);
                         if (X.flip_in) a.y = -a.y;
                         a = cmul(a, __ldg(X.premul + g));
+                        if (X.conj_in) a.y = -a.y;
+                    }
+                    v[i * R + r] = a;
+                }
+            } else if constexpr (FIRST && (FEAT & kFeatGather)) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const int k = j + r * NR;
+                    const int g = k * X.g_k + X.sel;
+                    C a = cmake<C>(T(0), T(0));
+                    if (X.line_ok && g < X.in_len) {
+                        a = X.gline[__ldg(X.perm_in + g)];
+                        if (X.flip_in) a.y = -a.y;
                         if (X.conj_in) a.y = -a.y;
                     }
                     v[i * R + r] = a;
@@ -231,9 +272,28 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 // natural order into shared memory: the transposed store, or the second FFT
                 // of a Bluestein convolution (after the spectrum multiply), follows
                 if constexpr (FEAT & kFeatMid) {
+                    C dc = cmake<C>(T(0), T(0));
+                    if constexpr (FEAT & kFeatRaderDC) {
+                        // bin 0 of this line (row 0, element 0): X[0] = x[0] + A0
+                        if (X.sel == 0 && j == 0 && X.line_ok) {
+                            dc = X.rx[0];
+                            if (X.dc_flip_in) dc.y = -dc.y;
+                            C y0 = cmake<C>(dc.x + u[0].x, dc.y + u[0].y);
+                            if (X.dc_flip_out) y0.y = -y0.y;
+                            y0.x *= X.dc_scale;
+                            y0.y *= X.dc_scale;
+                            X.ry[0] = y0;
+                        }
+                    }
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         u[r] = cmul(u[r], __ldg(X.pw + j + r * NR));
+                        if constexpr (FEAT & kFeatRaderDC) {
+                            if (r == 0) {
+                                u[0].x += dc.x;
+                                u[0].y += dc.y;
+                            }
+                        }
                         if (X.conj_mid) u[r].y = -u[r].y;
                     }
                 }
@@ -265,12 +325,19 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                             if (g >= X.out_len) continue;
                             a = cmul(a, __ldg(X.postmul + g));
                         }
+                        [[maybe_unused]] int g = 0;
+                        if constexpr (FEAT & kFeatScatter) {
+                            g = k * X.g_k + X.sel;
+                            if (g >= X.out_len) continue;
+                        }
                         a.x *= X.scale;
                         a.y *= X.scale;
-                        if constexpr (FEAT & kFeatPostmul) {
+                        if constexpr (FEAT & (kFeatPostmul | kFeatScatter)) {
                             if (X.flip_out) a.y = -a.y;
                         }
-                        C* dst = MODEC ? X.gout + (int64_t)k * X.out_ks : X.gout + k;
+                        C* dst = (FEAT & kFeatScatter) ? X.gline_out + __ldg(X.perm_out + g)
+                                 : MODEC               ? X.gout + (int64_t)k * X.out_ks
+                                                       : X.gout + k;
                         if constexpr (FEAT & kFeatStoreCS) __stcs(dst, a);
                         else *dst = a;
                     }
@@ -329,6 +396,8 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
     X.conj_mid = P.conj_mid != 0;
     X.flip_in = P.flip_in != 0;
     X.flip_out = P.flip_out != 0;
+    X.perm_in = P.perm_in;
+    X.perm_out = P.perm_out;
     const int tid = threadIdx.x;
     if constexpr (MODEC) {
         const int w = tid % W;
@@ -345,6 +414,8 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         X.sm = sm + w;
         X.gin = in + o * P.in_hi + c;
         X.gout = out + o * P.out_hi + c;
+        X.gline = in + o * P.in_hi;
+        X.gline_out = out + o * P.out_hi;
         X.in_ks = P.in_ks;
         X.out_ks = P.out_ks;
     } else {
@@ -364,12 +435,33 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         X.tw4_hi = static_cast<const C*>(P.tw4_hi);
         X.tw4_lo = static_cast<const C*>(P.tw4_lo);
         X.tw4_shift = P.tw4_shift;
+        X.gline = X.gin;
+        X.gline_out = X.gout;
+        if constexpr (FEAT & kFeatRaderDC) {
+            if constexpr (FEAT & kFeatGather) {
+                // whole line in this CTA row (fused single pass): its own line, scale and flips
+                X.rx = X.gin;
+                X.ry = X.gout;
+                X.dc_scale = X.scale;
+                X.dc_flip_in = X.flip_in;
+                X.dc_flip_out = X.flip_out;
+            } else {
+                // three-pass row kernel: row c is row c % rows of line c / rows
+                const int64_t o = c / P.rows;
+                X.rx = static_cast<const C*>(P.dc_x) + o * P.dc_x_pitch;
+                X.ry = static_cast<C*>(P.dc_y) + o * P.dc_y_pitch;
+                X.dc_scale = static_cast<T>(P.dc_scale);
+                X.dc_flip_in = P.dc_flip_in != 0;
+                X.dc_flip_out = P.dc_flip_out != 0;
+            }
+        }
     }
     if constexpr (FEAT & kFeatConv) {
         // Bluestein convolution: FFT, spectrum multiply (to shared memory), FFT again
         X.pw = static_cast<const C*>(P.pointwise) + (int64_t)X.sel * P.pw_stride;
-        fixed_stages<T, N, TPL, MODEC, W, (FEAT & kFeatPremul) | kFeatMid, 1, 0, true, Rs...>(X);
-        fixed_stages<T, N, TPL, MODEC, W, FEAT & ~(kFeatPremul | kFeatConv), 1, 0, false, Rs...>(X);
+        constexpr int kFirstOnly = kFeatPremul | kFeatGather | kFeatRaderDC;
+        fixed_stages<T, N, TPL, MODEC, W, (FEAT & kFirstOnly) | kFeatMid, 1, 0, true, Rs...>(X);
+        fixed_stages<T, N, TPL, MODEC, W, FEAT & ~(kFirstOnly | kFeatConv), 1, 0, false, Rs...>(X);
         return;
     }
     fixed_stages<T, N, TPL, MODEC, W, FEAT, 1, 0, true, Rs...>(X);

@@ -22,6 +22,6 @@
 // COLI_ID of bluestein_catalog.h) in one launch with the M-point intermediate in the ring.
 // X(ID, DOUBLE, N1, TPL1, W1, COLF_ID, N2, TPL2, W2, ROWS_ID, COLI_ID, THREADS, MINB, (RC...), (RR...))
 #define SFB_FUSEDBLUE_CATALOG(X)                                                                  \
-    X(0, 0, 512, 32, 16, 56, 320, 22, 16, 42, 57, 512, 2, (16, 16, 2), (16, 4, 5))               \
-    X(1, 1, 512, 64, 8, 112, 320, 64, 8, 98, 113, 512, 2, (8, 8, 8), (8, 8, 5))                  \
+    X(0, 0, 256, 16, 16, 54, 512, 32, 16, 45, 55, 512, 2, (16, 16), (16, 16, 2))                 \
+    X(1, 1, 256, 32, 8, 110, 512, 64, 8, 101, 111, 512, 2, (8, 8, 4), (8, 8, 8))                 \
     X(2, 1, 128, 16, 8, 108, 80, 16, 8, 90, 109, 128, 8, (8, 8, 2), (8, 2, 5))

@@ -3,7 +3,7 @@
 features kFeatPremul / kFeatConv / kFeatPostmul) instantiated by bluestein_variants.cu.
 
 Convolution lengths are 2^a * f, f in {1, 3, 5, 7}: a Bluestein axis of length L takes the
-smallest catalog length (or product of a column and a row length) >= 2L - 1, so the padding
+smallest catalog length (or product of a column and a row length) >= 2L - 2, so the padding
 stays within about 25% of the smallest 7-smooth length while every stage is a large radix.
 Run: python gen_bluestein_catalog.py > bluestein_catalog.h
 """

@@ -79,6 +79,10 @@ struct PassParams {
     // conj_in / conj_out by passes that carry premul / postmul tables (Bluestein), where the
     // plan's own conjugations sit between the FFTs and the chirp products.
     int flip_in = 0, flip_out = 0;
+    // Rader passes: int32 permutations of the line (load element g from perm_in[g], store
+    // element g to perm_out[g], both relative to the line start)
+    const void* perm_in = nullptr;
+    const void* perm_out = nullptr;
     // Size-specialised four-step row pass: row l (= o*ts_rows + k1) stored at
     // (l / ts_rows) * ts_line + l % ts_rows + k * ts_rows.
     int64_t ts_rows = 0, ts_line = 0;

@@ -118,6 +118,11 @@ struct Builder {
         return static_cast<int>(plan.tables.size()) - 1;
     }
 
+    int add_index_table(std::vector<int32_t> t) {
+        plan.index_tables.push_back(std::move(t));
+        return static_cast<int>(plan.index_tables.size()) - 1;
+    }
+
     // A table of n entries the device fills (no host data).
     int add_device_table(size_t n) {
         plan.table_sizes.push_back(n);
@@ -461,15 +466,227 @@ struct Builder {
         return w;
     }
 
+    // Rader on the size-specialised Bluestein kernels (contiguous axes, prime L): with g a
+    // primitive root mod L, X[g^-q] = x[0] + sum_{p<M} x[g^p] W^(g^(p-q)), M = L - 1, a cyclic
+    // convolution of a[p] = x[g^p] with b[m] = W^(g^-m) (W = exp(sgn 2 pi i / L)). It runs on
+    // the Bluestein kernels' Rader instantiations: the gather a[p] = x[perm_in[p]] replaces
+    // the chirp pre-multiply, the scatter y[perm_out[q]] the post-multiply and truncation, and
+    // bin 0 of the convolution pass gives X[0] = x[0] + sum a and adds x[0] to every output.
+    // M = L - 1 instead of Bluestein's >= 2L - 2 halves the convolution; taken where the catalog
+    // has a fused kernel of length M or a column x row split of it.
+    bool rader_fixed(int ax, int64_t L, int64_t O, Buf& cur) {
+        if (req.no_fixed || req.no_rader || L < 3 || L > (int64_t(1) << 30) || !is_prime(L)) return false;
+        const int64_t M = L - 1;
+        int count = 0;
+        const BlueEntry* cat = blue_entries(&count);
+        const int ps_shift = pad_shift_for(req.dbl);
+        const BlueEntry* fused = nullptr;
+        for (int i = 0; i < count && !fused; ++i) {
+            const BlueEntry& e = cat[i];
+            if (e.dbl == (req.dbl ? 1 : 0) && e.kind == kBlueFused && e.n == M &&
+                int64_t(kmode_pitch(e.n, ps_shift)) * cs <= smem_limit)
+                fused = &e;
+        }
+        const BlueEntry *cf = nullptr, *rc = nullptr, *ci = nullptr;
+        for (int i = 0; i < count && !fused; ++i) {
+            const BlueEntry& a = cat[i];
+            if (a.dbl != (req.dbl ? 1 : 0) || a.kind != kBlueColsFwd || M % a.n) continue;
+            if (int64_t(a.n) * a.w * cs > smem_limit) continue;
+            for (int k = 0; k < count; ++k) {
+                const BlueEntry& b = cat[k];
+                if (b.dbl != (req.dbl ? 1 : 0) || b.kind != kBlueRowsConv || int64_t(a.n) * b.n != M) continue;
+                if (int64_t(kmode_pitch(b.n, ps_shift)) * cs > smem_limit) continue;
+                if (!cf || std::abs(std::log(double(b.n) / a.n)) < std::abs(std::log(double(rc->n) / cf->n))) {
+                    cf = &a;
+                    rc = &b;
+                }
+            }
+        }
+        if (cf)
+            for (int i = 0; i < count; ++i)
+                if (cat[i].dbl == cf->dbl && cat[i].kind == kBlueColsInv && cat[i].n == cf->n) ci = &cat[i];
+        if (!fused && !(cf && rc && ci)) return false;
+
+        const int sgn = req.direction;
+        const int64_t E = static_cast<int64_t>(plan.elements);
+        const int64_t n1 = fused ? 0 : cf->n, n2 = fused ? 0 : rc->n;
+        const uint64_t g = primitive_root(static_cast<uint64_t>(L));
+        const uint64_t ginv = pow_mod(g, static_cast<uint64_t>(L) - 2, static_cast<uint64_t>(L));
+        std::vector<int32_t> pin(M), pout(M);
+        for (uint64_t i = 0, a = 1, b = 1; i < static_cast<uint64_t>(M); ++i) {
+            pin[i] = static_cast<int32_t>(a);
+            pout[i] = static_cast<int32_t>(b);
+            a = a * g % static_cast<uint64_t>(L);
+            b = b * ginv % static_cast<uint64_t>(L);
+        }
+        // spectrum of b / M (the inverse FFT of the product then carries no scale); three-pass
+        // plans take it permuted, K'[k1*n2 + k2] = K[k1 + n1*k2]
+        auto spec = cached_table({L, M, sgn, n1, n2, -500}, [&] {
+            std::vector<std::complex<double>> k(M);
+            for (int64_t m = 0; m < M; ++m) k[m] = cis_neg(-int64_t(sgn) * pout[m], L);
+            host_fft_fp64(k, -1);
+            for (auto& v : k) v /= static_cast<double>(M);
+            if (fused) return k;
+            std::vector<std::complex<double>> kp(M);
+            for (int64_t k1 = 0; k1 < n1; ++k1)
+                for (int64_t k2 = 0; k2 < n2; ++k2) kp[k1 * n2 + k2] = k[k1 + n1 * k2];
+            return kp;
+        });
+        const int spec_id = add_table(*spec);
+        const int pin_id = add_index_table(std::move(pin));
+        const int pout_id = add_index_table(std::move(pout));
+        if (fused) {
+            PassSpec ps;
+            ps.kind = "rader_fused";
+            ps.axis = ax;
+            PassParams& p = ps.p;
+            p.n = static_cast<int>(M);
+            p.mode = kModeK;
+            p.n_outer = 1;
+            p.n_cols = O;
+            p.in.cs = L;
+            p.in.ks = 1;
+            p.out = p.in;
+            p.in_len = p.out_len = M;
+            ps.tables.perm_in = pin_id;
+            ps.tables.perm_out = pout_id;
+            ps.tables.pointwise = spec_id;
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            p.fft1 = entry_seq(*fused);
+            p.fft2 = p.fft1;
+            use_base_table(ps);
+            ps.tables.tw2 = ps.tables.tw1;
+            p.pad_shift = ps_shift;
+            p.pitch = kmode_pitch(p.n, ps_shift);
+            p.tpl = fused->tpl;
+            p.w = lines_per_cta(fused->tpl, fused->maxt, p.pitch, O);
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.col_tiles;
+            ps.threads = round_up(p.w * p.tpl, 32);
+            ps.smem_bytes = static_cast<int64_t>(p.w) * p.pitch * cs;
+            ps.kc.maxt = fused->maxt;
+            ps.blue_id = fused->id;
+            ps.blue_kind = kBlueFused;
+            ps.rader = true;
+            ps.src = cur;
+            ps.dst = Buf::Output;
+            ps.bytes_moved = 2 * E * cs;
+            plan.passes.push_back(ps);
+            cur = Buf::Output;
+            return true;
+        }
+        plan.scratch_elements = std::max<uint64_t>(plan.scratch_elements, static_cast<uint64_t>(O * M));
+        auto cols = [&](PassSpec& a, const BlueEntry& e) {
+            PassParams& p = a.p;
+            p.n = static_cast<int>(n1);
+            p.mode = kModeC;
+            p.g_k = n2;
+            p.n_outer = O;
+            p.n_cols = n2;
+            p.sel_mode = kSelCol;
+            p.fft1 = entry_seq(e);
+            use_base_table(a);
+            p.tpl = e.tpl;
+            p.w = e.w;
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.n_outer * p.col_tiles;
+            a.threads = round_up(e.w * e.tpl, 32);
+            a.smem_bytes = static_cast<int64_t>(e.w) * n1 * cs;
+            a.kc.maxt = e.maxt;
+            a.blue_id = e.id;
+            a.blue_kind = e.kind;
+            a.rader = true;
+        };
+        // pass 1: columns of the gathered line a[p] = x[g^p]; W_M^(k1*c) on the store
+        PassSpec a;
+        a.kind = "rader_cols_fwd";
+        a.axis = ax;
+        cols(a, *cf);
+        a.p.in.hi = L; a.p.in.cs = 1; a.p.in.ks = n2;
+        a.p.out.hi = M; a.p.out.cs = 1; a.p.out.ks = n2;
+        a.p.in_len = M;
+        a.p.out_len = kNoLimit;
+        a.tables.perm_in = pin_id;
+        add_tw4(a, M, -1);
+        a.src = cur;
+        a.dst = Buf::Scratch;
+        a.bytes_moved = (E + O * M) * cs;
+        plan.passes.push_back(a);
+        // pass 2: rows: FFT, spectrum multiply (and the x[0] term, X[0] stored), inverse FFT,
+        // inverse twiddle, in place
+        PassSpec b;
+        b.kind = "rader_rows_conv";
+        b.axis = ax;
+        {
+            PassParams& p = b.p;
+            p.n = static_cast<int>(n2);
+            p.mode = kModeK;
+            p.n_outer = 1;
+            p.n_cols = O * n1;
+            p.in.cs = n2;
+            p.in.ks = 1;
+            p.out = p.in;
+            p.sel_mode = kSelColMod;
+            p.sel_d = n1;
+            p.in_len = p.out_len = kNoLimit;
+            b.tables.pointwise = spec_id;
+            p.pw_stride = n2;
+            p.conj_mid = 1;
+            p.conj_out = 1;
+            p.fft1 = entry_seq(*rc);
+            p.fft2 = p.fft1;
+            use_base_table(b);
+            b.tables.tw2 = b.tables.tw1;
+            add_tw4(b, M, +1);
+            p.pad_shift = ps_shift;
+            p.pitch = kmode_pitch(p.n, ps_shift);
+            p.tpl = rc->tpl;
+            p.w = lines_per_cta(rc->tpl, rc->maxt, p.pitch, p.n_cols);
+            p.col_tiles = (p.n_cols + p.w - 1) / p.w;
+            p.tiles = p.col_tiles;
+            b.threads = round_up(p.w * p.tpl, 32);
+            b.smem_bytes = static_cast<int64_t>(p.w) * p.pitch * cs;
+            b.kc.maxt = rc->maxt;
+            b.blue_id = rc->id;
+            b.blue_kind = kBlueRowsConv;
+            b.rader = true;
+            b.rader_dc = true;
+            b.rader_src = cur;
+            b.src = Buf::Scratch;
+            b.dst = Buf::Scratch;
+            b.bytes_moved = 2 * O * M * cs;
+        }
+        plan.passes.push_back(b);
+        // pass 3: columns: inverse FFT, scatter y[g^-q] (positions 1 .. L-1)
+        PassSpec c;
+        c.kind = "rader_cols_inv";
+        c.axis = ax;
+        cols(c, *ci);
+        c.p.in.hi = M; c.p.in.cs = 1; c.p.in.ks = n2;
+        c.p.out.hi = L; c.p.out.cs = 1; c.p.out.ks = n2;
+        c.p.in_len = kNoLimit;
+        c.p.out_len = M;
+        c.p.conj_in = 1;
+        c.p.conj_out = 1;
+        c.tables.perm_out = pout_id;
+        c.src = Buf::Scratch;
+        c.dst = Buf::Output;
+        c.bytes_moved = (O * M + E) * cs;
+        plan.passes.push_back(c);
+        cur = Buf::Output;
+        return true;
+    }
+
     // Bluestein on the size-specialised kernels (contiguous axes): the smallest catalog
-    // convolution length M >= 2L - 1, as one fused pass where a fused kernel of length M fits
-    // a CTA, else as M = n1 * n2 over a column kernel (n1) and a row kernel (n2) in three
-    // passes. Returns false (generic kernels) when the catalog has no such length.
+    // convolution length M >= 2L - 2 (bluestein_length), as one fused pass where a fused
+    // kernel of length M fits a CTA, else as M = n1 * n2 over a column kernel (n1) and a row
+    // kernel (n2) in three passes. Returns false (generic kernels) when the catalog has no such length.
     bool bluestein_fixed(int ax, int64_t L, int64_t O, Buf& cur) {
         if (req.no_fixed) return false;
         int count = 0;
         const BlueEntry* cat = blue_entries(&count);
-        const int64_t need = 2 * L - 1;
+        const int64_t need = 2 * L - 2;
         const int ps_shift = pad_shift_for(req.dbl);
         const BlueEntry* fused = nullptr;
         for (int i = 0; i < count; ++i) {
@@ -807,6 +1024,7 @@ struct Builder {
             return;
         }
 
+        if (s == 1 && rader_fixed(ax, L, O, cur)) return;
         if (s == 1 && bluestein_fixed(ax, L, O, cur)) return;
         // Bluestein: y_k = c_k * sum_n (x_n c_n) h_{k-n}, c_n = exp(-i*sgn*pi*n^2/L) conj-chirp,
         // h_n = conj(c_n) (exact n^2 mod 2L reduction), convolution of length M via FFT.
@@ -1102,14 +1320,55 @@ double normalization_scale(int mode, int direction, uint64_t n) {
     }
 }
 
+uint64_t pow_mod(uint64_t b, uint64_t e, uint64_t m) {
+    unsigned __int128 r = 1, x = b % m;
+    for (; e; e >>= 1) {
+        if (e & 1) r = r * x % m;
+        x = x * x % m;
+    }
+    return static_cast<uint64_t>(r);
+}
+
+bool is_prime(uint64_t n) {
+    if (n < 2) return false;
+    for (uint64_t d = 2; d * d <= n; ++d)
+        if (n % d == 0) return false;
+    return true;
+}
+
+// Smallest generator of the multiplicative group mod a prime p: g^((p-1)/q) != 1 for every
+// prime factor q of p - 1.
+uint64_t primitive_root(uint64_t p) {
+    if (p == 2) return 1;
+    std::vector<uint64_t> qs;
+    uint64_t m = p - 1;
+    for (uint64_t d = 2; d * d <= m; ++d) {
+        if (m % d) continue;
+        qs.push_back(d);
+        while (m % d == 0) m /= d;
+    }
+    if (m > 1) qs.push_back(m);
+    for (uint64_t g = 2; g < p; ++g) {
+        bool ok = true;
+        for (uint64_t q : qs) ok = ok && pow_mod(g, (p - 1) / q, p) != 1;
+        if (ok) return g;
+    }
+    throw std::invalid_argument("no primitive root");
+}
+
 bool smooth7(uint64_t n) {
     Factors f;
     return factor7(n, f);
 }
 
+// The cyclic convolution y[k] = sum_n a[n] b[k - n], k, n in [0, L), reads the chirp b at
+// d = k - n in [-(L-1), L-1]. A cyclic length M keeps those reads apart except where two of
+// them differ by M; for M = 2L - 2 the only such pair is d = L-1 and d = -(L-1), and the chirp
+// b[d] = exp(i pi d^2 / L) is even, so both read the same value: M >= 2L - 2 is exact (one less
+// than the usual 2L - 1, which makes M = 2^17 for L = 65537 instead of 163840).
 uint64_t bluestein_length(uint64_t len) {
     if (len > (uint64_t(1) << 40)) throw std::invalid_argument("Bluestein convolution size overflows");
-    uint64_t m = 2 * len - 1;
+    uint64_t m = 2 * len - 2;
     while (!smooth7(m)) ++m;
     return m;
 }
@@ -1330,7 +1589,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
            << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"tma\":" << (ps.tma ? 1 : 0) << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster_pipe\":" << (ps.cluster_pipe ? 1 : 0) << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
-           << ps.cl_p << "]}";
+           << ps.cl_p << "],\"rader\":" << (ps.rader ? 1 : 0) << "}";
     }
     os << "]}";
     return os.str();

@@ -11,8 +11,11 @@
 //   * 7-smooth and larger            -> four-step: L = N1 * N2, column pass with the
 //                                       W_L^(n2*k1) twiddle fused into its store, then a
 //                                       row pass storing transposed (two passes);
+//   * prime, L-1 in the catalog      -> Rader: a cyclic convolution of length M = L-1
+//     (contiguous axis)                 over the permuted line (generator powers), one fused
+//                                       pass or three passes as below;
 //   * otherwise (Bluestein)          -> convolution of length M (the smallest 7-smooth
-//                                       M >= 2L-1): one fused pass when M fits a CTA,
+//                                       M >= 2L-2): one fused pass when M fits a CTA,
 //                                       else three passes over an M-padded scratch.
 // The normalization scale is fused into the store of the last pass.
 #pragma once
@@ -32,6 +35,7 @@ struct TableIds {
     int tw1 = -1, tw2 = -1, premul = -1, pointwise = -1, postmul = -1, tw4_hi = -1, tw4_lo = -1;
     int tc_tw = -1;  // two-level W_N^k table of the tensor-core kernel
     int cl_base = -1;  // base twiddles of the pipelined cluster kernel's 256-point FFTs
+    int perm_in = -1, perm_out = -1;  // Rader permutations (PlanSpec::index_tables)
 };
 
 struct KernelChoice {
@@ -64,6 +68,12 @@ struct PassSpec {
     int blue_id = -1;        // size-specialised Bluestein kernel (bluestein_catalog.h)
     int blue_kind = -1;      // its kind: kBlueFused / kBlueColsFwd / kBlueRowsConv / kBlueColsInv
     bool cluster_pipe = false;  // cluster pass on the pipelined 16-CTA kernel (cluster_pipe.cu)
+    // Rader pass (blue_id then names the catalog kernel whose Rader instantiation runs):
+    // gather / scatter through the permutation tables; rader_dc: the convolution pass that
+    // also stores X[0], reading x[0] from the axis input rader_src
+    bool rader = false;
+    bool rader_dc = false;
+    Buf rader_src = Buf::Input;
 };
 
 // One entry of cluster_catalog.h as seen by the host.
@@ -144,6 +154,8 @@ struct PlanRequest {
     // complex<double> 65536-point lines: the cluster pass (cluster_p = 16) on the pipelined
     // cluster kernel (opt-in)
     bool cluster_pipe = false;
+    // prime lengths L take Bluestein's convolution even where the catalog covers L - 1 (Rader)
+    bool no_rader = false;
 };
 
 // A Bluestein axis whose chirp and chirp spectrum the provider generates on the device
@@ -166,6 +178,7 @@ struct PlanSpec {
     // Entries of each table; a table whose data is empty but whose size is not is generated on
     // the device (Bluestein chirp and spectrum with PlanRequest::device_spectrum).
     std::vector<size_t> table_sizes;
+    std::vector<std::vector<int32_t>> index_tables;  // int32 tables (Rader permutations)
     std::vector<PassSpec> passes;
     uint64_t scratch_elements = 0;
 };
@@ -181,6 +194,9 @@ double normalization_scale(int mode, int direction, uint64_t transform_size);
 // Helpers exposed for tests.
 bool smooth7(uint64_t n);
 uint64_t bluestein_length(uint64_t len);
+bool is_prime(uint64_t n);
+uint64_t pow_mod(uint64_t b, uint64_t e, uint64_t m);
+uint64_t primitive_root(uint64_t p);  // p prime
 std::vector<int> choose_radices(int n, int maxv);
 int threads_per_line(int n, const std::vector<int>& radices, int maxv);
 std::string describe_plan(const PlanSpec& plan);  // JSON

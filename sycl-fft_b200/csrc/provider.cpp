@@ -166,6 +166,8 @@ FixedParams to_fixed(const PassParams& p) {
     f.conj_mid = p.conj_mid;
     f.flip_in = p.flip_in;
     f.flip_out = p.flip_out;
+    f.perm_in = static_cast<const int*>(p.perm_in);
+    f.perm_out = static_cast<const int*>(p.perm_out);
     return f;
 }
 
@@ -452,6 +454,8 @@ DevicePlan* create_plan(const syclfft_b200_plan_config_v1& cfg, uint32_t flags, 
     if (const char* k = std::getenv("SYCLFFT_B200_TMA")) req.use_tma = std::strcmp(k, "1") == 0;
     // SYCLFFT_B200_PIPED=0: never use the copy-engine-pipelined kernels.
     if (const char* k = std::getenv("SYCLFFT_B200_PIPED")) req.no_piped = std::strcmp(k, "0") == 0;
+    // SYCLFFT_B200_RADER=0: prime lengths keep Bluestein's convolution (tests, comparisons).
+    if (const char* k = std::getenv("SYCLFFT_B200_RADER")) req.no_rader = std::strcmp(k, "0") == 0;
     if (const char* k = std::getenv("SYCLFFT_B200_FUSED4_SINGLE")) req.fused_single = std::strcmp(k, "1") == 0;
     if (const char* k = std::getenv("SYCLFFT_B200_FUSED4")) {
         if (std::strcmp(k, "1") != 0) req.fused_single = false;
@@ -496,12 +500,17 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
     plan->spec.tuning = tuning;
     const size_t cs = req.dbl ? 16 : 8;
 
-    // All tables in one allocation, each 256-byte aligned.
-    std::vector<size_t> offsets(plan->spec.tables.size());
+    // All tables in one allocation, each 256-byte aligned: the complex tables (cast to the
+    // plan precision), then the int32 index tables.
+    std::vector<size_t> offsets(plan->spec.tables.size()), ioffsets(plan->spec.index_tables.size());
     size_t total = 0;
     for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
         offsets[i] = total;
         total += (plan->spec.table_sizes[i] * cs + 255) / 256 * 256;
+    }
+    for (size_t i = 0; i < plan->spec.index_tables.size(); ++i) {
+        ioffsets[i] = total;
+        total += (plan->spec.index_tables[i].size() * sizeof(int32_t) + 255) / 256 * 256;
     }
     const size_t table_bytes = std::max<size_t>(total, 256);
     cudaStream_t ms = memory_stream(device);
@@ -511,6 +520,10 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
     for (size_t i = 0; i < plan->spec.tables.size(); ++i) {
         if (req.dbl) pack_table<double>(plan->spec.tables[i], blob->data, offsets[i]);
         else pack_table<float>(plan->spec.tables[i], blob->data, offsets[i]);
+    }
+    for (size_t i = 0; i < plan->spec.index_tables.size(); ++i) {
+        const auto& t = plan->spec.index_tables[i];
+        if (!t.empty()) std::memcpy(static_cast<unsigned char*>(blob->data) + ioffsets[i], t.data(), t.size() * sizeof(int32_t));
     }
     cudaError_t up = cudaMallocAsync(&plan->table_mem, table_bytes, ms);
     if (up == cudaSuccess) up = cudaMemcpyAsync(plan->table_mem, blob->data, table_bytes, cudaMemcpyHostToDevice, ms);
@@ -573,6 +586,11 @@ DevicePlan* build_plan(PlanRequest req, int device, uint32_t flags, const std::s
         bp.p.postmul = tab(ps.tables.postmul);
         bp.p.tw4_hi = tab(ps.tables.tw4_hi);
         bp.p.tw4_lo = tab(ps.tables.tw4_lo);
+        auto itab = [&](int id) -> const void* {
+            return id < 0 ? nullptr : static_cast<const unsigned char*>(plan->table_mem) + ioffsets[id];
+        };
+        bp.p.perm_in = itab(ps.tables.perm_in);
+        bp.p.perm_out = itab(ps.tables.perm_out);
         bp.fp = to_fixed(bp.p);
         bp.cp = to_cluster(bp.p);
         if (ps.cluster_pipe) {
@@ -643,13 +661,13 @@ BoundPass rescale(const BoundPass& bp, uint64_t batch, uint64_t planned) {
 void apply_override(BoundPass& bp, bool first, bool last_pass, bool flip, double scale, bool set_scale) {
     bool last = last_pass;
     const PassSpec& ps = bp.spec_ref();
-    if (flip && first && ps.tables.premul >= 0) {
-        bp.p.flip_in ^= 1;  // conjugate before the chirp pre-multiply
+    if (flip && first && (ps.tables.premul >= 0 || ps.tables.perm_in >= 0)) {
+        bp.p.flip_in ^= 1;  // conjugate before the chirp pre-multiply (the Rader gather)
         bp.fp.flip_in ^= 1;
         first = false;
     }
-    if (flip && last && ps.tables.postmul >= 0) {
-        bp.p.flip_out ^= 1;  // conjugate after the chirp post-multiply
+    if (flip && last && (ps.tables.postmul >= 0 || ps.tables.perm_out >= 0)) {
+        bp.p.flip_out ^= 1;  // conjugate after the chirp post-multiply (the Rader scatter)
         bp.fp.flip_out ^= 1;
         last = false;
     }
@@ -1078,7 +1096,7 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
     const bool aligned = (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0);
     const PassSpec& ps = bp.spec_ref();
     if (ps.blue_id >= 0) {
-        check(launch_blue(ps.blue_id, plan->spec.req.dbl, ps.blue_kind, bp.fp, ps.threads,
+        check(launch_blue(ps.blue_id, plan->spec.req.dbl, ps.blue_kind, ps.rader, bp.fp, ps.threads,
                           static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
               "FFT Bluestein pass launch");
     } else if (ps.tc_id >= 0) {
@@ -1210,6 +1228,23 @@ void execute_plan(DevicePlan* plan, const void* in, void* out, cudaStream_t stre
                   "FFT fused Bluestein launch");
             i += 2;
             continue;
+        }
+        if (bp.spec_ref().rader_dc && i > 0 && i + 1 < np) {
+            // Rader convolution pass: X[0] of each line, from x[0] of the axis input, with the
+            // flips and scale that the column passes around it apply to the other outputs
+            BoundPass ba = rescale(plan->passes[i - 1], batch, planned);
+            BoundPass bc = rescale(plan->passes[i + 1], batch, planned);
+            if (flip || set_scale) {
+                apply_override(ba, i - 1 == 0, false, flip, scale, set_scale);
+                apply_override(bc, false, i + 2 == np, flip, scale, set_scale);
+            }
+            bp.fp.dc_x = buf(bp.spec_ref().rader_src);
+            bp.fp.dc_y = buf(bc.spec_ref().dst);
+            bp.fp.dc_x_pitch = ba.p.in.hi;
+            bp.fp.dc_y_pitch = bc.p.out.hi;
+            bp.fp.dc_scale = bc.fp.scale;
+            bp.fp.dc_flip_in = ba.fp.flip_in;
+            bp.fp.dc_flip_out = bc.fp.flip_out;
         }
         launch_bound_pass(plan, bp, buf(bp.spec_ref().src), buf(bp.spec_ref().dst), stream);
     }

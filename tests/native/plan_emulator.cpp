@@ -5,8 +5,9 @@
 // per tile line, load with zero-padding/pre-multiply/conjugation, the Stockham stage
 // sequence with the planner's twiddle tables, the point-wise multiply and second
 // FFT, and the store with conjugation, four-step twiddle, post-multiply, scale and
-// truncation. Used by tests/ to check plan decompositions (four-step, Bluestein,
-// strided axes) without a GPU. Never used by the product library.
+// truncation, the Rader gather, bin-0 term and scatter. Used by tests/ to check plan
+// decompositions (four-step, Bluestein, Rader, strided axes) without a GPU. Never used by
+// the product library.
 #include <complex>
 #include <cstdlib>
 #include <cstring>
@@ -85,7 +86,16 @@ void run_cluster(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* ds
     }
 }
 
-void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) {
+// The bin-0 term of a Rader convolution pass (kFeatRaderDC): line starts of the axis input
+// and output, their pitch, and the scale of the outputs around it.
+struct RaderDC {
+    const cd* x = nullptr;
+    cd* y = nullptr;
+    int64_t x_pitch = 0, y_pitch = 0;
+    double scale = 1.0;
+};
+
+void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst, const RaderDC& dc = RaderDC()) {
     if (ps.cluster_id >= 0) {
         run_cluster(plan, ps, src, dst);
         return;
@@ -97,6 +107,9 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
     const auto* postmul = table(ps.tables.postmul);
     const auto* hi = table(ps.tables.tw4_hi);
     const auto* lo = table(ps.tables.tw4_lo);
+    auto itable = [&](int id) -> const std::vector<int32_t>* { return id < 0 ? nullptr : &plan.index_tables[id]; };
+    const auto* perm_in = itable(ps.tables.perm_in);
+    const auto* perm_out = itable(ps.tables.perm_out);
     // Read every tile line first so in-place passes behave like the kernel (a tile is read
     // before it is written, and tiles are disjoint).
     struct Line { int64_t o, c; std::vector<cd> v; };
@@ -111,7 +124,8 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
                 const int64_t g = int64_t(k) * p.g_k + sel;
                 cd a = 0.0;
                 if (g < p.in_len) {
-                    a = src[ib + int64_t(k) * p.in.ks];
+                    // Rader gather: element g of the line is x[perm_in[g]] (from the line start)
+                    a = perm_in ? src[ib - sel + (*perm_in)[g]] : src[ib + int64_t(k) * p.in.ks];
                     if (premul) a *= (*premul)[g];
                     if (p.conj_in) a = std::conj(a);
                 }
@@ -125,8 +139,19 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
                             : p.sel_mode == kSelColMod ? L.c % p.sel_d : 0;
         stockham(L.v, p.fft1, plan.tables[ps.tables.tw1], p.n, ps.tw_base);
         if (p.fft2.nstages > 0) {
+            cd x0 = 0.0;
+            if (ps.rader && sel == 0) {
+                // bin 0: X[0] = x[0] + sum of the gathered line; x[0] joins bin 0 of the product
+                const bool fused = perm_in != nullptr;
+                const int64_t line = fused ? L.c : L.c / p.sel_d;
+                const cd* xl = fused ? src + line_base(p.in, L.o, L.c) : dc.x + line * dc.x_pitch;
+                cd* yl = fused ? dst + line_base(p.out, L.o, L.c) : dc.y + line * dc.y_pitch;
+                x0 = xl[0];
+                yl[0] = (x0 + L.v[0]) * (fused ? p.scale : dc.scale);
+            }
             for (int k = 0; k < p.n; ++k) {
                 if (pointwise) L.v[k] *= (*pointwise)[k + sel * p.pw_stride];
+                if (k == 0) L.v[0] += x0;
                 if (p.conj_mid) L.v[k] = std::conj(L.v[k]);
             }
             stockham(L.v, p.fft2, plan.tables[ps.tables.tw2], p.n, ps.tw_base);
@@ -150,6 +175,10 @@ void run_pass(const PlanSpec& plan, const PassSpec& ps, const cd* src, cd* dst) 
                 // size-specialised row pass: flat row l stored transposed
                 const int64_t l = L.c, o = l / p.ts_rows;
                 dst[o * p.ts_line + (l - o * p.ts_rows) + int64_t(k) * p.ts_rows] = v;
+                continue;
+            }
+            if (perm_out) {
+                dst[ob - sel + (*perm_out)[g]] = v;  // Rader scatter
                 continue;
             }
             dst[ob + int64_t(k) * p.out.ks] = v;
@@ -182,6 +211,8 @@ extern "C" int emu_describe(int dbl, int dir, int norm, int in_place, unsigned r
         req.smem_limit = smem_limit;
         req.split_bf16 = split_bf16 != 0;
         req.device_spectrum = true;
+        const char* rd = std::getenv("SYCLFFT_B200_RADER");
+        req.no_rader = rd && std::strcmp(rd, "0") == 0;
         set_err(desc, desc_cap, describe_plan(make_plan(req)));
         return 0;
     } catch (const std::exception& e) {
@@ -209,19 +240,32 @@ int run_request(int dbl, int dir, int norm, int in_place, unsigned rank, const u
         // the provider's switch for fused four-step routing of lines that fit one block
         const char* fs = std::getenv("SYCLFFT_B200_FUSED4_SINGLE");
         req.fused_single = fs && std::strcmp(fs, "1") == 0;
+        // the provider's switch that keeps prime lengths on Bluestein's convolution
+        const char* rd = std::getenv("SYCLFFT_B200_RADER");
+        req.no_rader = rd && std::strcmp(rd, "0") == 0;
         PlanSpec plan = make_plan(req);
         set_err(desc, desc_cap, describe_plan(plan));
         const int64_t E = static_cast<int64_t>(plan.elements);
         std::vector<cd> input(E), output(E), scratch(plan.scratch_elements);
         for (int64_t i = 0; i < E; ++i) input[i] = cd(in[2 * i], in[2 * i + 1]);
         if (req.in_place) output = input;
-        for (const auto& ps : plan.passes) {
-            auto buf = [&](Buf b) -> cd* {
-                if (b == Buf::Input) return req.in_place ? output.data() : input.data();
-                if (b == Buf::Output) return output.data();
-                return scratch.data();
-            };
-            run_pass(plan, ps, buf(ps.src), buf(ps.dst));
+        auto buf = [&](Buf b) -> cd* {
+            if (b == Buf::Input) return req.in_place ? output.data() : input.data();
+            if (b == Buf::Output) return output.data();
+            return scratch.data();
+        };
+        for (size_t i = 0; i < plan.passes.size(); ++i) {
+            const PassSpec& ps = plan.passes[i];
+            RaderDC dc;
+            if (ps.rader_dc) {
+                // between the Rader column passes: their line pitches and the outputs' scale
+                dc.x = buf(ps.rader_src);
+                dc.y = output.data();
+                dc.x_pitch = plan.passes[i - 1].p.in.hi;
+                dc.y_pitch = plan.passes[i + 1].p.out.hi;
+                dc.scale = plan.passes[i + 1].p.scale;
+            }
+            run_pass(plan, ps, buf(ps.src), buf(ps.dst), dc);
         }
         for (int64_t i = 0; i < E; ++i) {
             out[2 * i] = output[i].real();
@@ -250,3 +294,6 @@ extern "C" int emu_run_skip(int dbl, int dir, int norm, int in_place, unsigned r
     return run_request(dbl, dir, norm, in_place, rank, shape, batch, 0, 0, skip_axes, in, out, desc, desc_cap, err,
                        cap);
 }
+
+// The generator the planner's Rader tables are built from.
+extern "C" uint64_t emu_primitive_root(uint64_t p) { return primitive_root(p); }

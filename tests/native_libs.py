@@ -78,3 +78,11 @@ def describe(shape, batch, direction=-1, norm=0, double=False, in_place=False, s
     if rc != 0:
         raise ValueError(err.value.decode())
     return json.loads(desc.value.decode())
+
+
+def primitive_root(p):
+    """The planner's primitive root mod the prime p (the generator of its Rader tables)."""
+    L = _load("libplan_emulator.so")
+    L.emu_primitive_root.restype = ctypes.c_uint64
+    L.emu_primitive_root.argtypes = [ctypes.c_uint64]
+    return int(L.emu_primitive_root(int(p)))

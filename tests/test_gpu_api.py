@@ -72,7 +72,10 @@ def test_scratch_size(sf, torch, monkeypatch):
     assert sf.plan_many_dft("double", [65536], 4, sf.direction.forward).scratch_size_bytes() == 0  # cluster kernel
     monkeypatch.delenv("SYCLFFT_B200_CLUSTER")
     assert sf.plan_many_dft("double", [65536, 3], 1, sf.direction.forward).scratch_size_bytes() >= 65536 * 3 * 16
-    assert sf.plan_many_dft("float", [65537], 2, sf.direction.forward).scratch_size_bytes() >= 2 * 131073 * 8
+    # Rader: the convolution of a prime length L runs over L - 1 (65536) points
+    assert sf.plan_many_dft("float", [65537], 2, sf.direction.forward).scratch_size_bytes() == 2 * 65536 * 8
+    # Bluestein: over M >= 2L - 2 (131072 for L = 65521)
+    assert sf.plan_many_dft("float", [65521], 2, sf.direction.forward).scratch_size_bytes() >= 2 * 131072 * 8
 
 
 def test_raw_c_abi(sf, torch):

@@ -379,8 +379,8 @@ def test_pipelined_cluster_kernel(sf, torch, in_place, monkeypatch):
         assert rel_l2(out, ref) <= spec_tol(n, True)
 
 
-@pytest.mark.parametrize("shape,batch,dbl", [([65536], 8, False), ([65536], 6, True), ([65537], 6, False),
-                                             ([65537], 5, True), ([4099], 6, True), ([24, 65536], 1, False),
+@pytest.mark.parametrize("shape,batch,dbl", [([65536], 8, False), ([65536], 6, True), ([65521], 6, False),
+                                             ([65521], 5, True), ([4099], 6, True), ([24, 65536], 1, False),
                                              ([13440], 7, False)],
                          ids=lambda v: str(v))
 def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, batch, dbl):
@@ -413,3 +413,52 @@ def test_fused_multipass_matches_separate_passes(sf, torch, monkeypatch, shape, 
             outs[(fused, d, nm)] = got
     for d, nm in ((-1, 0), (1, 2), (-1, 3)):
         assert rel_l2(outs[("1", d, nm)], outs[("0", d, nm)]) <= spec_tol(n, dbl)
+
+
+@pytest.mark.parametrize("shape,batch,dbl", [([257], 64, False), ([641], 9, True), ([12289], 8, False),
+                                             ([12289], 5, True), ([65537], 6, False), ([65537], 5, True),
+                                             ([5, 257], 3, False)],
+                         ids=lambda v: str(v))
+def test_rader_lengths(sf, torch, monkeypatch, shape, batch, dbl):
+    """Prime lengths whose L - 1 the catalog covers run Rader's algorithm (gather by generator
+    powers, length-(L-1) convolution with the x[0] term, scatter): against FP64 and against
+    the same plan on Bluestein's convolution (SYCLFFT_B200_RADER=0), in both directions and
+    with every normalization through execute_ex's overrides, in place, and on a sub-batch."""
+    import ctypes
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 17 + n, dt)
+    xi = torch.from_numpy(x).cuda()
+    outs = {}
+    for rader in ("1", "0"):
+        monkeypatch.setenv("SYCLFFT_B200_RADER", rader)
+        p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)
+        kinds = [q["kind"] for q in p.describe()["passes"]]
+        assert any(k.startswith("rader") for k in kinds) == (rader == "1"), kinds
+        for d, nm in ((-1, 0), (1, 2), (-1, 3), (1, 1)):
+            out = torch.empty_like(xi)
+            rc = p._lib.syclfft_b200_execute_ex(p._handle, xi.data_ptr(), out.data_ptr(), 0, d, nm,
+                                                torch.cuda.current_stream().cuda_stream, p._err, 1024)
+            assert rc == 0, p._err.value
+            torch.cuda.synchronize()
+            got = out.cpu().numpy()
+            assert rel_l2(got, fp64_fft(x, shape, batch, d, norm_scale(nm, d, n))) <= spec_tol(n, dbl), (rader, d, nm)
+            outs[(rader, d, nm)] = got
+    for d, nm in ((-1, 0), (1, 2), (-1, 3), (1, 1)):
+        assert rel_l2(outs[("1", d, nm)], outs[("0", d, nm)]) <= 2 * spec_tol(n, dbl)
+    monkeypatch.delenv("SYCLFFT_B200_RADER")
+    # in place, backward plan, orthogonal normalization
+    got, p = run(sf, torch, x, shape, batch, sf.direction.backward, norm=3, dbl=dbl, in_place=True)
+    assert any(q["kind"].startswith("rader") for q in p.describe()["passes"])
+    assert rel_l2(got, fp64_fft(x, shape, batch, 1, norm_scale(3, 1, n))) <= spec_tol(n, dbl)
+    # the first b lines of a plan made for the whole batch
+    p = sf.plan_many_dft("double" if dbl else "float", shape, batch, sf.direction.forward)
+    b = max(1, batch // 2)
+    out = torch.zeros_like(xi)
+    rc = p._lib.syclfft_b200_execute_ex(p._handle, xi.data_ptr(), out.data_ptr(), b, -1, 1,
+                                        torch.cuda.current_stream().cuda_stream, p._err, 1024)
+    assert rc == 0, p._err.value
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    assert rel_l2(got[:n * b], fp64_fft(x[:n * b], shape, b, -1, norm_scale(1, -1, n))) <= spec_tol(n, dbl)
+    assert not np.any(got[n * b:])  # lines past the sub-batch untouched

@@ -2,6 +2,8 @@
 register butterflies vs a direct DFT, and every plan decomposition (single pass,
 four-step, fused and three-pass Bluestein, strided axes, copy) run through the FP64
 pass emulator against numpy's FP64 FFT."""
+import os
+
 import numpy as np
 import pytest
 
@@ -50,9 +52,12 @@ def test_plan_kinds():
     assert [p["kind"] for p in d["passes"]][1:] == ["fourstep_cols", "fourstep_rows"]
     _, d = emulate(np.zeros(1009), [1009], 1, -1)
     assert [p["kind"] for p in d["passes"]] == ["bluestein_fused"]
-    _, d = emulate(np.zeros(65537), [65537], 1, -1)
+    _, d = emulate(np.zeros(65537), [65537], 1, -1)  # prime, 65536 = 256 x 256: Rader
+    assert [p["kind"] for p in d["passes"]] == ["rader_cols_fwd", "rader_rows_conv", "rader_cols_inv"]
+    assert d["scratch_elements"] == 65536
+    _, d = emulate(np.zeros(65539), [65539], 1, -1)  # prime, 65538 = 2 * 3 * 29 * 113: Bluestein
     assert [p["kind"] for p in d["passes"]] == ["bluestein_cols_fwd", "bluestein_rows_conv", "bluestein_cols_inv"]
-    assert d["scratch_elements"] >= 2 * 65537 - 1
+    assert d["scratch_elements"] >= 2 * 65539 - 2
 
 
 def test_in_place_emulated():
@@ -87,7 +92,7 @@ def test_split_precision_pass_selection():
 
 
 def test_bluestein_on_catalog_kernels():
-    """Contiguous Bluestein axes take the smallest catalog convolution length >= 2L - 1: one
+    """Contiguous Bluestein axes take the smallest catalog convolution length >= 2L - 2: one
     fused pass where it fits a CTA, else three passes over M = n1 * n2; strided axes and
     the generic-kernel switch keep the runtime-parameterised passes."""
     from native_libs import describe, emulate
@@ -98,9 +103,13 @@ def test_bluestein_on_catalog_kernels():
 
     assert kinds([1009]) == [("bluestein_fused", 2048, True)]
     assert kinds([4099]) == [("bluestein_fused", 10240, True)]
-    k = kinds([65537])
+    os.environ["SYCLFFT_B200_RADER"] = "0"  # 65537 is a Rader length; Bluestein on request
+    try:
+        k = kinds([65537])
+    finally:
+        del os.environ["SYCLFFT_B200_RADER"]
     assert [x[0] for x in k] == ["bluestein_cols_fwd", "bluestein_rows_conv", "bluestein_cols_inv"]
-    assert all(x[2] for x in k) and k[0][1] * k[1][1] >= 2 * 65537 - 1
+    assert all(x[2] for x in k) and k[0][1] * k[1][1] == 2 * 65537 - 2  # M = 2L - 2 = 2^17
     assert all(x[2] for x in kinds([4099], dbl=True))
     assert not any(x[2] for x in kinds([1009, 6]))           # strided prime axis: generic passes
     rng = np.random.default_rng(9)
@@ -110,6 +119,57 @@ def test_bluestein_on_catalog_kernels():
         out, _ = emulate(x, shape, 2, -1, norm=1, double=dbl)
         ref = np.fft.fft(x.reshape(2, n), axis=1).reshape(-1) / n
         assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-13
+
+
+@pytest.mark.parametrize("shape,batch,dbl,kinds", [
+    ([257], 3, False, ["rader_fused"]),
+    ([641], 2, True, ["rader_fused"]),
+    ([12289], 2, False, ["rader_fused"]),
+    ([12289], 2, True, ["rader_cols_fwd", "rader_rows_conv", "rader_cols_inv"]),
+    ([65537], 2, False, ["rader_cols_fwd", "rader_rows_conv", "rader_cols_inv"]),
+    ([65537], 1, True, ["rader_cols_fwd", "rader_rows_conv", "rader_cols_inv"]),
+    ([5, 257], 2, False, ["rader_fused", "single"]),
+    ([257, 6], 1, False, ["single", "generic_or_bluestein"]),
+    ([7681], 1, False, ["bluestein_fused"]),
+])
+def test_rader_plans_emulated(shape, batch, dbl, kinds, monkeypatch):
+    """Prime lengths L whose L - 1 the Bluestein catalog covers run Rader's algorithm on the
+    catalog kernels (gather through generator powers, length-(L-1) convolution with the x[0]
+    term at bin 0, scatter); the FP64 emulation of those passes is the DFT in both directions,
+    for every normalization, in place and out of place. Strided prime axes and primes whose
+    L - 1 is not a catalog length (7680 = 2^9 * 15) stay on Bluestein."""
+    from native_libs import describe
+    d = describe(shape, batch, double=dbl)
+    got = [p["kind"] for p in d["passes"]]
+    if kinds[-1] == "generic_or_bluestein":
+        assert got[0] == "single" and not any(k.startswith("rader") for k in got)
+    else:
+        assert got == kinds
+    assert all(p["rader"] == p["kind"].startswith("rader") for p in d["passes"])
+    n = int(np.prod(shape))
+    rng = np.random.default_rng(n + batch)
+    x = rng.standard_normal(n * batch) + 1j * rng.standard_normal(n * batch)
+    for direction, norm, ip in ((-1, 0, False), (1, 2, True), (-1, 3, True), (1, 1, False)):
+        out, _ = emulate(x, shape, batch, direction, norm=norm, double=dbl, in_place=ip)
+        ref = fp64_fft(x, shape, batch, direction, norm_scale(norm, direction, n))
+        assert rel_l2(out, ref) < 1e-13, (direction, norm, ip)
+    # the same plan on Bluestein's convolution agrees
+    monkeypatch.setenv("SYCLFFT_B200_RADER", "0")
+    out_b, d_b = emulate(x, shape, batch, -1, double=dbl)
+    assert not any(p["rader"] for p in d_b["passes"])
+    assert rel_l2(out_b, fp64_fft(x, shape, batch, -1, 1.0)) < 1e-13
+
+
+def test_primitive_roots():
+    """The generator the Rader tables are built from: its powers run through every residue."""
+    from native_libs import primitive_root
+    for p in (3, 5, 7, 257, 641, 12289, 65537, 786433):
+        g = primitive_root(p)
+        seen, v = set(), 1
+        for _ in range(p - 1):
+            seen.add(v)
+            v = v * g % p
+        assert len(seen) == p - 1 and v == 1, p
 
 
 def test_fused_single_routes_13440_through_a_catalogued_split(monkeypatch):

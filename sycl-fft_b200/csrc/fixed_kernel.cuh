@@ -101,6 +101,17 @@ enum : int {
     kFeatRaderDC = 65536, // Rader: X[0] and the x[0] term at bin 0 of the convolution pass
 };
 
+// 4-byte global -> shared copy that completes asynchronously (cp.async), and its wait.
+__device__ __forceinline__ void cp_async4(int* dst, const int* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_all;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_commit_only() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
 template <int FEAT, class C>
 __device__ __forceinline__ C fixed_load(const C* p) {
     if constexpr (FEAT & kFeatLoadCG) return __ldcg(p);
@@ -148,6 +159,8 @@ struct FixedCtx {
     const int *perm_in, *perm_out;  // Rader permutations
     const C* gline;                  // start of this thread's input line (kFeatGather)
     C* gline_out;                    // start of its output line (kFeatScatter)
+    const int* sidx;                 // kModeC kFeatScatter: this column's perm_out entries in
+                                     // shared memory (element k at sidx[k * W])
     const C* rx;                     // x line and y line of the bin-0 term (kFeatRaderDC)
     C* ry;
     T dc_scale;
@@ -200,13 +213,19 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                     v[i * R + r] = a;
                 }
             } else if constexpr (FIRST && (FEAT & kFeatGather)) {
+                // all of this butterfly's indices first, then all its gathers: the two
+                // dependent loads cost one round trip each instead of one per element
+                int src[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r) {
-                    const int k = j + r * NR;
-                    const int g = k * X.g_k + X.sel;
+                    const int g = (j + r * NR) * X.g_k + X.sel;
+                    src[r] = X.line_ok && g < X.in_len ? __ldg(X.perm_in + g) : -1;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
                     C a = cmake<C>(T(0), T(0));
-                    if (X.line_ok && g < X.in_len) {
-                        a = X.gline[__ldg(X.perm_in + g)];
+                    if (src[r] >= 0) {
+                        a = X.gline[src[r]];
                         if (X.flip_in) a.y = -a.y;
                         if (X.conj_in) a.y = -a.y;
                     }
@@ -254,6 +273,11 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                 for (int r = 0; r < R; ++r) v[i * R + r] = X.sm[pidx<T>(j + r * NR)];
             }
         }
+    }
+    if constexpr (LAST && MODEC && (FEAT & kFeatScatter)) {
+        // the scatter indices this thread's copies brought to shared memory (kernel start)
+        cp_async_commit_wait_all();
+        if constexpr (FIRST) __syncthreads();
     }
     if constexpr (!FIRST || (FEAT & kFeatSmemIn)) __syncthreads();
 #pragma unroll
@@ -335,9 +359,10 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                         if constexpr (FEAT & (kFeatPostmul | kFeatScatter)) {
                             if (X.flip_out) a.y = -a.y;
                         }
-                        C* dst = (FEAT & kFeatScatter) ? X.gline_out + __ldg(X.perm_out + g)
-                                 : MODEC               ? X.gout + (int64_t)k * X.out_ks
-                                                       : X.gout + k;
+                        C* dst;
+                        if constexpr ((FEAT & kFeatScatter) && MODEC) dst = X.gline_out + X.sidx[k * W];
+                        else if constexpr (FEAT & kFeatScatter) dst = X.gline_out + __ldg(X.perm_out + g);
+                        else dst = MODEC ? X.gout + (int64_t)k * X.out_ks : X.gout + k;
                         if constexpr (FEAT & kFeatStoreCS) __stcs(dst, a);
                         else *dst = a;
                     }
@@ -418,6 +443,19 @@ __global__ void __launch_bounds__(MAXT, fixed_min_blocks<T, MAXT, REGS>())
         X.gline_out = out + o * P.out_hi;
         X.in_ks = P.in_ks;
         X.out_ks = P.out_ks;
+        if constexpr (FEAT & kFeatScatter) {
+            // the tile's scatter indices perm_out[k * g_k + c] (the planner adds N * W ints of
+            // shared memory after the tile) fetched asynchronously while the stages run
+            int* sidx = reinterpret_cast<int*>(sm + N * W);
+            const int64_t c0 = (tile - o * P.col_tiles) * W;
+            for (int e = tid; e < N * W; e += blockDim.x) {
+                const int k = e / W;
+                const int64_t cc = c0 + (e - k * W);
+                if (cc < P.n_cols) cp_async4(sidx + e, P.perm_out + (int64_t)k * P.g_k + cc);
+            }
+            cp_async_commit_only();
+            X.sidx = sidx + w;
+        }
     } else {
         const int w = tid / TPL;
         X.t = tid - w * TPL;

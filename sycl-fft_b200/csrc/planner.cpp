@@ -670,6 +670,7 @@ struct Builder {
         c.p.conj_in = 1;
         c.p.conj_out = 1;
         c.tables.perm_out = pout_id;
+        c.smem_bytes += static_cast<int64_t>(ci->w) * n1 * static_cast<int64_t>(sizeof(int32_t));  // scatter indices
         c.src = Buf::Scratch;
         c.dst = Buf::Output;
         c.bytes_moved = (O * M + E) * cs;

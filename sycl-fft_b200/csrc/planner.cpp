@@ -253,6 +253,15 @@ struct Builder {
     }
 
     // Fill launch geometry for a pass whose FFT length is p.n and mode is set.
+    // Lines per CTA of a runtime-parameterised four-step pass: about 256 threads (several CTAs
+    // per SM; CTAs of ~1000 threads leave one per SM, every stage barrier then stalls the SM),
+    // at least 4 lines (32-byte segments) and at most `cap`, a power of two.
+    static int fourstep_w(int tpl, int cap) {
+        int w = std::max(4, std::min(cap, 256 / std::max(1, tpl)));
+        while (w & (w - 1)) w &= w - 1;
+        return w;
+    }
+
     void geometry(PassSpec& ps, const SingleCfg& cfg, int want_w) {
         PassParams& p = ps.p;
         p.tpl = cfg.tpl;
@@ -984,7 +993,7 @@ struct Builder {
                 SingleCfg cfg = single_cfg(n1, req.dbl, req.force_maxv);
                 set_fft(a, p.fft1, &a.tables.tw1, p.n, cfg);
                 add_tw4(a, L, -1);
-                geometry(a, cfg, 0);
+                geometry(a, cfg, s == 1 ? fourstep_w(cfg.tpl, req.dbl ? 8 : 16) : 0);
                 if (s == 1) try_fixed_fourstep(a, kFixedTw4);
                 a.src = cur;
                 a.dst = Buf::Scratch;
@@ -1014,7 +1023,7 @@ struct Builder {
                 SingleCfg cfg = single_cfg(n2, req.dbl, req.force_maxv);
                 set_fft(b, p.fft1, &b.tables.tw1, p.n, cfg);
                 // rows per CTA: enough for 128-byte segments of the transposed store
-                geometry(b, cfg, s == 1 ? std::max(1, 128 / cs) : 0);
+                geometry(b, cfg, s == 1 ? fourstep_w(cfg.tpl, std::max(1, 128 / cs)) : 0);
                 if (s == 1) try_fixed_fourstep(b, kFixedTStore, n1, L);
                 b.src = Buf::Scratch;
                 b.dst = Buf::Output;

@@ -15,10 +15,17 @@ from __future__ import annotations
 import ctypes
 import enum
 import json
+import sys
 import threading
+import weakref
 from dataclasses import dataclass
 
 from . import _provider
+
+try:  # CPython fast call into the provider's execute entry (csrc/fastcall.c); ctypes otherwise
+    from . import _fastcall
+except ImportError:  # pragma: no cover - the Makefile builds it beside this file
+    _fastcall = None
 
 
 class direction(enum.IntEnum):
@@ -144,6 +151,7 @@ def _torch():
 
 
 _EVENT_CLS = None
+_EVENT_BASE_RECORD = None
 
 
 def _event_class():
@@ -182,7 +190,28 @@ def _event_class():
                                            "this execution is incomplete")
 
         _EVENT_CLS = ExecutionEvent
+        global _EVENT_BASE_RECORD
+        _EVENT_BASE_RECORD = torch._C._CudaEventBase.record  # record(event, stream), no current-stream lookup
     return _EVENT_CLS
+
+
+_STREAMS = {}  # (device, raw cudaStream_t) -> torch.cuda.Stream: events are recorded through these
+
+
+def _stream_object(torch, handle, device, given=None):
+    """A torch.cuda.Stream for the raw stream `handle` of `device` (cached: building one from
+    the current-stream query costs more than the rest of a small execute)."""
+    key = (device, handle)
+    s = _STREAMS.get(key)
+    if s is None:
+        s = given
+        if s is None:
+            cur = torch.cuda.current_stream(device)
+            s = cur if cur.cuda_stream == handle else torch.cuda.ExternalStream(handle, device=device)
+        if len(_STREAMS) > 256:
+            _STREAMS.clear()
+        _STREAMS[key] = s
+    return s
 
 
 def _host_tensor(t):
@@ -328,6 +357,25 @@ class Plan:
         self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
         self._execute = self._api.execute
+        self._bind_fast_path()
+
+    def _bind_fast_path(self):
+        self._checked = {}  # name -> (weak tensor, data_ptr, numel) of the last validated buffer
+        self._events = []   # ExecutionEvents this plan may record again once nobody holds them
+        self._exec_addr = ctypes.cast(self._execute, ctypes.c_void_p).value
+        self._err_addr = ctypes.addressof(self._err)
+
+    def _event(self, capturing):
+        """An ExecutionEvent to record: one of this plan's earlier events that nothing outside
+        the plan references any more (re-recording it is then unobservable), else a new one."""
+        if not capturing:
+            for e in self._events:
+                if sys.getrefcount(e) <= 3:  # the list, the loop variable and the argument
+                    return e
+        ev = (_EVENT_CLS or _event_class())(self._lib, (self,))
+        if not capturing and len(self._events) < 4:
+            self._events.append(ev)
+        return ev
 
     # -- properties (syclfft.hpp:62-66) --
     def shape(self):
@@ -365,6 +413,18 @@ class Plan:
 
     # -- execution (sycl.cpp:615-641, 818-874) --
     def _pointer(self, t, name):
+        # the buffer validated last time, unchanged: same tensor object, storage and size
+        c = self._checked.get(name)
+        if c is not None and c[0]() is t:
+            ptr = t.data_ptr()
+            if ptr == c[1] and t.numel() == c[2] and t.is_contiguous():
+                return ptr
+        ptr = self._validate_pointer(t, name)
+        if not isinstance(t, int):
+            self._checked[name] = (weakref.ref(t), ptr, t.numel())
+        return ptr
+
+    def _validate_pointer(self, t, name):
         torch = _torch()
         if t is None:
             raise SyclfftError(error_code.invalid_pointer, f"{name} must be non-null")
@@ -421,28 +481,45 @@ class Plan:
         if pl == placement.out_of_place and inp == out:
             raise SyclfftError(error_code.invalid_argument, "Out-of-place plan requires distinct allocations")
         torch = _torch()
-        current = torch.cuda.current_stream(self._device)
-        s = stream or current
-        with self._lock:
+        dev = self._device
+        tc = torch._C
+        if stream is None and tc._cuda_getDevice() == dev:
+            # the current stream of the current device: its raw handle and capture state
+            # without building a Stream object
+            s = None
+            handle = tc._cuda_getCurrentRawStream(dev)
+            capturing = tc._cuda_isCurrentStreamCapturing()
+        else:
+            current = torch.cuda.current_stream(dev)
+            s = stream or current
+            handle = s.cuda_stream
             if s is current or s == current:
-                capturing = torch.cuda.is_current_stream_capturing()
+                with torch.cuda.device(dev):
+                    capturing = torch.cuda.is_current_stream_capturing()
             else:
                 with torch.cuda.stream(s):
                     capturing = torch.cuda.is_current_stream_capturing()
+        with self._lock:
             for dep in dependencies or ():
+                s = s or _stream_object(torch, handle, dev)
                 s.wait_event(dep)
-            handle = s.cuda_stream
             if self._last_event is not None and not capturing and self._last_stream != handle:
                 # A graph cannot depend on work outside its capture; captured launches run
                 # only at replay, which the caller orders against earlier executes. On the
                 # stream of the previous execute, stream order already serialises them.
+                s = s or _stream_object(torch, handle, dev)
                 s.wait_event(self._last_event)
             err = self._err
             # the provider writes the error buffer only on failure (a non-zero return)
-            if self._execute(self._handle, inp, out, handle, err, _provider.ERR_CAP) != 0:
+            if _fastcall is not None:
+                rc = _fastcall.execute(self._exec_addr, self._handle, inp, out, handle, self._err_addr,
+                                       _provider.ERR_CAP)
+            else:
+                rc = self._execute(self._handle, inp, out, handle, err, _provider.ERR_CAP)
+            if rc != 0:
                 raise SyclfftError(error_code.execution_failed, err.value.decode() or "execution failed")
-            ev = (_EVENT_CLS or _event_class())(self._lib, (self,))
-            ev.record(s)
+            ev = self._event(capturing)
+            _EVENT_BASE_RECORD(ev, _stream_object(torch, handle, dev, s))
             # an event recorded inside a capture belongs to the graph: ordering of replays
             # against later executes is the caller's, as for any captured work
             self._last_event = None if capturing else ev
@@ -533,6 +610,7 @@ class RealPlan(Plan):
         self._last_stream = None
         self._err = ctypes.create_string_buffer(_provider.ERR_CAP)
         self._execute = self._api.execute
+        self._bind_fast_path()
 
     @property
     def kind(self):

@@ -86,8 +86,15 @@ SYCLFFT_B200_EXPORT void* syclfft_b200_family_create(uint32_t scalar, int32_t de
             }
         }
         if (f->device != prev) check(cudaSetDevice(f->device), "cudaSetDevice");
+        // The copy is waited for on a stream of its own: a synchronous cudaMemcpy from pageable
+        // memory can return before its DMA reaches the device, and the launches that read these
+        // tables run on non-blocking streams, which are not ordered after it.
         cudaError_t e = cudaMalloc(&f->tw, blob.size());
-        if (e == cudaSuccess) e = cudaMemcpy(f->tw, blob.data(), blob.size(), cudaMemcpyHostToDevice);
+        cudaStream_t up = nullptr;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(f->tw, blob.data(), blob.size(), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(up);
+        if (up) cudaStreamDestroy(up);
         if (f->device != prev) cudaSetDevice(prev);
         check(e, "family tables");
         return f.release();

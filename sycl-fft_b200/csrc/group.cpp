@@ -97,8 +97,15 @@ SYCLFFT_B200_EXPORT void* syclfft_b200_group_create(uint32_t scalar, uint64_t n,
             ns *= R;
         }
         if (blob.empty()) blob.resize(16, 0);
+        // The copy is waited for on a stream of its own: a synchronous cudaMemcpy from pageable
+        // memory can return before its DMA reaches the device, and the launches that read these
+        // tables run on non-blocking streams, which are not ordered after it.
         cudaError_t e = cudaMalloc(&g->tw, blob.size());
-        if (e == cudaSuccess) e = cudaMemcpy(g->tw, blob.data(), blob.size(), cudaMemcpyHostToDevice);
+        cudaStream_t up = nullptr;
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(g->tw, blob.data(), blob.size(), cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(up);
+        if (up) cudaStreamDestroy(up);
         if (g->device != prev) cudaSetDevice(prev);
         check(e, "group tables");
         return g.release();

@@ -1546,6 +1546,42 @@ const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
     return nullptr;
 }
 
+// Runtime-length passes whose layout the contiguous kernel (lean_kernel.cuh) covers: whole
+// contiguous lines, or the column / row pass of a contiguous four-step, with no table,
+// padding or second FFT, at least two stages in the radix order 16, 8, 4, 2, 3, 5, 7 and a
+// power-of-two tile width. Values of lean_feat: 0 plain, 1 four-step twiddle, 2 transposed store.
+static void mark_lean(PassSpec& ps) {
+    const PassParams& p = ps.p;
+    if (ps.fixed_id >= 0 || ps.cluster_id >= 0 || ps.piped_id >= 0 || ps.tc_id >= 0 || ps.blue_id >= 0 || ps.rader ||
+        ps.cluster_pipe || ps.tw_base)
+        return;
+    if (p.fft2.nstages > 0 || p.fft1.nstages < 2 || ps.tables.premul >= 0 || ps.tables.postmul >= 0 ||
+        ps.tables.pointwise >= 0 || ps.tables.perm_in >= 0 || ps.tables.perm_out >= 0)
+        return;
+    if (p.in.d != 1 || p.out.d != 1 || p.flip_in || p.flip_out || p.w < 1 || (p.w & (p.w - 1)) != 0) return;
+    static const int order[] = {16, 8, 4, 2, 3, 5, 7};
+    int pos = 0;
+    for (int s = 0; s < p.fft1.nstages; ++s) {
+        while (pos < 7 && order[pos] != p.fft1.radix[s]) ++pos;
+        if (pos == 7) return;  // a radix outside the order, or out of order
+    }
+    const int64_t n = p.n;
+    if (p.mode == kModeK && !p.store_via_smem && p.tw4_sign == 0 && p.sel_mode == kSelNone && p.g_k == 1 &&
+        p.in.ks == 1 && p.out.ks == 1 && p.in_len >= n && p.out_len >= n) {
+        ps.lean = true;
+        ps.lean_feat = 0;
+    } else if (p.mode == kModeC && !p.store_via_smem && p.tw4_sign != 0 && p.sel_mode == kSelCol &&
+               p.in.cs == 1 && p.out.cs == 1 && p.g_k == p.n_cols && p.in_len >= n * p.g_k && p.out_len >= n * p.g_k &&
+               n * p.g_k <= (int64_t(1) << 30)) {
+        ps.lean = true;
+        ps.lean_feat = 1;
+    } else if (p.mode == kModeK && p.store_via_smem && p.tw4_sign == 0 && p.sel_mode == kSelNone && p.g_k == 1 &&
+               p.in.ks == 1 && p.out.cs == 1 && p.in_len >= n && p.out_len >= n) {
+        ps.lean = true;
+        ps.lean_feat = 2;
+    }
+}
+
 PlanSpec make_plan(const PlanRequest& req) {
     if (req.direction != -1 && req.direction != 1) throw std::invalid_argument("Invalid FFT direction");
     if (req.normalization < 0 || req.normalization > 3) throw std::invalid_argument("Invalid normalization");
@@ -1570,6 +1606,7 @@ PlanSpec make_plan(const PlanRequest& req) {
     }
     if (plan.passes.empty()) b.copy_pass(cur);
     plan.passes.back().p.scale = plan.scale;
+    for (auto& ps : plan.passes) mark_lean(ps);
     // The batch is the outermost index of every pass: the pass's outer count when it has
     // one (n_outer > 1 or strided columns), else its line count.
     for (auto& ps : plan.passes) {
@@ -1599,7 +1636,7 @@ std::string describe_plan(const PlanSpec& plan) {
            << ",\"dst\":" << int(ps.dst) << ",\"bytes\":" << ps.bytes_moved
            << ",\"store_via_smem\":" << p.store_via_smem << ",\"fixed_id\":" << ps.fixed_id
            << ",\"piped_id\":" << ps.piped_id << ",\"tc_id\":" << ps.tc_id << ",\"blue_id\":" << ps.blue_id << ",\"tma\":" << (ps.tma ? 1 : 0) << ",\"cluster_id\":" << ps.cluster_id << ",\"cluster_pipe\":" << (ps.cluster_pipe ? 1 : 0) << ",\"cluster\":[" << ps.cl_n1 << "," << ps.cl_n2 << ","
-           << ps.cl_p << "],\"rader\":" << (ps.rader ? 1 : 0) << "}";
+           << ps.cl_p << "],\"rader\":" << (ps.rader ? 1 : 0) << ",\"lean\":" << (ps.lean ? 1 : 0) << "}";
     }
     os << "]}";
     return os.str();

@@ -74,6 +74,10 @@ struct PassSpec {
     bool rader = false;
     bool rader_dc = false;
     Buf rader_src = Buf::Input;
+    // runtime-length pass on the contiguous-layout kernel (lean_kernel.cuh) instead of the
+    // general one; lean_feat: kLeanPlain / kLeanTw4 / kLeanTStore
+    bool lean = false;
+    int lean_feat = 0;
 };
 
 // One entry of cluster_catalog.h as seen by the host.

@@ -26,6 +26,7 @@
 #include "cluster_launch.hpp"
 #include "fixed_launch.hpp"
 #include "launch.hpp"
+#include "lean_launch.hpp"
 #include "piped_launch.hpp"
 #include "tc_launch.hpp"
 #include "tma_launch.hpp"
@@ -1091,6 +1092,54 @@ bool launch_tma(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cud
     return true;
 }
 
+// Parameters of the contiguous runtime-length kernel for a bound pass (after its batch and
+// direction / normalization overrides): the pass's geometry, the stage sequence with a
+// multiply-shift quotient per stage (exact for the butterfly indices, j < 2^31), and the
+// four-step twiddle.
+LeanParams to_lean(const PassParams& p) {
+    LeanParams L;
+    L.n = p.n;
+    L.tpl = p.tpl;
+    L.w = p.w;
+    while ((1 << L.w_shift) < p.w) ++L.w_shift;
+    L.pitch = p.pitch;
+    L.pad_shift = p.pad_shift;
+    L.nstages = p.fft1.nstages;
+    for (int s = 0; s < L.nstages; ++s) {
+        L.radix[s] = p.fft1.radix[s];
+        L.ns[s] = p.fft1.ns[s];
+        L.tw_off[s] = p.fft1.tw_off[s];
+        const uint32_t d = static_cast<uint32_t>(p.fft1.ns[s]);
+        int l = 0;
+        while ((uint64_t(2) << l) <= d) ++l;  // floor(log2 d)
+        if ((d & (d - 1)) == 0) {
+            L.ns_magic[s] = 0;
+            L.ns_shift[s] = l;
+        } else {
+            // ceil(2^(32+l) / d) < 2^32: floor(j * m / 2^(32+l)) = floor(j / d) for j < 2^31
+            L.ns_magic[s] = static_cast<uint32_t>(((uint64_t(1) << (32 + l)) + d - 1) / d);
+            L.ns_shift[s] = l;
+        }
+    }
+    L.tw = p.fft1.tw;
+    L.n_cols = p.n_cols;
+    L.col_tiles = p.col_tiles;
+    L.in_hi = p.in.hi;
+    L.in_cs = p.in.cs;
+    L.out_hi = p.out.hi;
+    L.out_cs = p.out.cs;
+    L.in_ks = static_cast<int>(p.in.ks);
+    L.out_ks = static_cast<int>(p.out.ks);
+    L.conj_in = p.conj_in;
+    L.conj_out = p.conj_out;
+    L.scale = p.scale;
+    L.tw4_hi = p.tw4_hi;
+    L.tw4_lo = p.tw4_lo;
+    L.tw4_shift = p.tw4_shift;
+    L.tw4_conj = p.tw4_sign > 0 ? 1 : 0;
+    return L;
+}
+
 // Launches one bound pass of a plan on its kernel family.
 void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* dst, cudaStream_t stream) {
     const bool aligned = (reinterpret_cast<uintptr_t>(src) % 16 == 0) && (reinterpret_cast<uintptr_t>(dst) % 16 == 0);
@@ -1114,6 +1163,10 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
     } else if (ps.fixed_id >= 0) {
         check(launch_fixed(ps.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, ps.threads,
                            static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
+              "FFT pass launch");
+    } else if (ps.lean && has_lean_variant(plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt)) {
+        check(launch_lean(to_lean(bp.p), plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt, bp.p.mode == kModeC, ps.lean_feat,
+                          ps.threads, static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
               "FFT pass launch");
     } else {
         check(launch_pass(bp.p, plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt, ps.threads, static_cast<size_t>(ps.smem_bytes),

@@ -189,3 +189,23 @@ def test_fused_single_routes_13440_through_a_catalogued_split(monkeypatch):
                                                                     ("fourstep_rows", [8, 15])]
     ref = np.fft.fft(x.reshape(b, n), axis=1).reshape(-1)
     assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-14
+
+
+def test_lean_passes_marked():
+    """Runtime-length passes over contiguous lines (whole lines, and the column and row passes of
+    a contiguous four-step) run on the lean kernel; strided axes, size-specialised, Bluestein and
+    single-stage passes do not. The lean kernel has the general kernel's semantics, so the FP64
+    emulation of these plans (the SHAPES cases above) covers them."""
+    from native_libs import describe
+
+    def lean(shape, dbl=False):
+        return [(p["kind"], p["lean"]) for p in describe(shape, 4, double=dbl)["passes"]]
+
+    assert lean([3000]) == [("single", 1)]
+    assert lean([680400]) == [("fourstep_cols", 1), ("fourstep_rows", 1)]
+    assert lean([784000], True) == [("fourstep_cols", 1), ("fourstep_rows", 1)]
+    assert lean([3000, 6]) == [("single", 1), ("single", 0)]  # the strided axis stays general
+    assert lean([4096]) == [("single", 0)]                     # size-specialised
+    assert lean([1009]) == [("bluestein_fused", 0)]
+    for p in describe([680400], 4)["passes"]:
+        assert p["w"] & (p["w"] - 1) == 0 and len(p["radices"]) >= 2

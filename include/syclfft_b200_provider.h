@@ -253,6 +253,36 @@ SYCLFFT_B200_EXPORT int syclfft_b200_family_execute(void *family, const syclfft_
                                                     uint32_t count, void *stream, char *err, size_t cap);
 SYCLFFT_B200_EXPORT void syclfft_b200_family_destroy(void *family);
 
+/* ---- Serving helpers (no reference counterpart): one call per admission round. ----
+ *
+ * syclfft_b200_execute_many runs `count` executes on `stream` in order, each like
+ * syclfft_b200_execute_ex (plan, buffers, batch 0 = the plan's, direction 0 = the plan's,
+ * normalization -1 = the plan's); it stops at the first failure and names its index in err.
+ * syclfft_b200_fill_uniform writes `count` reals uniform in [-1, 1) into each item's buffer,
+ * value i a function of (seed, i) only (SplitMix64 output function), in one launch per 256
+ * items. Both return 0, or write err and return non-zero. */
+typedef struct syclfft_b200_exec_item_v1 {
+    void *plan;
+    const void *in;
+    void *out;
+    uint64_t batch;
+    int32_t direction;
+    int32_t normalization;
+} syclfft_b200_exec_item_v1;
+
+typedef struct syclfft_b200_fill_item_v1 {
+    void *data;
+    uint64_t count;  /* reals */
+    uint64_t seed;
+    uint32_t scalar; /* SYCLFFT_B200_SCALAR_FLOAT / _DOUBLE */
+    uint32_t reserved;
+} syclfft_b200_fill_item_v1;
+
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_many(const syclfft_b200_exec_item_v1 *items, uint32_t count, void *stream,
+                                                  char *err, size_t cap);
+SYCLFFT_B200_EXPORT int syclfft_b200_fill_uniform(const syclfft_b200_fill_item_v1 *items, uint32_t count,
+                                                  void *stream, char *err, size_t cap);
+
 /* ---- Transform without device allocation (no counterpart in the reference). ----
  *
  * For callers that cannot allocate device memory at the point they need a transform:

@@ -1801,6 +1801,28 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void* plan, const void* in, void
     }
 }
 
+SYCLFFT_B200_EXPORT int syclfft_b200_execute_many(const syclfft_b200_exec_item_v1* items, uint32_t count, void* stream,
+                                                  char* err, size_t cap) {
+    if (count && !items) {
+        sfb::set_error(err, cap, "execute items must be non-null");
+        return 1;
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        const syclfft_b200_exec_item_v1& it = items[i];
+        try {
+            if (it.direction != 0 && it.direction != -1 && it.direction != 1)
+                throw std::invalid_argument("Invalid FFT direction");
+            if (it.normalization > 3) throw std::invalid_argument("Invalid normalization");
+            sfb::execute_plan(static_cast<sfb::DevicePlan*>(it.plan), it.in, it.out, static_cast<cudaStream_t>(stream),
+                              it.batch, it.direction, it.normalization);
+        } catch (const std::exception& e) {
+            sfb::set_error(err, cap, "execute item " + std::to_string(i) + ": " + e.what());
+            return 1;
+        }
+    }
+    return 0;
+}
+
 namespace sfb {
 namespace {
 // Every plan of a plan tree (a real or strided plan holds its complex plans in inner / outer).

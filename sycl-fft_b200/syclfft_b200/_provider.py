@@ -79,6 +79,27 @@ class FamilyItemV1(ctypes.Structure):
     ]
 
 
+class ExecItemV1(ctypes.Structure):
+    _fields_ = [
+        ("plan", ctypes.c_void_p),
+        ("in_", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("batch", ctypes.c_uint64),
+        ("direction", ctypes.c_int32),
+        ("normalization", ctypes.c_int32),
+    ]
+
+
+class FillItemV1(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("count", ctypes.c_uint64),
+        ("seed", ctypes.c_uint64),
+        ("scalar", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
 class HostStageV1(ctypes.Structure):
     _fields_ = [
         ("plan", ctypes.c_void_p),
@@ -121,6 +142,8 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_family_supports",
     "syclfft_b200_family_create",
     "syclfft_b200_family_execute",
+    "syclfft_b200_execute_many",
+    "syclfft_b200_fill_uniform",
     "syclfft_b200_family_destroy",
     "syclfft_b200_create_real",
     "syclfft_b200_create_strided",
@@ -183,6 +206,12 @@ def load(path: str | None = None):
     lib.syclfft_b200_family_execute.restype = ctypes.c_int
     lib.syclfft_b200_family_execute.argtypes = [ctypes.c_void_p, ctypes.POINTER(FamilyItemV1), ctypes.c_uint32,
                                                 ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_execute_many.restype = ctypes.c_int
+    lib.syclfft_b200_execute_many.argtypes = [ctypes.POINTER(ExecItemV1), ctypes.c_uint32, ctypes.c_void_p,
+                                              ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_fill_uniform.restype = ctypes.c_int
+    lib.syclfft_b200_fill_uniform.argtypes = [ctypes.POINTER(FillItemV1), ctypes.c_uint32, ctypes.c_void_p,
+                                              ctypes.c_char_p, ctypes.c_size_t]
     lib.syclfft_b200_family_destroy.restype = None
     lib.syclfft_b200_family_destroy.argtypes = [ctypes.c_void_p]
     lib.syclfft_b200_group_destroy.restype = None

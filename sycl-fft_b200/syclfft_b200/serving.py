@@ -46,7 +46,9 @@ class Request:
     # filled while serving
     nbytes: int = 0
     t_done: float = 0.0
-    inp: object = None
+    in_ptr: int = 0   # device addresses of the request's input and output in the arena
+    out_ptr: int = 0
+    inp: object = None  # tensor views of them, made only when asked for (keep_results)
     out: object = None
     result: object = None
 
@@ -144,16 +146,39 @@ class Arena:
         return self.t[off: off + nbytes].view(dtype)
 
 
-def synthetic_input(r: Request, out=None, generator=None):
-    """The request's input: 2 * elements reals uniform in [-1, 1) from its seed, viewed as
-    complex (written into `out` when given, on the current stream)."""
+def _fill_items(reqs, lib=None):
+    """FillItemV1 array of the requests' inputs (2 * elements reals each, at r.in_ptr)."""
+    items = (_provider.FillItemV1 * len(reqs))()
+    for i, r in enumerate(reqs):
+        items[i].data = r.in_ptr
+        items[i].count = 2 * r.elements
+        items[i].seed = r.seed
+        items[i].scalar = _provider.SCALAR_DOUBLE if r.double else _provider.SCALAR_FLOAT
+    return items
+
+
+def fill_inputs(reqs, stream_handle, lib=None):
+    """Write every request's synthetic input (uniform[-1, 1) from its seed) at r.in_ptr, in one
+    launch per 256 requests on the given raw stream."""
+    if not reqs:
+        return
+    lib = lib or _provider.load()
+    err = ctypes.create_string_buffer(ERR)
+    if lib.syclfft_b200_fill_uniform(_fill_items(reqs), len(reqs), stream_handle, err, ERR):
+        raise RuntimeError(err.value.decode())
+
+
+def synthetic_input(r: Request, out=None):
+    """The request's input: 2 * elements reals uniform in [-1, 1), value i a function of
+    (r.seed, i) only (syclfft_b200_fill_uniform), viewed as complex; written into `out` when
+    given, on the current stream."""
     import torch
     fdt = torch.float64 if r.double else torch.float32
     if out is None:
         out = torch.empty(2 * r.elements, device="cuda", dtype=fdt)
-    g = generator if generator is not None else torch.Generator(device=out.device)
-    g.manual_seed(r.seed)
-    out.uniform_(-1.0, 1.0, generator=g)
+    q = Request(r.rid, r.lengths, r.batch, r.double, r.direction, r.normalization, r.seed, r.arrival)
+    q.in_ptr = out.data_ptr()
+    fill_inputs([q], torch.cuda.current_stream(out.device).cuda_stream)
     return torch.view_as_complex(out.view(-1, 2))
 
 
@@ -189,7 +214,6 @@ class Server:
         self.max_waiting = 0
         self.pending = {}   # plan key -> future of a plan being created ahead of use
         self.pool = None
-        self._gen = None
         self.arena = None   # request buffers of a run (Arena)
 
     # ---------------------------------------------------------------- resident state
@@ -225,13 +249,18 @@ class Server:
         self.plans[key] = h
         self.plan_bytes += nbytes
         self.plans_created += 1
+        return h
+
+    def _evict(self):
+        """Release least recently used plans over the plan budget once their last launch is
+        done. Called after a round's launches are enqueued, so no plan of the round is released
+        before its execute is issued (the release itself is ordered after it on the device)."""
         while self.plan_bytes > self.plan_budget and len(self.plans) > 1:
             _, (oh, ob, oev) = self.plans.popitem(last=False)
             self.plan_bytes -= ob
             self.retired.append((oh, oev))
             self.evictions += 1
         self._reap()
-        return h
 
     def _reap(self, wait=False):
         keep = []
@@ -291,46 +320,53 @@ class Server:
         self.torch.cuda.empty_cache()
 
     # ---------------------------------------------------------------- data
-    def _fill(self, r: Request, stream=None):
-        """Input and output buffers of a request from the arena (r.buf_off, reserved at
-        admission), the input filled with uniform[-1, 1) from the request's seed on `stream`
-        (default: the current stream)."""
+    def _views(self, r: Request):
+        """Tensor views of a request's input and output in the arena (made on demand)."""
         torch = self.torch
         fdt = torch.float64 if r.double else torch.float32
         buf = self.arena.view(r.buf_off, r.nbytes, fdt)
-        if self._gen is None:
-            self._gen = torch.Generator(device=f"cuda:{self.dev}")
-        if stream is None:
-            r.inp = synthetic_input(r, buf[: 2 * r.elements], self._gen)
-        else:
-            with torch.cuda.stream(stream):
-                r.inp = synthetic_input(r, buf[: 2 * r.elements], self._gen)
+        r.inp = torch.view_as_complex(buf[: 2 * r.elements].view(-1, 2))
         r.out = torch.view_as_complex(buf[2 * r.elements:].view(-1, 2))
 
     def _reserve(self, r: Request):
         off = self.arena.alloc(r.nbytes)
         if off is not None:
             r.buf_off = off
+            r.in_ptr = self.arena_base + off
+            r.out_ptr = r.in_ptr + r.nbytes // 2
         return off is not None
 
     def _release(self, r: Request):
         self.arena.release(r.buf_off, r.nbytes)
         r.inp = r.out = None
 
-    def _execute_one(self, r: Request, stream):
-        h = self._plan(r)
-        rc = self.lib.syclfft_b200_execute_ex(h[0], r.inp.data_ptr(), r.out.data_ptr(), r.batch, r.direction,
-                                              r.normalization, stream.cuda_stream, self.err, ERR)
-        if rc:
+    def _fill(self, reqs, stream):
+        fill_inputs(reqs, stream.cuda_stream, self.lib)
+
+    def _execute_plans(self, reqs, stream):
+        """The requests on their resident plans, one native call (syclfft_b200_execute_many)."""
+        items = (_provider.ExecItemV1 * len(reqs))()
+        used = []
+        for i, r in enumerate(reqs):
+            h = self._plan(r)
+            used.append(h)
+            items[i].plan = h[0]
+            items[i].in_ = r.in_ptr
+            items[i].out = r.out_ptr
+            items[i].batch = r.batch
+            items[i].direction = r.direction
+            items[i].normalization = r.normalization
+        if self.lib.syclfft_b200_execute_many(items, len(reqs), stream.cuda_stream, self.err, ERR):
             raise RuntimeError(self.err.value.decode())
-        return h
+        self._evict()
+        return used
 
     def _execute_family(self, double, reqs, stream):
         f = self._family(double)
         items = (_provider.FamilyItemV1 * len(reqs))()
         for i, r in enumerate(reqs):
-            items[i].in_ = r.inp.data_ptr()
-            items[i].out = r.out.data_ptr()
+            items[i].in_ = r.in_ptr
+            items[i].out = r.out_ptr
             items[i].n = r.lengths[0]
             items[i].batch = r.batch
             items[i].direction = r.direction
@@ -344,8 +380,8 @@ class Server:
         g = self._group(n, double)
         items = (_provider.GroupItemV1 * len(reqs))()
         for i, r in enumerate(reqs):
-            items[i].in_ = r.inp.data_ptr()
-            items[i].out = r.out.data_ptr()
+            items[i].in_ = r.in_ptr
+            items[i].out = r.out_ptr
             items[i].batch = r.batch
             items[i].direction = r.direction
             items[i].normalization = r.normalization
@@ -357,9 +393,12 @@ class Server:
     def _keep(self, r: Request, keep_results):
         """What a run keeps of a finished request's output before its buffer is reused: all of
         it on the host (keep_results True) or what a callable returns for it."""
+        if not keep_results:
+            return
+        self._views(r)
         if callable(keep_results):
             r.result = keep_results(r)
-        elif keep_results:
+        else:
             r.result = r.out.cpu()
 
     def run(self, requests, mode="served", keep_results=False):
@@ -384,6 +423,7 @@ class Server:
         if size < max(r.nbytes for r in reqs):
             raise RuntimeError("admission budget smaller than the largest request")
         self.arena = Arena(torch.empty(size, dtype=torch.uint8, device=f"cuda:{self.dev}"))
+        self.arena_base = self.arena.t.data_ptr()
         torch.cuda.synchronize(self.dev)
         t0 = time.perf_counter()
         start.record(self.streams[0])
@@ -396,14 +436,14 @@ class Server:
                 while time.perf_counter() - t0 < r.arrival:
                     pass
                 self._reserve(r)
-                self._fill(r, s)
+                self._fill([r], s)
                 cfg = _provider.make_config(list(r.lengths), r.batch, r.direction, r.double, False, r.normalization,
                                             False, self.dev)
                 h = self.api.create(ctypes.byref(cfg), self.err, ERR)
                 if not h:
                     raise RuntimeError(self.err.value.decode())
                 self.plans_created += 1
-                rc = self.api.execute(h, r.inp.data_ptr(), r.out.data_ptr(), s.cuda_stream, self.err, ERR)
+                rc = self.api.execute(h, r.in_ptr, r.out_ptr, s.cuda_stream, self.err, ERR)
                 if rc:
                     raise RuntimeError(self.err.value.decode())
                 with torch.cuda.stream(s):
@@ -420,11 +460,10 @@ class Server:
                 while time.perf_counter() - t0 < r.arrival:
                     pass
                 self._reserve(r)
-                self._fill(r, s)
-                with torch.cuda.stream(s):
-                    h = self._execute_one(r, s)
-                    ev = torch.cuda.Event(enable_timing=True)
-                    ev.record(s)
+                self._fill([r], s)
+                h = self._execute_plans([r], s)[0]
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(s)
                 h[2] = ev
                 ev.synchronize()
                 r.t_done = start.elapsed_time(ev) / 1e3
@@ -490,18 +529,15 @@ class Server:
                 si = hash(key) % S
                 s = self.streams[si]
                 used_plans = []
-                with torch.cuda.stream(s):
-                    for r in rs:
-                        self._fill(r)
-                    if key[0] == "f":
-                        self._execute_family(key[1], rs, s)
-                    elif key[0] == "g":
-                        self._execute_group((key[1], key[2]), rs, s)
-                    else:
-                        for r in rs:
-                            used_plans.append(self._execute_one(r, s))
-                    ev = torch.cuda.Event(enable_timing=True)
-                    ev.record(s)
+                self._fill(rs, s)
+                if key[0] == "f":
+                    self._execute_family(key[1], rs, s)
+                elif key[0] == "g":
+                    self._execute_group((key[1], key[2]), rs, s)
+                else:
+                    used_plans = self._execute_plans(rs, s)
+                ev = torch.cuda.Event(enable_timing=True)
+                ev.record(s)
                 for h in used_plans:
                     h[2] = ev
                 in_flight[si].append((ev, rs))

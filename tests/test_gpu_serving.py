@@ -306,3 +306,55 @@ def test_execute_ex_direction_override(torch, shape, dbl):
             ref = fp64_fft(x, shape, batch, d, norm_scale(nm, d, n))
             assert rel_l2(out.cpu().numpy(), ref) <= spec_tol(n, dbl), (plan_dir, d, nm)
         api.destroy(h)
+
+
+def test_serving_helpers_fill_and_execute_many(torch):
+    """syclfft_b200_fill_uniform: value i depends on (seed, i) only -- the same whether a buffer
+    is filled alone or among 300 others (two launches of up to 256 items), in [-1, 1), mean
+    about 0; syclfft_b200_execute_many gives what one execute_ex per item gives."""
+    from syclfft_b200 import _provider, serving
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    reqs = [serving.Request(i, (int(n),), 3, bool(i % 3 == 0), -1, 0, 1000 + i, 0.0)
+            for i, n in enumerate(np.random.default_rng(2).choice([64, 100, 1024, 3000, 65536], 300))]
+    bufs = [torch.empty(2 * r.elements, dtype=torch.float64 if r.double else torch.float32, device="cuda")
+            for r in reqs]
+    for r, b in zip(reqs, bufs):
+        r.in_ptr = b.data_ptr()
+    serving.fill_inputs(reqs, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    for r, b in list(zip(reqs, bufs))[::37]:
+        alone = serving.synthetic_input(r).view(torch.float64 if r.double else torch.float32)
+        torch.cuda.synchronize()
+        assert torch.equal(alone, b)
+        assert float(b.min()) >= -1.0 and float(b.max()) < 1.0
+    allv = torch.cat([b.double() for b in bufs])
+    assert abs(float(allv.mean())) < 5e-3 and abs(float(allv.var()) - 1 / 3) < 5e-3
+    # execute_many vs execute_ex, mixed plans, directions and normalizations
+    plans = {}
+    items = (_provider.ExecItemV1 * 12)()
+    outs_many, outs_one = [], []
+    for i, r in enumerate(reqs[:12]):
+        key = (r.lengths[0], r.double)
+        if key not in plans:
+            cfg = _provider.make_config([r.lengths[0]], 8, -1, r.double, False, 0, False, 0)
+            plans[key] = lib.syclfft_b200_create_ex(ctypes.byref(cfg), 0, err, 1024)
+            assert plans[key], err.value
+        o1, o2 = torch.empty_like(bufs[i]), torch.empty_like(bufs[i])
+        outs_many.append(o1)
+        outs_one.append(o2)
+        d, nm = (-1, 1) if i % 2 else (1, 3)
+        items[i].plan, items[i].in_, items[i].out = plans[key], bufs[i].data_ptr(), o1.data_ptr()
+        items[i].batch, items[i].direction, items[i].normalization = r.batch, d, nm
+        assert lib.syclfft_b200_execute_ex(plans[key], bufs[i].data_ptr(), o2.data_ptr(), r.batch, d, nm,
+                                           torch.cuda.current_stream().cuda_stream, err, 1024) == 0, err.value
+    assert lib.syclfft_b200_execute_many(items, 12, torch.cuda.current_stream().cuda_stream, err, 1024) == 0, err.value
+    torch.cuda.synchronize()
+    for a, b in zip(outs_many, outs_one):
+        assert torch.equal(a, b)
+    items[3].direction = 5
+    assert lib.syclfft_b200_execute_many(items, 12, torch.cuda.current_stream().cuda_stream, err, 1024) != 0
+    assert b"execute item 3" in err.value and b"direction" in err.value
+    torch.cuda.synchronize()
+    for h in plans.values():
+        _provider.provider(lib).destroy(h)

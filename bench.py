@@ -840,6 +840,71 @@ def _layout_rows(sf, torch, dev, peak, timed, prefix=""):
     return rows
 
 
+def run_serve_devtime(args):
+    """Device time of the serving stream's requests: every request executed back to back on
+    one stream (no admission loop), CUDA events around each; one JSON line per plan shape
+    (requests, device ms, share, algorithmic GB/s) and a total. The floor of any loop that runs
+    these requests on these kernels without overlapping them."""
+    import collections
+    import ctypes
+    import torch
+    from syclfft_b200 import _provider, serving
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    torch.cuda.set_device(0)
+    reqs = serving.make_request_stream(count=args.requests, rate=args.rate, seed=5)
+    biggest = {}
+    for r in reqs:
+        k = (r.lengths[0], r.double)
+        biggest[k] = max(biggest.get(k, 0), r.batch)
+    plans, shape = {}, {}
+    desc = ctypes.create_string_buffer(1 << 16)
+    for (n, dbl), b in biggest.items():
+        cfg = _provider.make_config([n], b, -1, dbl, False, 0, False, 0)
+        h = lib.syclfft_b200_create_ex(ctypes.byref(cfg), _provider.CREATE_STREAM_SCRATCH, err, 1024)
+        if not h:
+            raise RuntimeError(err.value.decode())
+        plans[(n, dbl)] = h
+        lib.syclfft_b200_describe_plan(h, desc, len(desc))
+        passes = json.loads(desc.value.decode())["passes"]
+        shape[(n, dbl)] = ("c128 " if dbl else "c64 ") + "+".join(
+            q["kind"] + ("(lean)" if q.get("lean") else
+                         "(general)" if max(q["fixed_id"], q["blue_id"], q["piped_id"], q["cluster_id"], q["tc_id"]) < 0
+                         else "") for q in passes)
+    most = {False: 0, True: 0}
+    for r in reqs:
+        most[r.double] = max(most[r.double], r.elements)
+    bufs = {d: [torch.zeros(most[d], dtype=torch.complex128 if d else torch.complex64, device="cuda") for _ in range(2)]
+            for d in (False, True)}
+    s = torch.cuda.Stream()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(len(reqs) + 1)]
+    for record in (False, True):
+        if record:
+            evs[0].record(s)
+        for i, r in enumerate(reqs):
+            x, y = bufs[r.double]
+            if lib.syclfft_b200_execute_ex(plans[(r.lengths[0], r.double)], x.data_ptr(), y.data_ptr(), r.batch,
+                                           r.direction, r.normalization, s.cuda_stream, err, 1024):
+                raise RuntimeError(err.value.decode())
+            if record:
+                evs[i + 1].record(s)
+        torch.cuda.synchronize()
+    agg = collections.defaultdict(lambda: [0, 0.0, 0.0])
+    for i, r in enumerate(reqs):
+        a = agg[shape[(r.lengths[0], r.double)]]
+        a[0] += 1
+        a[1] += evs[i].elapsed_time(evs[i + 1])
+        a[2] += 2 * r.elements * (16 if r.double else 8)
+    total = sum(a[1] for a in agg.values())
+    for k, (c, ms, b) in sorted(agg.items(), key=lambda kv: -kv[1][1]):
+        print(json.dumps({"shape": k, "requests": c, "device_ms": round(ms, 1), "share": round(ms / total, 3),
+                          "gbs_alg": round(b / ms / 1e6, 1)}))
+    print(json.dumps({"metric": "serving stream device time, requests back to back on one stream", "unit": "ms",
+                      "value": round(total, 1), "requests": len(reqs), "plans": len(plans)}))
+    for h in plans.values():
+        _provider.provider(lib).destroy(h)
+
+
 def run_serve(args):
     """Serving configuration: the mixed request stream through the continuous-batching loop
     and through per-request plain executes; one JSON line with both."""
@@ -894,6 +959,8 @@ def main():
     ap.add_argument("--split", action="store_true",
                     help="complex<float> plans on the split-precision tensor-core path where it applies")
     ap.add_argument("--serve", action="store_true", help="run the serving-stream benchmark instead")
+    ap.add_argument("--serve-devtime", action="store_true",
+                    help="the serving stream's device time by plan shape (requests back to back, one stream)")
     ap.add_argument("--table", action="store_true", help="every configuration's rows (plain, autotuned, cuFFT via torch, CPU)")
     ap.add_argument("--table-rows", default="", help="with --table: only the rows whose name starts with this")
     ap.add_argument("--config", type=int, choices=[3, 4], default=0,
@@ -907,6 +974,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve_devtime:
+        return run_serve_devtime(args)
     if args.serve:
         return run_serve(args)
     if args.config:

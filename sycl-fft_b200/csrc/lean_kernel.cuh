@@ -62,6 +62,9 @@ __device__ __forceinline__ int lean_sidx(const LeanParams& P, int k) {
 
 // One radix-R Stockham stage over the tile: first stage loads from HBM, the last stores to HBM
 // (or to shared memory for the transposed store), inner stages exchange through shared memory.
+// Global and column-tile addresses advance by a per-stage step (one add per element; a second
+// path for padded line rows whose step is a multiple of the padding unit cost more registers
+// than it saved), and the first stage (Ns = 1) and the last (j < Ns) need no quotient.
 template <int R, class T, int MAXV, bool MODEC, int FEAT, bool FIRST, bool LAST>
 __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T>& X) {
     using C = cplx<T>;
@@ -69,52 +72,72 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
     const int nr = P.n / R;
     const int Ns = P.ns[s];
     C v[NB * R];
+    // loads: element k = j + r * nr
+    constexpr bool lin_in = MODEC;
+    const int in_step = FIRST ? (MODEC ? nr * P.in_ks : nr) : (MODEC ? nr << P.w_shift : 0);
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * P.tpl;
         if (X.active && j < nr) {
+            if constexpr (FIRST) {
+                const C* g = X.gin + (MODEC ? j * P.in_ks : j);
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int k = j + r * nr;
-                C a;
-                if constexpr (FIRST) {
-                    a = cmake<C>(T(0), T(0));
+                for (int r = 0; r < R; ++r) {
+                    C a = cmake<C>(T(0), T(0));
                     if (X.line_ok) {
-                        a = X.gin[MODEC ? k * P.in_ks : k];
+                        a = g[r * in_step];
                         if (P.conj_in) a.y = -a.y;
                     }
-                } else {
-                    a = X.sm[lean_sidx<T, MODEC>(P, k)];
+                    v[i * R + r] = a;
                 }
-                v[i * R + r] = a;
+            } else if constexpr (lin_in) {
+                const C* p = X.sm + lean_sidx<T, MODEC>(P, j);
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[i * R + r] = p[r * in_step];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[i * R + r] = X.sm[lean_sidx<T, MODEC>(P, j + r * nr)];
             }
         }
     }
     if constexpr (!FIRST) __syncthreads();
     constexpr bool to_global = LAST && FEAT != kLeanTStore;
+    // stores: element k = base + r * Ns (base = j in the last stage)
+    constexpr bool lin_out = MODEC;
+    const int out_step = to_global ? (MODEC ? nr * P.out_ks : nr) : (MODEC ? Ns << P.w_shift : 0);
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * P.tpl;
         if (X.active && j < nr) {
             C* u = &v[i * R];
-            const int q = lean_quot(P, s, j);
-            const int jm = j - q * Ns;
-            if (R > 1 && Ns > 1) {
+            int q, jm;
+            if constexpr (FIRST) {
+                q = j;
+                jm = 0;
+            } else if constexpr (LAST) {
+                q = 0;
+                jm = j;
+            } else {
+                q = lean_quot(P, s, j);
+                jm = j - q * Ns;
+            }
+            if (R > 1 && !FIRST && Ns > 1) {
                 const C* tw = static_cast<const C*>(P.tw) + P.tw_off[s] + jm * (R - 1);
 #pragma unroll
                 for (int r = 1; r < R; ++r) u[r] = cmul(u[r], __ldg(tw + (r - 1)));
             }
             dft<R, T>(u);
             const int base = q * Ns * R + jm;
+            if constexpr (to_global) {
+                if (X.line_ok) {
+                    C* g = X.gout + (MODEC ? j * P.out_ks : j);
+                    const int m0 = j * X.c, mstep = nr * X.c;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                const int k = base + r * Ns;
-                if constexpr (to_global) {
-                    if (X.line_ok) {
+                    for (int r = 0; r < R; ++r) {
                         C a = u[r];
                         if (P.conj_out) a.y = -a.y;
                         if constexpr (FEAT == kLeanTw4) {
-                            const int m = k * X.c;
+                            const int m = m0 + r * mstep;
                             C w = cmul(__ldg(static_cast<const C*>(P.tw4_hi) + (m >> P.tw4_shift)),
                                        __ldg(static_cast<const C*>(P.tw4_lo) + (m & ((1 << P.tw4_shift) - 1))));
                             if (P.tw4_conj) w.y = -w.y;
@@ -122,11 +145,16 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
                         }
                         a.x *= static_cast<T>(P.scale);
                         a.y *= static_cast<T>(P.scale);
-                        X.gout[MODEC ? k * P.out_ks : k] = a;
+                        g[r * out_step] = a;
                     }
-                } else {
-                    X.sm[lean_sidx<T, MODEC>(P, k)] = u[r];
                 }
+            } else if constexpr (lin_out) {
+                C* p = X.sm + lean_sidx<T, MODEC>(P, base);
+#pragma unroll
+                for (int r = 0; r < R; ++r) p[r * out_step] = u[r];
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) X.sm[lean_sidx<T, MODEC>(P, base + r * Ns)] = u[r];
             }
         }
     }

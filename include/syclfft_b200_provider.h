@@ -188,7 +188,7 @@ SYCLFFT_B200_EXPORT int syclfft_b200_plan_set_wait_limit(void *plan, int64_t pol
  * one after the other on `batch` transforms (0 = the first plan's batch count) read from the
  * page-locked host buffer `in` and written to the page-locked host buffer `out` (in == out
  * allowed). All stages have the same precision, transform size and device, and at least
- * `batch` transforms. The batch is cut into chunks (SYCLFFT_B200_HOST_CHUNK_MB, 32 by
+ * `batch` transforms. The batch is cut into chunks (SYCLFFT_B200_HOST_CHUNK_MB, 64 by
  * default) that pass through device staging slots: copy in on an internal stream, the
  * stages on `stream`, copy out on another internal stream, so both copy directions and the
  * kernels overlap. Stream-ordered: the copies start after earlier work on `stream`, and

@@ -1351,7 +1351,7 @@ size_t host_chunk_bytes() {
     static const size_t bytes = [] {
         const char* v = std::getenv("SYCLFFT_B200_HOST_CHUNK_MB");
         const long mb = v ? std::strtol(v, nullptr, 10) : 0;
-        return static_cast<size_t>(mb > 0 ? mb : 32) << 20;
+        return static_cast<size_t>(mb > 0 ? mb : 64) << 20;
     }();
     return bytes;
 }

@@ -2,9 +2,10 @@
 // shared-memory scheme as pass_kernel.cuh for lengths the size-specialised catalog does not
 // have (7-smooth lengths with factors 3, 5, 7), with the layout and the fused feature fixed at
 // compile time and the per-element work cut to what the three contiguous cases need:
-//   kLeanPlain  (kModeK): whole lines, conjugation and scale on load / store;
-//   kLeanTw4    (kModeC): four-step column pass, W_L^(k*c) twiddle on the store;
-//   kLeanTStore (kModeK): four-step row pass, stored transposed through shared memory.
+//   kLeanPlain, kModeK: whole lines, conjugation and scale on load / store;
+//   kLeanTw4,   kModeC: four-step column pass, W_L^(k*c) twiddle on the store;
+//   kLeanPlain, kModeC: four-step row pass as a column tile (lanes walk adjacent rows, element
+//                       stride 1 on load and the transposed element stride on store).
 // Element offsets within a line are 32-bit, the butterfly index j mod Ns uses a precomputed
 // multiply-shift quotient (ns_magic / ns_shift), and no table, padding or second-FFT branch
 // is compiled in. Strided layouts and the Bluestein extras stay on fft_pass_kernel.
@@ -17,7 +18,7 @@
 
 namespace sfb {
 
-enum : int { kLeanPlain = 0, kLeanTw4 = 1, kLeanTStore = 2 };
+enum : int { kLeanPlain = 0, kLeanTw4 = 1 };
 
 struct LeanParams {
     int n = 0, tpl = 1, w = 1, w_shift = 0;  // w: lines per tile, a power of two (w = 1 << w_shift)
@@ -60,8 +61,8 @@ __device__ __forceinline__ int lean_sidx(const LeanParams& P, int k) {
     else return k + (k >> P.pad_shift);
 }
 
-// One radix-R Stockham stage over the tile: first stage loads from HBM, the last stores to HBM
-// (or to shared memory for the transposed store), inner stages exchange through shared memory.
+// One radix-R Stockham stage over the tile: first stage loads from HBM, the last stores to HBM,
+// inner stages exchange through shared memory.
 // Global and column-tile addresses advance by a per-stage step (one add per element; a second
 // path for padded line rows whose step is a multiple of the padding unit cost more registers
 // than it saved), and the first stage (Ns = 1) and the last (j < Ns) need no quotient.
@@ -101,7 +102,7 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
         }
     }
     if constexpr (!FIRST) __syncthreads();
-    constexpr bool to_global = LAST && FEAT != kLeanTStore;
+    constexpr bool to_global = LAST;
     // stores: element k = base + r * Ns (base = j in the last stage)
     constexpr bool lin_out = MODEC;
     const int out_step = to_global ? (MODEC ? nr * P.out_ks : nr) : (MODEC ? Ns << P.w_shift : 0);
@@ -230,21 +231,6 @@ __global__ void __launch_bounds__(MAXT, 65536 / (MAXT * lean_regs<T, MAXV>()))
     lean_group<5, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<7, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_edge<T, MAXV, MODEC, FEAT, false, true>(P, P.nstages - 1, X);
-    if constexpr (FEAT == kLeanTStore) {
-        static_assert(!MODEC, "the transposed store is a kModeK row pass");
-        // rows c0 .. c0 + w - 1 are consecutive output columns: walk (row fastest, element)
-        const int total = P.w * P.n;
-        const T sc = static_cast<T>(P.scale);
-        const T sy = P.conj_out ? -sc : sc;
-        C* dst = out + o * P.out_hi + c0 * P.out_cs;
-        for (int idx = tid; idx < total; idx += blockDim.x) {
-            const int k = idx >> P.w_shift;
-            const int w = idx & (P.w - 1);
-            if (c0 + w >= P.n_cols) continue;
-            const C a = sm[w * P.pitch + k + (k >> P.pad_shift)];
-            dst[w * P.out_cs + static_cast<int64_t>(k) * P.out_ks] = cmake<C>(a.x * sc, a.y * sy);
-        }
-    }
 }
 
 }  // namespace sfb

@@ -1,6 +1,6 @@
 // Instantiations of the runtime-length contiguous pass kernel (lean_kernel.cuh): float with 16
 // values per thread, double with 8 or 16, CTA bounds 256 / 512 / 1024, and the three
-// (layout, feature) pairs kModeK plain, kModeC four-step twiddle, kModeK transposed store.
+// (layout, feature) pairs kModeK plain, kModeC four-step twiddle, kModeC plain (four-step rows).
 #include <atomic>
 #include <climits>
 
@@ -40,8 +40,7 @@ cudaError_t by_layout(const LeanParams& p, bool modec, int feat, int threads, si
                       const void* in, void* out, cudaStream_t stream) {
     if (!modec && feat == kLeanPlain) return run<T, MAXV, MAXT, false, kLeanPlain>(p, threads, smem, grid, in, out, stream);
     if (modec && feat == kLeanTw4) return run<T, MAXV, MAXT, true, kLeanTw4>(p, threads, smem, grid, in, out, stream);
-    if (!modec && feat == kLeanTStore)
-        return run<T, MAXV, MAXT, false, kLeanTStore>(p, threads, smem, grid, in, out, stream);
+    if (modec && feat == kLeanPlain) return run<T, MAXV, MAXT, true, kLeanPlain>(p, threads, smem, grid, in, out, stream);
     return cudaErrorInvalidDeviceFunction;
 }
 

@@ -271,7 +271,10 @@ struct Builder {
         if (p.mode == kModeK) {
             p.pad_shift = pad_shift_for(req.dbl);
             p.pitch = kmode_pitch(p.n, p.pad_shift);
+            // lines per CTA: about 256 threads, a power of two (the lean kernel's tiles)
             w = want_w > 0 ? want_w : std::max(1, 256 / cfg.tpl);
+            if (want_w <= 0)
+                while (w & (w - 1)) w &= w - 1;
             w = static_cast<int>(std::min<int64_t>(w, p.n_cols));
             while (w > 1 && (w * cfg.tpl > max_threads ||
                              static_cast<int64_t>(w) * p.pitch * cs > smem_limit))
@@ -1549,8 +1552,8 @@ const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
 // Runtime-length passes whose layout the contiguous kernel (lean_kernel.cuh) covers: whole
 // contiguous lines, or the column / row pass of a contiguous four-step, with no table,
 // padding or second FFT, at least two stages in the radix order 16, 8, 4, 2, 3, 5, 7 and a
-// power-of-two tile width. Values of lean_feat: 0 plain, 1 four-step twiddle, 2 transposed store.
-static void mark_lean(PassSpec& ps) {
+// power-of-two tile width. Values of lean_feat: 0 plain, 1 four-step twiddle.
+static void mark_lean(PassSpec& ps, int64_t cs) {
     const PassParams& p = ps.p;
     if (ps.fixed_id >= 0 || ps.cluster_id >= 0 || ps.piped_id >= 0 || ps.tc_id >= 0 || ps.blue_id >= 0 || ps.rader ||
         ps.cluster_pipe || ps.tw_base)
@@ -1577,8 +1580,16 @@ static void mark_lean(PassSpec& ps) {
         ps.lean_feat = 1;
     } else if (p.mode == kModeK && p.store_via_smem && p.tw4_sign == 0 && p.sel_mode == kSelNone && p.g_k == 1 &&
                p.in.ks == 1 && p.out.cs == 1 && p.in_len >= n && p.out_len >= n) {
+        // The row pass of a contiguous four-step as a column-tile pass: lanes walk the tile's w
+        // adjacent rows (loads are runs of 64 / 128 bytes per row, stores runs of w consecutive
+        // output columns), so neither the padded row layout nor a transposed-store phase is
+        // needed and every shared-memory address steps linearly.
+        PassParams& q = ps.p;
+        q.mode = kModeC;
+        q.store_via_smem = 0;
+        ps.smem_bytes = static_cast<int64_t>(q.w) * q.n * cs;
         ps.lean = true;
-        ps.lean_feat = 2;
+        ps.lean_feat = 0;
     }
 }
 
@@ -1606,7 +1617,7 @@ PlanSpec make_plan(const PlanRequest& req) {
     }
     if (plan.passes.empty()) b.copy_pass(cur);
     plan.passes.back().p.scale = plan.scale;
-    for (auto& ps : plan.passes) mark_lean(ps);
+    for (auto& ps : plan.passes) mark_lean(ps, req.dbl ? 16 : 8);
     // The batch is the outermost index of every pass: the pass's outer count when it has
     // one (n_outer > 1 or strided columns), else its line count.
     for (auto& ps : plan.passes) {

@@ -75,7 +75,7 @@ struct PassSpec {
     bool rader_dc = false;
     Buf rader_src = Buf::Input;
     // runtime-length pass on the contiguous-layout kernel (lean_kernel.cuh) instead of the
-    // general one; lean_feat: kLeanPlain / kLeanTw4 / kLeanTStore
+    // general one; lean_feat: kLeanPlain / kLeanTw4
     bool lean = false;
     int lean_feat = 0;
 };

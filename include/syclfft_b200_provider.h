@@ -280,6 +280,11 @@ typedef struct syclfft_b200_fill_item_v1 {
 
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_many(const syclfft_b200_exec_item_v1 *items, uint32_t count, void *stream,
                                                   char *err, size_t cap);
+/* Release the scratch arena that plans made with SYCLFFT_B200_CREATE_STREAM_SCRATCH borrowed
+ * on `stream` of `device` (freed in stream order, after the work already on the stream); the
+ * next such execute on the stream allocates a new one. Call before destroying a stream that ran
+ * stream-scratch plans: arenas are kept per stream and are otherwise held until exit. */
+SYCLFFT_B200_EXPORT void syclfft_b200_release_stream_scratch(void *stream, int32_t device);
 SYCLFFT_B200_EXPORT int syclfft_b200_fill_uniform(const syclfft_b200_fill_item_v1 *items, uint32_t count,
                                                   void *stream, char *err, size_t cap);
 

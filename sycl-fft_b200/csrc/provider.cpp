@@ -308,14 +308,17 @@ struct DevicePlan {
 
 // Scratch arenas, one per (device, stream): stream-ordered (cudaMallocAsync on the stream
 // itself), grown on demand, shared by every stream-scratch plan executed on that stream.
+struct StreamArena {
+    void* ptr = nullptr;
+    size_t size = 0;
+};
+std::mutex g_arena_mu;
+std::map<std::pair<int, cudaStream_t>, StreamArena> g_arenas;
+
 void* stream_arena(int device, cudaStream_t stream, size_t bytes, bool capturing) {
-    struct Arena {
-        void* ptr = nullptr;
-        size_t size = 0;
-    };
-    static std::mutex mu;
-    static std::map<std::pair<int, cudaStream_t>, Arena> arenas;
-    std::lock_guard<std::mutex> lock(mu);
+    auto& arenas = g_arenas;
+    using Arena = StreamArena;
+    std::lock_guard<std::mutex> lock(g_arena_mu);
     Arena& a = arenas[{device, stream}];
     if (a.size < bytes) {
         // memory allocated inside a CUDA-graph capture would belong to the graph
@@ -1799,6 +1802,20 @@ SYCLFFT_B200_EXPORT int syclfft_b200_execute_ex(void* plan, const void* in, void
         sfb::set_error(err, cap, e.what());
         return 1;
     }
+}
+
+SYCLFFT_B200_EXPORT void syclfft_b200_release_stream_scratch(void* stream, int32_t device) {
+    std::lock_guard<std::mutex> lock(sfb::g_arena_mu);
+    auto it = sfb::g_arenas.find({device, static_cast<cudaStream_t>(stream)});
+    if (it == sfb::g_arenas.end()) return;
+    if (it->second.ptr) {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        if (prev != device) cudaSetDevice(device);
+        cudaFreeAsync(it->second.ptr, static_cast<cudaStream_t>(stream));  // after the stream's work
+        if (prev != device) cudaSetDevice(prev);
+    }
+    sfb::g_arenas.erase(it);
 }
 
 SYCLFFT_B200_EXPORT int syclfft_b200_execute_many(const syclfft_b200_exec_item_v1* items, uint32_t count, void* stream,

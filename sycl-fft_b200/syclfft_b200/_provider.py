@@ -144,6 +144,7 @@ EXPORTED_SYMBOLS = (
     "syclfft_b200_family_execute",
     "syclfft_b200_execute_many",
     "syclfft_b200_fill_uniform",
+    "syclfft_b200_release_stream_scratch",
     "syclfft_b200_family_destroy",
     "syclfft_b200_create_real",
     "syclfft_b200_create_strided",
@@ -209,6 +210,8 @@ def load(path: str | None = None):
     lib.syclfft_b200_execute_many.restype = ctypes.c_int
     lib.syclfft_b200_execute_many.argtypes = [ctypes.POINTER(ExecItemV1), ctypes.c_uint32, ctypes.c_void_p,
                                               ctypes.c_char_p, ctypes.c_size_t]
+    lib.syclfft_b200_release_stream_scratch.restype = None
+    lib.syclfft_b200_release_stream_scratch.argtypes = [ctypes.c_void_p, ctypes.c_int32]
     lib.syclfft_b200_fill_uniform.restype = ctypes.c_int
     lib.syclfft_b200_fill_uniform.argtypes = [ctypes.POINTER(FillItemV1), ctypes.c_uint32, ctypes.c_void_p,
                                               ctypes.c_char_p, ctypes.c_size_t]

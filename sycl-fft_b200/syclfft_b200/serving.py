@@ -306,6 +306,8 @@ class Server:
         self.pending.clear()
         self.torch.cuda.synchronize(self.dev)
         self._reap(wait=True)
+        for st in self.streams:  # the plans' scratch arenas on this server's streams
+            self.lib.syclfft_b200_release_stream_scratch(st.cuda_stream, self.dev)
         for handle, _, _ in self.plans.values():
             self.api.destroy(handle)
         for g in self.groups.values():
@@ -496,9 +498,13 @@ class Server:
             self.pool.shutdown(wait=True)
             self.pool = None
 
+    ADMIT_WINDOW = 64      # requests behind a head that does not fit that may be admitted first
+    HEAD_PATIENCE = 0.05   # seconds a head may be passed over before everything waits for it
+
     def _serve_loop(self, reqs, t0, start, keep_results):
         torch = self.torch
         nxt = 0
+        head_blocked = None  # when the current head first failed to fit
         waiting = deque()
         S = len(self.streams)
         in_flight = [deque() for _ in range(S)]  # per stream, in launch order: (event, [requests])
@@ -510,13 +516,29 @@ class Server:
                 self._prefetch(reqs[nxt])  # start its plan while it waits for admission
                 nxt += 1
             self.max_waiting = max(self.max_waiting, len(waiting))
-            # admission by HBM budget: FIFO, while the request's buffers fit in the arena
+            # admission by HBM budget: FIFO while the request's buffers fit in the arena; when the
+            # head does not fit, up to ADMIT_WINDOW requests behind it that do fit go ahead (the
+            # GPU would otherwise idle behind one large request), unless the head has already
+            # been passed over for HEAD_PATIENCE seconds, which keeps it from starving
             bins = {}
-            while waiting:
-                r = waiting[0]
-                if not self._reserve(r):
-                    break
-                waiting.popleft()
+            admitted = []
+            i = skipped = 0
+            while i < len(waiting) and skipped <= self.ADMIT_WINDOW:
+                r = waiting[i]
+                if self._reserve(r):
+                    admitted.append(r)
+                    del waiting[i]
+                    if i == 0:
+                        head_blocked = None
+                    continue
+                if i == 0:
+                    if head_blocked is None:
+                        head_blocked = now
+                    elif now - head_blocked > self.HEAD_PATIENCE:
+                        break
+                skipped += 1
+                i += 1
+            for r in admitted:
                 if self.family_member(r):
                     key = ("f", r.double)
                 elif self.groupable(r):

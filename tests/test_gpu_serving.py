@@ -358,3 +358,28 @@ def test_serving_helpers_fill_and_execute_many(torch):
     torch.cuda.synchronize()
     for h in plans.values():
         _provider.provider(lib).destroy(h)
+
+
+def test_release_stream_scratch_and_execute_again(torch):
+    """A stream-scratch plan's arena released between executes (as Server.close does before its
+    streams go) is allocated again by the next execute on that stream: same results."""
+    from syclfft_b200 import _provider
+    lib = _provider.load()
+    err = ctypes.create_string_buffer(1024)
+    cfg = _provider.make_config([65536], 8, -1, False, False, 0, False, 0)
+    h = lib.syclfft_b200_create_ex(ctypes.byref(cfg), _provider.CREATE_STREAM_SCRATCH, err, 1024)
+    assert h, err.value
+    s = torch.cuda.Stream()
+    x = torch.randn(65536 * 8, dtype=torch.complex64, device="cuda")
+    outs = []
+    for _ in range(2):
+        y = torch.empty_like(x)
+        assert lib.syclfft_b200_execute_ex(h, x.data_ptr(), y.data_ptr(), 0, -1, 0, s.cuda_stream, err, 1024) == 0, err.value
+        lib.syclfft_b200_release_stream_scratch(s.cuda_stream, torch.cuda.current_device())
+        outs.append(y)
+    lib.syclfft_b200_release_stream_scratch(s.cuda_stream, torch.cuda.current_device())  # nothing held: no-op
+    torch.cuda.synchronize()
+    assert torch.equal(outs[0], outs[1])
+    ref = torch.fft.fft(x.view(8, 65536).to(torch.complex128), dim=1).reshape(-1)
+    assert float((outs[0] - ref).abs().norm() / ref.abs().norm()) < 1e-5 * 16
+    _provider.provider(lib).destroy(h)

@@ -1,14 +1,18 @@
 // Runtime-length pass kernel for contiguous layouts ("lean"): the same Stockham register /
 // shared-memory scheme as pass_kernel.cuh for lengths the size-specialised catalog does not
-// have (7-smooth lengths with factors 3, 5, 7), with the layout and the fused feature fixed at
+// have (7-smooth lengths with factors 3, 5, 7; a 3 and a 5 stage run as one prime-factor radix
+// 15 where 16 values a thread fit), with the layout and the fused feature fixed at
 // compile time and the per-element work cut to what the three contiguous cases need:
 //   kLeanPlain, kModeK: whole lines, conjugation and scale on load / store;
 //   kLeanTw4,   kModeC: four-step column pass, W_L^(k*c) twiddle on the store;
 //   kLeanPlain, kModeC: four-step row pass as a column tile (lanes walk adjacent rows, element
 //                       stride 1 on load and the transposed element stride on store).
 // Element offsets within a line are 32-bit, the butterfly index j mod Ns uses a precomputed
-// multiply-shift quotient (ns_magic / ns_shift), and no table, padding or second-FFT branch
-// is compiled in. Strided layouts and the Bluestein extras stay on fft_pass_kernel.
+// multiply-shift quotient (ns_magic / ns_shift), each butterfly's R - 1 twiddles are read from
+// the stage's table (L1-resident; forming them as powers of one base twiddle in registers
+// measured 15-30% slower here, the kernel being bound by its FMA and ALU issue), and no
+// padding or second-FFT branch is compiled in.
+// Strided layouts and the Bluestein extras stay on fft_pass_kernel.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -163,13 +167,16 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
 }
 
 // The first and the last stage touch HBM and are compiled apart from the inner stages, which
-// run grouped by radix (16, 8, 4, 2, 3, 5, 7, the order the planner gives them), so no stage
+// run grouped by radix (16, 8, 4, 2, 15, 3, 5, 7, the order the planner gives them), so no stage
 // carries the register cost of both kinds of access. At least two stages.
 template <class T, int MAXV, bool MODEC, int FEAT, bool FIRST, bool LAST>
 __device__ __forceinline__ void lean_edge(const LeanParams& P, int s, LeanCtx<T>& X) {
     switch (P.radix[s]) {
         case 16:
             if constexpr (MAXV >= 16) lean_stage<16, T, MAXV, MODEC, FEAT, FIRST, LAST>(P, s, X);
+            break;
+        case 15:
+            if constexpr (MAXV >= 16) lean_stage<15, T, MAXV, MODEC, FEAT, FIRST, LAST>(P, s, X);
             break;
         case 8: lean_stage<8, T, MAXV, MODEC, FEAT, FIRST, LAST>(P, s, X); break;
         case 4: lean_stage<4, T, MAXV, MODEC, FEAT, FIRST, LAST>(P, s, X); break;
@@ -227,6 +234,7 @@ __global__ void __launch_bounds__(MAXT, 65536 / (MAXT * lean_regs<T, MAXV>()))
     lean_group<8, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<4, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<2, T, MAXV, MODEC, FEAT>(P, X, s);
+    if constexpr (MAXV >= 16) lean_group<15, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<3, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<5, T, MAXV, MODEC, FEAT>(P, X, s);
     lean_group<7, T, MAXV, MODEC, FEAT>(P, X, s);

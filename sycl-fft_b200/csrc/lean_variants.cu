@@ -5,6 +5,7 @@
 #include <climits>
 
 #include "lean_launch.hpp"
+#include "planner.hpp"
 
 namespace sfb {
 namespace {
@@ -46,11 +47,7 @@ cudaError_t by_layout(const LeanParams& p, bool modec, int feat, int threads, si
 
 }  // namespace
 
-bool has_lean_variant(bool dbl, int maxv, int maxt) {
-    if (maxt != 256 && maxt != 512 && maxt != 1024) return false;
-    if (!dbl) return maxv == 16;
-    return maxv == 8 || (maxv == 16 && maxt <= 512);
-}
+bool has_lean_variant(bool dbl, int maxv, int maxt) { return lean_variant_exists(dbl, maxv, maxt); }
 
 cudaError_t launch_lean(const LeanParams& p, bool dbl, int maxv, int maxt, bool modec, int feat, int threads,
                         size_t smem, int64_t grid, const void* in, void* out, cudaStream_t stream) {

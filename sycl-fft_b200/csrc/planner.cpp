@@ -1553,20 +1553,48 @@ const FixedEntry* find_fixed(bool dbl, int mode, int n, int feat) {
 // contiguous lines, or the column / row pass of a contiguous four-step, with no table,
 // padding or second FFT, at least two stages in the radix order 16, 8, 4, 2, 3, 5, 7 and a
 // power-of-two tile width. Values of lean_feat: 0 plain, 1 four-step twiddle.
+// Lean passes with 16 values per thread run each (3, 5) pair of stages as one prime-factor
+// radix-15 stage: a radix-3, -5 or -15 stage all need n / 15 threads per line at 16 values a
+// thread, so the tile shape is unchanged and a shared-memory round trip and a barrier go.
+// Returns the new radix sequence, or an empty one when nothing changes.
+static std::vector<int> lean_radix15(const PassSpec& ps) {
+    const StageSeq& f = ps.p.fft1;
+    if (ps.kc.maxv < 16) return {};
+    int n3 = 0, n5 = 0;
+    for (int s = 0; s < f.nstages; ++s) {
+        n3 += f.radix[s] == 3;
+        n5 += f.radix[s] == 5;
+    }
+    const int k = std::min(n3, n5);
+    if (k == 0) return {};
+    std::vector<int> r;
+    for (int s = 0; s < f.nstages; ++s)
+        if (f.radix[s] != 3 && f.radix[s] != 5 && f.radix[s] != 7) r.push_back(f.radix[s]);
+    for (int i = 0; i < k; ++i) r.push_back(15);
+    for (int i = k; i < n3; ++i) r.push_back(3);
+    for (int i = k; i < n5; ++i) r.push_back(5);
+    for (int s = 0; s < f.nstages; ++s)
+        if (f.radix[s] == 7) r.push_back(7);
+    // the lean kernel runs at least two stages (a first from and a last to global memory)
+    if (r.size() < 2 || threads_per_line(static_cast<int>(ps.p.n), r, ps.kc.maxv) != ps.p.tpl) return {};
+    return r;
+}
+
 static void mark_lean(PassSpec& ps, int64_t cs) {
     const PassParams& p = ps.p;
     if (ps.fixed_id >= 0 || ps.cluster_id >= 0 || ps.piped_id >= 0 || ps.tc_id >= 0 || ps.blue_id >= 0 || ps.rader ||
         ps.cluster_pipe || ps.tw_base)
         return;
+    if (!lean_variant_exists(cs == 16, ps.kc.maxv, ps.kc.maxt)) return;
     if (p.fft2.nstages > 0 || p.fft1.nstages < 2 || ps.tables.premul >= 0 || ps.tables.postmul >= 0 ||
         ps.tables.pointwise >= 0 || ps.tables.perm_in >= 0 || ps.tables.perm_out >= 0)
         return;
     if (p.in.d != 1 || p.out.d != 1 || p.flip_in || p.flip_out || p.w < 1 || (p.w & (p.w - 1)) != 0) return;
-    static const int order[] = {16, 8, 4, 2, 3, 5, 7};
+    static const int order[] = {16, 8, 4, 2, 15, 3, 5, 7};
     int pos = 0;
     for (int s = 0; s < p.fft1.nstages; ++s) {
-        while (pos < 7 && order[pos] != p.fft1.radix[s]) ++pos;
-        if (pos == 7) return;  // a radix outside the order, or out of order
+        while (pos < 8 && order[pos] != p.fft1.radix[s]) ++pos;
+        if (pos == 8) return;  // a radix outside the order, or out of order
     }
     const int64_t n = p.n;
     if (p.mode == kModeK && !p.store_via_smem && p.tw4_sign == 0 && p.sel_mode == kSelNone && p.g_k == 1 &&
@@ -1617,7 +1645,12 @@ PlanSpec make_plan(const PlanRequest& req) {
     }
     if (plan.passes.empty()) b.copy_pass(cur);
     plan.passes.back().p.scale = plan.scale;
-    for (auto& ps : plan.passes) mark_lean(ps, req.dbl ? 16 : 8);
+    for (auto& ps : plan.passes) {
+        mark_lean(ps, req.dbl ? 16 : 8);
+        if (!ps.lean) continue;
+        const std::vector<int> r = lean_radix15(ps);
+        if (!r.empty()) ps.p.fft1 = b.make_seq(static_cast<int>(ps.p.n), r, ps.kc.maxv, &ps.tables.tw1);
+    }
     // The batch is the outermost index of every pass: the pass's outer count when it has
     // one (n_outer > 1 or strided columns), else its line count.
     for (auto& ps : plan.passes) {

@@ -75,10 +75,19 @@ struct PassSpec {
     bool rader_dc = false;
     Buf rader_src = Buf::Input;
     // runtime-length pass on the contiguous-layout kernel (lean_kernel.cuh) instead of the
-    // general one; lean_feat: kLeanPlain / kLeanTw4
+    // general one; lean_feat: kLeanPlain / kLeanTw4. A lean pass reads base twiddles
+    // (tw_base), so it only runs on the lean kernel.
     bool lean = false;
     int lean_feat = 0;
 };
+
+// The lean kernel's instantiations (lean_variants.cu): float with 16 values per thread, double
+// with 8 (or 16 up to 512 threads); CTA bounds 256 / 512 / 1024.
+inline bool lean_variant_exists(bool dbl, int maxv, int maxt) {
+    if (maxt != 256 && maxt != 512 && maxt != 1024) return false;
+    if (!dbl) return maxv == 16;
+    return maxv == 8 || (maxv == 16 && maxt <= 512);
+}
 
 // One entry of cluster_catalog.h as seen by the host.
 struct ClusterEntry {

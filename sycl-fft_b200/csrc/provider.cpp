@@ -1167,7 +1167,10 @@ void launch_bound_pass(DevicePlan* plan, const BoundPass& bp, void* src, void* d
         check(launch_fixed(ps.fixed_id, plan->spec.req.dbl, bp.p.mode == kModeC, bp.fp, ps.threads,
                            static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
               "FFT pass launch");
-    } else if (ps.lean && has_lean_variant(plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt)) {
+    } else if (ps.lean) {
+        // lean passes may hold radix-15 stages, which the general kernel does not have
+        if (!has_lean_variant(plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt))
+            throw std::runtime_error("runtime-length pass has no lean kernel instantiation");
         check(launch_lean(to_lean(bp.p), plan->spec.req.dbl, ps.kc.maxv, ps.kc.maxt, bp.p.mode == kModeC, ps.lean_feat,
                           ps.threads, static_cast<size_t>(ps.smem_bytes), bp.p.tiles, src, dst, stream),
               "FFT pass launch");

@@ -28,6 +28,21 @@ def butterfly(radix, x, double=True):
     return out[0::2] + 1j * out[1::2]
 
 
+def twiddle_powers(mode, radix, w, x, double=True):
+    """u[r] * w^r (r = 1..radix-1, u[0] unchanged) through the size-specialised kernels'
+    twiddle_powers (mode 0: the balanced product tree)."""
+    L = _load("libbutterfly_check.so")
+    dt = np.float64 if double else np.float32
+    xin = np.ascontiguousarray(np.stack([x.real, x.imag], -1).reshape(-1).astype(dt))
+    out = np.zeros_like(xin)
+    fn = L.sfb_check_powers_f64 if double else L.sfb_check_powers_f32
+    real = ctypes.c_double if double else ctypes.c_float
+    fn.argtypes = [ctypes.c_int, ctypes.c_int, real, real, ctypes.c_void_p, ctypes.c_void_p]
+    rc = fn(int(mode), int(radix), w.real, w.imag, ctypes.c_void_p(xin.ctypes.data), ctypes.c_void_p(out.ctypes.data))
+    assert rc == 0
+    return out[0::2] + 1j * out[1::2]
+
+
 def emulate(x, shape, batch, direction, norm=0, double=False, in_place=False, force_maxv=0, smem_limit=0):
     """Run a plan through the FP64 pass emulator; returns (output, plan description)."""
     L = _load("libplan_emulator.so")

@@ -180,6 +180,39 @@ def test_config1_exact_case_vs_oracle(sf, torch, oracle_mod):
     assert np.all(np.abs(out - ora) <= 4e-4 * (1 + np.abs(ora)))
 
 
+LEAN = [
+    # (length, batch, double, stage radices the planner gives the first pass)
+    ([810], 33, False, [2, 15, 3, 3, 3]),
+    ([3000], 9, False, [8, 15, 5, 5]),
+    ([105], 40, False, [15, 7]),
+    ([45], 100, False, [15, 3]),
+    ([2187], 4, False, [3, 3, 3, 3, 3, 3, 3]),
+    ([6125], 3, False, [5, 5, 5, 7, 7]),
+    ([840], 17, True, [8, 3, 5, 7]),
+    ([1125], 5, True, [3, 3, 5, 5, 5]),
+    ([30000], 3, False, [2, 15, 5]),
+    ([680400], 2, False, [2, 15, 3, 3, 3]),
+    ([784000], 1, True, [5, 5, 5, 7]),
+]
+
+
+@pytest.mark.parametrize("shape,batch,dbl,radices", LEAN, ids=lambda v: str(v))
+def test_runtime_length_lean_kernel(sf, torch, shape, batch, dbl, radices):
+    """7-smooth lengths without a size-specialised kernel run on the lean runtime-length kernel
+    (whole lines, or the column and row passes of a four-step), whose stages form each
+    butterfly's twiddles from one base twiddle and, at 16 values a thread, run a (3, 5) pair of
+    stages as one radix-15 stage: both directions and two normalizations against an FP64 FFT."""
+    n = int(np.prod(shape))
+    dt = np.complex128 if dbl else np.complex64
+    x = uniform_complex(n * batch, 4242 + n, dt)
+    for d, norm in ((-1, 0), (1, 3)):
+        out, p = run(sf, torch, x, shape, batch, d, norm, dbl)
+        passes = p.describe()["passes"]
+        assert all(ps["lean"] for ps in passes), passes
+        assert passes[0]["radices"] == radices
+        assert rel_l2(out, fp64_fft(x, shape, batch, d, norm_scale(norm, d, n))) <= spec_tol(n, dbl)
+
+
 GENERIC = [([4096], 16, False), ([13440], 2, False), ([256, 64], 2, True), ([64, 48, 40], 1, False),
            ([2048], 8, True), ([128, 256], 2, False), ([65536], 4, True)]
 

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import fp64_fft, gaussian_complex, norm_scale, rel_l2
-from native_libs import butterfly, emulate
+from native_libs import butterfly, emulate, twiddle_powers
 
 
 @pytest.mark.parametrize("radix", [1, 2, 3, 4, 5, 7, 8, 15, 16])
@@ -21,6 +21,25 @@ def test_butterflies_fp64(radix):
 def test_butterflies_fp32(radix):
     x = gaussian_complex(radix, radix + 100, np.complex128)
     assert np.max(np.abs(butterfly(radix, x, double=False) - np.fft.fft(x))) < 2e-6 * radix
+
+
+@pytest.mark.parametrize("mode", [0])
+@pytest.mark.parametrize("radix", [2, 3, 4, 5, 7, 8, 16])
+def test_twiddle_powers(mode, radix):
+    """The size-specialised kernels form a butterfly's twiddles from one base twiddle
+    W_(Ns*R)^jm by a balanced product tree: u[r] * w^r, exact in FP64 up to rounding and within
+    a few float roundings in FP32."""
+    rng = np.random.default_rng(radix + 10 * mode)
+    for ns in (7, 45, 1024):
+        for jm in (0, 1, ns - 1, int(rng.integers(0, ns))):
+            w = np.exp(-2j * np.pi * jm / (ns * radix))
+            x = gaussian_complex(radix, radix + 7 * jm, np.complex128)
+            want = x * w ** np.arange(radix)
+            got = twiddle_powers(mode, radix, w, x)
+            assert np.max(np.abs(got - want)) < 1e-14 * np.max(np.abs(x)), (ns, jm)
+            w32 = np.complex64(w)
+            got32 = twiddle_powers(mode, radix, w32, x, double=False)
+            assert np.max(np.abs(got32 - want)) < 1e-6 * np.max(np.abs(x)), (ns, jm)
 
 
 SHAPES = [
@@ -194,8 +213,8 @@ def test_fused_single_routes_13440_through_a_catalogued_split(monkeypatch):
 def test_lean_passes_marked():
     """Runtime-length passes over contiguous lines (whole lines, and the column and row passes of
     a contiguous four-step) run on the lean kernel; strided axes, size-specialised, Bluestein and
-    single-stage passes do not. The lean kernel has the general kernel's semantics, so the FP64
-    emulation of these plans (the SHAPES cases above) covers them."""
+    single-stage passes do not. The lean kernel has the general kernel's semantics (plus the
+    radix-15 stage), so the FP64 emulation of these plans (the SHAPES cases above) covers them."""
     from native_libs import describe
 
     def lean(shape, dbl=False):

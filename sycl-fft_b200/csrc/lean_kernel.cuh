@@ -26,7 +26,7 @@ enum : int { kLeanPlain = 0, kLeanTw4 = 1 };
 
 struct LeanParams {
     int n = 0, tpl = 1, w = 1, w_shift = 0;  // w: lines per tile, a power of two (w = 1 << w_shift)
-    int pitch = 0, pad_shift = 31;          // kModeK shared-memory line pitch and padding
+    int pitch = 0;                          // kModeK shared-memory line pitch (padding: kLeanPad)
     int nstages = 0;
     int radix[kMaxStages] = {};
     int ns[kMaxStages] = {};
@@ -59,10 +59,14 @@ __device__ __forceinline__ int lean_quot(const LeanParams& P, int s, int j) {
     return m ? static_cast<int>(__umulhi(static_cast<uint32_t>(j), m) >> P.ns_shift[s]) : (j >> P.ns_shift[s]);
 }
 
+// kModeK rows hold one padding element per 2^kLeanPad (the planner's pad for the precision).
+template <class T>
+constexpr int kLeanPad = sizeof(T) == 4 ? 4 : 3;
+
 template <class T, bool MODEC>
 __device__ __forceinline__ int lean_sidx(const LeanParams& P, int k) {
     if constexpr (MODEC) return k << P.w_shift;
-    else return k + (k >> P.pad_shift);
+    else return k + (k >> kLeanPad<T>);
 }
 
 // One radix-R Stockham stage over the tile: first stage loads from HBM, the last stores to HBM,
@@ -80,6 +84,7 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
     // loads: element k = j + r * nr
     constexpr bool lin_in = MODEC;
     const int in_step = FIRST ? (MODEC ? nr * P.in_ks : nr) : (MODEC ? nr << P.w_shift : 0);
+    [[maybe_unused]] const T in_sy = P.conj_in ? T(-1) : T(1);  // conjugated input: im * -1
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * P.tpl;
@@ -91,7 +96,7 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
                     C a = cmake<C>(T(0), T(0));
                     if (X.line_ok) {
                         a = g[r * in_step];
-                        if (P.conj_in) a.y = -a.y;
+                        a.y *= in_sy;
                     }
                     v[i * R + r] = a;
                 }
@@ -110,6 +115,11 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
     // stores: element k = base + r * Ns (base = j in the last stage)
     constexpr bool lin_out = MODEC;
     const int out_step = to_global ? (MODEC ? nr * P.out_ks : nr) : (MODEC ? Ns << P.w_shift : 0);
+    // Output conjugation folded into the scale (and, with the four-step twiddle, into that
+    // twiddle's sign: conj(u) * w = conj(u * conj(w))), so the store has no select.
+    [[maybe_unused]] const T out_sx = static_cast<T>(P.scale);
+    [[maybe_unused]] const T out_sy = P.conj_out ? -out_sx : out_sx;
+    [[maybe_unused]] const T tw4_sy = (P.tw4_conj != P.conj_out) ? T(-1) : T(1);
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * P.tpl;
@@ -140,16 +150,15 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         C a = u[r];
-                        if (P.conj_out) a.y = -a.y;
                         if constexpr (FEAT == kLeanTw4) {
                             const int m = m0 + r * mstep;
                             C w = cmul(__ldg(static_cast<const C*>(P.tw4_hi) + (m >> P.tw4_shift)),
                                        __ldg(static_cast<const C*>(P.tw4_lo) + (m & ((1 << P.tw4_shift) - 1))));
-                            if (P.tw4_conj) w.y = -w.y;
+                            w.y *= tw4_sy;
                             a = cmul(a, w);
                         }
-                        a.x *= static_cast<T>(P.scale);
-                        a.y *= static_cast<T>(P.scale);
+                        a.x *= out_sx;
+                        a.y *= out_sy;
                         g[r * out_step] = a;
                     }
                 }

@@ -1598,7 +1598,8 @@ static void mark_lean(PassSpec& ps, int64_t cs) {
     }
     const int64_t n = p.n;
     if (p.mode == kModeK && !p.store_via_smem && p.tw4_sign == 0 && p.sel_mode == kSelNone && p.g_k == 1 &&
-        p.in.ks == 1 && p.out.ks == 1 && p.in_len >= n && p.out_len >= n) {
+        p.in.ks == 1 && p.out.ks == 1 && p.in_len >= n && p.out_len >= n &&
+        p.pad_shift == pad_shift_for(cs == 16)) {  // the lean kernel's compile-time row padding
         ps.lean = true;
         ps.lean_feat = 0;
     } else if (p.mode == kModeC && !p.store_via_smem && p.tw4_sign != 0 && p.sel_mode == kSelCol &&

@@ -1106,7 +1106,6 @@ LeanParams to_lean(const PassParams& p) {
     L.w = p.w;
     while ((1 << L.w_shift) < p.w) ++L.w_shift;
     L.pitch = p.pitch;
-    L.pad_shift = p.pad_shift;
     L.nstages = p.fft1.nstages;
     for (int s = 0; s < L.nstages; ++s) {
         L.radix[s] = p.fft1.radix[s];

@@ -228,3 +228,29 @@ def test_lean_passes_marked():
     assert lean([1009]) == [("bluestein_fused", 0)]
     for p in describe([680400], 4)["passes"]:
         assert p["w"] & (p["w"] - 1) == 0 and len(p["radices"]) >= 2
+
+
+def test_lean_radix15_stages():
+    """Float lean passes run each (3, 5) pair of stages as one radix-15 stage (a radix-3, -5 or
+    -15 stage all need n / 15 threads per line at 16 values a thread, so the tile is the same);
+    double lean passes (8 values a thread) keep 3 and 5; a pass is never fused down to a single
+    stage, and the order stays 16, 8, 4, 2, 15, 3, 5, 7."""
+    from native_libs import describe
+
+    def first(n, dbl=False):
+        p = describe([n], 4, double=dbl)["passes"][0]
+        return p["lean"], p["radices"], p["threads"]
+
+    assert first(3000) == (1, [8, 15, 5, 5], 224)
+    assert first(810)[1] == [2, 15, 3, 3, 3]
+    assert first(1125)[1] == [15, 15, 5]
+    assert first(105)[1] == [15, 7]
+    assert first(15)[1] == [3, 5]                      # one radix-15 stage would be a single stage
+    assert first(840, True)[1] == [8, 3, 5, 7]         # double: no radix 15
+    assert first(2187)[1] == [3] * 7                    # no 5 to pair with
+    order = [16, 8, 4, 2, 15, 3, 5, 7]
+    for n in (810, 1125, 3000, 12000, 6125, 30000, 680400):
+        for p in describe([n], 2)["passes"]:
+            if p["lean"]:
+                pos = [order.index(r) for r in p["radices"]]
+                assert pos == sorted(pos), (n, p["radices"])

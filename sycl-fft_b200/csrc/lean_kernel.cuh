@@ -63,6 +63,13 @@ __device__ __forceinline__ int lean_quot(const LeanParams& P, int s, int j) {
 template <class T>
 constexpr int kLeanPad = sizeof(T) == 4 ? 4 : 3;
 
+// Four-step twiddle W_L^m = tw4_hi[m >> tw4_shift] * tw4_lo[m & mask] (m = k * c < L).
+template <class C>
+__device__ __forceinline__ C lean_tw4(const LeanParams& P, int m) {
+    return cmul(__ldg(static_cast<const C*>(P.tw4_hi) + (m >> P.tw4_shift)),
+                __ldg(static_cast<const C*>(P.tw4_lo) + (m & ((1 << P.tw4_shift) - 1))));
+}
+
 template <class T, bool MODEC>
 __device__ __forceinline__ int lean_sidx(const LeanParams& P, int k) {
     if constexpr (MODEC) return k << P.w_shift;
@@ -120,6 +127,16 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
     [[maybe_unused]] const T out_sx = static_cast<T>(P.scale);
     [[maybe_unused]] const T out_sy = P.conj_out ? -out_sx : out_sx;
     [[maybe_unused]] const T tw4_sy = (P.tw4_conj != P.conj_out) ? T(-1) : T(1);
+    // The four-step twiddles of one butterfly's outputs k = j + r * nr form a geometric
+    // sequence, W^(k*c) = W^(j*c) * (W^(nr*c))^r: one table lookup per butterfly, the step once
+    // per thread, then one product per output (at most 14 deep; the last radix is at most 15).
+    [[maybe_unused]] C tw4_step = cmake<C>(T(1), T(0));
+    if constexpr (LAST && FEAT == kLeanTw4) {
+        if (X.line_ok) {
+            tw4_step = lean_tw4<C>(P, nr * X.c);
+            tw4_step.y *= tw4_sy;
+        }
+    }
 #pragma unroll
     for (int i = 0; i < NB; ++i) {
         const int j = X.t + i * P.tpl;
@@ -146,15 +163,16 @@ __device__ __forceinline__ void lean_stage(const LeanParams& P, int s, LeanCtx<T
             if constexpr (to_global) {
                 if (X.line_ok) {
                     C* g = X.gout + (MODEC ? j * P.out_ks : j);
-                    const int m0 = j * X.c, mstep = nr * X.c;
+                    [[maybe_unused]] C w;
+                    if constexpr (FEAT == kLeanTw4) {
+                        w = lean_tw4<C>(P, j * X.c);
+                        w.y *= tw4_sy;
+                    }
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         C a = u[r];
                         if constexpr (FEAT == kLeanTw4) {
-                            const int m = m0 + r * mstep;
-                            C w = cmul(__ldg(static_cast<const C*>(P.tw4_hi) + (m >> P.tw4_shift)),
-                                       __ldg(static_cast<const C*>(P.tw4_lo) + (m & ((1 << P.tw4_shift) - 1))));
-                            w.y *= tw4_sy;
+                            if (r > 0) w = cmul(w, tw4_step);
                             a = cmul(a, w);
                         }
                         a.x *= out_sx;

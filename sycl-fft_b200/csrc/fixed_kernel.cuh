@@ -332,12 +332,30 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
             } else if constexpr (LAST) {
                 // last stage: base == j, outputs at j + r * NR
                 if (X.line_ok) {
+                    // complex<double>: the four-step twiddles of this butterfly's outputs form a
+                    // geometric sequence, W^((j + r*NR)*sel) = W^(j*sel) * (W^(NR*sel))^r, so the
+                    // two-level table is read twice per butterfly instead of per output (R - 1
+                    // products deep; float keeps the per-output lookup, its last radix being 16)
+                    constexpr bool kGeo = (FEAT & kFeatTw4) && sizeof(T) == 8;
+                    [[maybe_unused]] C w4, w4_step;
+                    if constexpr (kGeo) {
+                        const int m0 = j * X.sel, ms = NR * X.sel, mask = (1 << X.tw4_shift) - 1;
+                        w4 = cmul(__ldg(X.tw4_hi + (m0 >> X.tw4_shift)), __ldg(X.tw4_lo + (m0 & mask)));
+                        w4_step = cmul(__ldg(X.tw4_hi + (ms >> X.tw4_shift)), __ldg(X.tw4_lo + (ms & mask)));
+                        if constexpr (FEAT & kFeatTw4Conj) {
+                            w4.y = -w4.y;
+                            w4_step.y = -w4_step.y;
+                        }
+                    }
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int k = j + r * NR;
                         C a = u[r];
                         if (X.conj_out) a.y = -a.y;
-                        if constexpr (FEAT & kFeatTw4) {
+                        if constexpr (kGeo) {
+                            if (r > 0) w4 = cmul(w4, w4_step);
+                            a = cmul(a, w4);
+                        } else if constexpr (FEAT & kFeatTw4) {
                             const int m = k * X.sel;
                             C w = cmul(__ldg(X.tw4_hi + (m >> X.tw4_shift)),
                                        __ldg(X.tw4_lo + (m & ((1 << X.tw4_shift) - 1))));

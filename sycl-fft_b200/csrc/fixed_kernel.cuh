@@ -347,11 +347,17 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                             w4_step.y = -w4_step.y;
                         }
                     }
+                    // with nothing between the output conjugation and the scale, the conjugation
+                    // is the sign of the imaginary part's scale (no select per output)
+                    constexpr bool kFold = !(FEAT & (kFeatTw4 | kFeatPostmul));
+                    [[maybe_unused]] const T sy_out = X.conj_out ? -X.scale : X.scale;
 #pragma unroll
                     for (int r = 0; r < R; ++r) {
                         const int k = j + r * NR;
                         C a = u[r];
-                        if (X.conj_out) a.y = -a.y;
+                        if constexpr (!kFold) {
+                            if (X.conj_out) a.y = -a.y;
+                        }
                         if constexpr (kGeo) {
                             if (r > 0) w4 = cmul(w4, w4_step);
                             a = cmul(a, w4);
@@ -373,7 +379,7 @@ __device__ __forceinline__ void fixed_stage(FixedCtx<T>& X) {
                             if (g >= X.out_len) continue;
                         }
                         a.x *= X.scale;
-                        a.y *= X.scale;
+                        a.y *= kFold ? sy_out : X.scale;
                         if constexpr (FEAT & (kFeatPostmul | kFeatScatter)) {
                             if (X.flip_out) a.y = -a.y;
                         }
